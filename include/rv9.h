@@ -1,0 +1,122 @@
+/*
+ * rv9.h — C ABI of the B200 VP9 decoder.
+ *
+ * The drop-in for rivet-vp9's decoder API (safewords/rivet-vp9):
+ *
+ *   rv9_decoder_new         replaces Decoder::new          src/decoder/mod.rs:150
+ *   rv9_decoder_set_threads replaces Decoder::set_threads  src/decoder/mod.rs:174
+ *   rv9_decoder_set_max_pixels  Decoder::set_max_pixels    src/decoder/mod.rs:186
+ *   rv9_decoder_frames_decoded  Decoder::frames_decoded    src/decoder/mod.rs:214
+ *   rv9_decode              replaces Decoder::decode       src/decoder/mod.rs:193
+ *   rv9_decode_all          replaces Decoder::decode_all   src/decoder/mod.rs:198
+ *   rv9_frame               is Frame (data, planes)        src/frame.rs:115-137
+ *   rv9_status              is Error (Bitstream, Unsupported, InvalidInput)
+ *                                                          src/lib.rs:66-81
+ *
+ * Parsing runs on the host (tile columns on threads); reconstruction —
+ * dequantisation, inverse transforms, inter and intra prediction, compound
+ * averaging and the loop filter — runs as CUDA kernels for sm_100a on the
+ * decoder's GPU. There is no CPU reconstruction path: without a usable CUDA
+ * device rv9_decoder_new returns NULL and rv9_last_global_error says why.
+ *
+ * Frames come back in the reference's Frame layout: the visible Y, U, V
+ * planes one after another, tightly packed (stride == width), one byte per
+ * sample at 8 bits and little-endian uint16 above.
+ */
+#ifndef RV9_H
+#define RV9_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "rv9_records.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rv9_status {
+  RV9_OK = 0,
+  RV9_BITSTREAM = 1,     /* malformed stream (Error::Bitstream) */
+  RV9_UNSUPPORTED = 2,   /* valid but not supported, e.g. over max pixels */
+  RV9_INVALID_INPUT = 3, /* unusable argument (Error::InvalidInput) */
+  RV9_DEVICE = 4,        /* CUDA error or a device-side wait that timed out */
+} rv9_status;
+
+typedef enum rv9_chroma {
+  RV9_YUV420 = 0,
+  RV9_YUV422 = 1,
+  RV9_YUV440 = 2,
+  RV9_YUV444 = 3,
+} rv9_chroma;
+
+typedef struct rv9_plane {
+  size_t offset;   /* byte offset of the plane in data */
+  uint32_t width;  /* samples */
+  uint32_t height;
+} rv9_plane;
+
+typedef struct rv9_frame {
+  uint32_t width, height;      /* luma size */
+  uint32_t bit_depth;          /* 8, 10, 12 */
+  uint32_t chroma;             /* rv9_chroma */
+  uint32_t color_space;        /* as coded, 0..7 (7 = sRGB) */
+  uint32_t full_range;         /* color_range */
+  uint32_t render_width, render_height;
+  uint8_t* data;               /* owned by the frame: rv9_frame_release */
+  size_t size;                 /* bytes in data */
+  rv9_plane planes[3];         /* Y, U, V */
+} rv9_frame;
+
+typedef struct rv9_decoder rv9_decoder;
+
+/* A decoder on CUDA device `device` (-1: the current device). NULL when no
+ * usable device is present or the kernels fail to load. */
+rv9_decoder* rv9_decoder_new(int device);
+void rv9_decoder_free(rv9_decoder* dec);
+/* Host parsing threads: 0 = one per core (default), 1 = the calling thread. */
+void rv9_decoder_set_threads(rv9_decoder* dec, uint32_t threads);
+/* Frames of more than `pixels` luma samples are refused (RV9_UNSUPPORTED). */
+void rv9_decoder_set_max_pixels(rv9_decoder* dec, uint64_t pixels);
+uint64_t rv9_decoder_frames_decoded(const rv9_decoder* dec);
+/* Message of the decoder's last error (valid until the next call). */
+const char* rv9_last_error(const rv9_decoder* dec);
+/* Why the last rv9_decoder_new failed. */
+const char* rv9_last_global_error(void);
+
+/* Decodes one packet (a frame or a superframe). Shown frames go to out[0..],
+ * at most `cap`; *n_out receives how many the packet showed. */
+rv9_status rv9_decode_all(rv9_decoder* dec, const uint8_t* packet, size_t len,
+                          rv9_frame* out, size_t cap, size_t* n_out);
+/* Decodes one packet; the last frame it shows goes to *out and *shown = 1. */
+rv9_status rv9_decode(rv9_decoder* dec, const uint8_t* packet, size_t len,
+                      rv9_frame* out, int* shown);
+/* Frees a frame's data (from rv9_decode / rv9_decode_all). */
+void rv9_frame_release(rv9_frame* frame);
+
+/* Decodes `n` packets in order with host parsing overlapped with device
+ * reconstruction, writing every shown frame's packed samples one after
+ * another into `out` (`cap` bytes). *n_frames and *bytes receive the count
+ * and size written. Frame geometry is that of rv9_decode_all's frames. */
+rv9_status rv9_decode_packets(rv9_decoder* dec, const uint8_t* const* packets,
+                              const size_t* lens, size_t n, uint8_t* out, size_t cap,
+                              size_t* n_frames, size_t* bytes);
+
+/* Timing of the device work since the last reset: reconstruction kernel
+ * time (CUDA events on the decoder's stream), frames reconstructed, and the
+ * algorithmic bytes of those frames (records read, reference samples
+ * predicted from, samples written; 1 byte per sample at 8 bits, 2 above). */
+typedef struct rv9_stats {
+  double device_ms;
+  double parse_ms;
+  uint64_t frames;
+  uint64_t algorithmic_bytes;
+  uint64_t kernel_launches;
+} rv9_stats;
+void rv9_decoder_stats(rv9_decoder* dec, rv9_stats* out, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RV9_H */

@@ -1,0 +1,130 @@
+// Bit readers of the VP9 syntax: the plain f(n)/s(n) reader of the
+// uncompressed header (spec 4.9, 9.1; reference src/bits.rs:13-90) and the
+// boolean arithmetic decoder of spec 9.2 (reference src/bool_coder.rs:12-126).
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+namespace rv9 {
+
+struct HeaderError {
+  const char* msg;
+};
+
+// f(n) / s(n) reader, most significant bit first. Reading past the end throws
+// HeaderError (the uncompressed header is cut short).
+class BitReader {
+ public:
+  BitReader(const uint8_t* d, size_t n) : data_(d), len_(n), pos_(0) {}
+  uint32_t bit() {
+    size_t byte = pos_ >> 3;
+    if (byte >= len_) throw HeaderError{"uncompressed header runs past the end of the frame"};
+    uint32_t b = (data_[byte] >> (7 - (pos_ & 7))) & 1;
+    ++pos_;
+    return b;
+  }
+  uint32_t f(int n) {
+    uint32_t x = 0;
+    for (int i = 0; i < n; ++i) x = (x << 1) | bit();
+    return x;
+  }
+  bool flag() { return bit() != 0; }
+  int32_t s(int n) {
+    int32_t v = (int32_t)f(n);
+    return flag() ? -v : v;
+  }
+  void byte_align() { pos_ = (pos_ + 7) & ~(size_t)7; }
+  size_t position() const { return pos_; }
+
+ private:
+  const uint8_t* data_;
+  size_t len_;
+  size_t pos_;
+};
+
+// Boolean decoder. `value` holds the decoder's current byte (BoolValue of the
+// specification) in bits 63..56 followed by stream bits not yet consumed;
+// `bits` counts the valid bits from bit 63 down. Bits past the end of the
+// data read as zero.
+class BoolDecoder {
+ public:
+  BoolDecoder() = default;
+  // init_bool(sz). Returns false if the data is empty or the marker bit is 1.
+  bool init(const uint8_t* d, size_t n) {
+    p_ = d;
+    end_ = d + n;
+    start_ = d;
+    value_ = 0;
+    bits_ = 0;
+    range_ = 255;
+    if (n == 0) return false;
+    fill();
+    return !read(128);
+  }
+
+  inline bool read(int prob) {
+    uint32_t split = 1 + (((range_ - 1) * (uint32_t)prob) >> 8);
+    uint64_t big = (uint64_t)split << 56;
+    bool bit;
+    if (value_ < big) {
+      range_ = split;
+      bit = false;
+    } else {
+      range_ -= split;
+      value_ -= big;
+      bit = true;
+    }
+    int shift = __builtin_clz(range_) - 24;
+    range_ <<= shift;
+    value_ <<= shift;
+    bits_ -= shift;
+    if (bits_ < 16) fill();
+    return bit;
+  }
+
+  uint32_t literal(int n) {
+    uint32_t x = 0;
+    for (int i = 0; i < n; ++i) x = (x << 1) | (uint32_t)read(128);
+    return x;
+  }
+
+  // Tree decode (spec 9.3.3): `probs(node)` gives the probability of node
+  // index n >> 1.
+  template <class P>
+  inline int tree(const int8_t* t, P probs) {
+    int n = 0;
+    do {
+      n = t[n + (int)read(probs(n >> 1))];
+    } while (n > 0);
+    return -n;
+  }
+
+  // Whether the bits not yet read (the padding, spec 9.2.3) are all zero.
+  bool padding_is_zero() const {
+    if (value_ & ((1ull << 56) - 1)) return false;
+    for (const uint8_t* q = p_; q < end_; ++q)
+      if (*q) return false;
+    return true;
+  }
+
+ private:
+  inline void fill() {
+    while (bits_ <= 56) {
+      if (p_ < end_) {
+        value_ |= (uint64_t)(*p_++) << (56 - bits_);
+        bits_ += 8;
+      } else {
+        bits_ = 64;  // zeros from here on
+        break;
+      }
+    }
+  }
+  const uint8_t* p_ = nullptr;
+  const uint8_t* end_ = nullptr;
+  const uint8_t* start_ = nullptr;
+  uint64_t value_ = 0;
+  int bits_ = 0;
+  uint32_t range_ = 255;
+};
+
+}  // namespace rv9

@@ -1,0 +1,93 @@
+// The host side of the decoder: frame headers, tile and block syntax, motion
+// vector prediction, coefficient tokens and the decoder's frame-to-frame
+// state (reference frame slots' sizes and formats, four frame contexts,
+// previous motion vectors and segment ids). Everything of VP9 decoding except
+// the samples: a parsed frame comes out as records (rv9_records.h) for a
+// reconstruction engine.
+//
+// Follows the reference decoder's frame process (src/decoder/mod.rs:218-422)
+// and its parse-only mode (src/decoder/block.rs:368-1715, mvpred.rs,
+// header.rs, probs.rs), restated in C++.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../../include/rv9_records.h"
+#include "probs.h"
+
+namespace rv9 {
+
+enum Status : int {
+  ST_OK = 0,
+  ST_BITSTREAM = 1,
+  ST_UNSUPPORTED = 2,
+  ST_INVALID_INPUT = 3,
+  ST_DEVICE = 4,
+};
+
+struct Mv {
+  int32_t r, c;
+  bool operator==(const Mv& o) const { return r == o.r && c == o.c; }
+  bool operator!=(const Mv& o) const { return !(*this == o); }
+};
+
+// Per 8x8 position (the MiInfo of reference src/decoder/block.rs:19-31).
+struct MiInfo {
+  uint8_t mi_size;
+  uint8_t skip;
+  uint8_t tx_size;
+  uint8_t y_mode;
+  uint8_t sub_modes[4];
+  uint8_t segment_id;
+  int8_t ref_frame[2];
+  uint8_t interp_filter;
+  Mv mv[2][4];
+};
+
+// A parsed frame: what to do with the reference slots, and the records.
+struct ParsedFrame {
+  bool show_existing = false;  // show_existing_frame: output slot `show_slot`
+  int show_slot = 0;
+  bool show_frame = false;
+  uint8_t refresh_mask = 0;    // slots that receive this frame
+  int ref_slot[3] = {0, 0, 0}; // slots of LAST, GOLDEN, ALTREF (inter frames)
+  rv9_frame_desc desc{};
+  std::vector<rv9_block> blocks;
+  std::vector<rv9_tok> toks;
+  std::vector<uint32_t> coefs;
+  double parse_seconds = 0;
+};
+
+struct SlotInfo {
+  bool valid = false;
+  uint32_t width = 0, height = 0;
+  uint32_t ss_x = 1, ss_y = 1, bit_depth = 8;
+};
+
+class Parser {
+ public:
+  Parser();
+  ~Parser();
+  // 0: one thread per core (tile columns parse in parallel).
+  void set_threads(int n) { threads_ = n; }
+  void set_max_pixels(uint64_t p) { max_pixels_ = p; }
+  uint64_t frames_decoded() const { return frames_; }
+  // Parses one frame (not a superframe). On error returns the status and
+  // fills `err`.
+  Status parse_frame(const uint8_t* data, size_t len, ParsedFrame* out, std::string* err);
+
+  struct Impl;
+
+ private:
+  Impl* impl_;
+  int threads_ = 0;
+  uint64_t max_pixels_ = 8192ull * 8192ull;
+  uint64_t frames_ = 0;
+};
+
+// Annex B: splits a packet into its frames (reference src/superframe.rs:6-53).
+void superframe_split(const uint8_t* pkt, size_t len, std::vector<std::pair<size_t, size_t>>* out);
+
+}  // namespace rv9
