@@ -1132,3 +1132,25 @@ rv9_status rv9o_decode_packets(rv9o_decoder* d, const uint8_t* const* pkts, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Entry points for the kernel-arithmetic tests: the oracle's sample
+// operations on caller buffers.
+extern "C" {
+
+void rv9o_test_itx(const int32_t* coefs, int n, int tx_type, int lossless, int eob, int bit_depth, uint16_t* dst,
+                   int stride) {
+  oracle::inverse_transform_add(coefs, n, tx_type, lossless != 0, eob, bit_depth, dst, stride);
+}
+
+void rv9o_test_intra(int mode, int log2, const int32_t* above, const int32_t* left, int have_left, int have_above,
+                     int bit_depth, uint16_t* dst, int stride) {
+  oracle::intra_predict(mode, log2, above, left, have_left != 0, have_above != 0, bit_depth, dst, stride);
+}
+
+// Filters the line of 16 samples whose q0 is buf[8].
+void rv9o_test_lf(uint16_t* buf, int filter_size, int limit, int blimit, int thresh, int bit_depth) {
+  oracle::lf_filter(buf, 8, 1, filter_size, limit, blimit, thresh, bit_depth);
+}
+
+}  // extern "C"

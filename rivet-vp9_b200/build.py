@@ -1,0 +1,81 @@
+#!/usr/bin/env python3
+"""Builds the decoder library in-tree: rivet-vp9_b200/_build/librv9.so.
+
+The CUDA kernels are compiled for sm_100a (B200) only; the host parser, the
+engine and the C ABI are compiled into the same shared library. nvcc
+cross-compiles, so this runs on a machine without a GPU.
+
+Usage: python rivet-vp9_b200/build.py [--force]
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "_build")
+LIB = os.path.join(OUT, "librv9.so")
+
+SOURCES = [
+    "gpu/kernels.cu",
+    "gpu/engine.cpp",
+    "api/rv9_api.cpp",
+    "host/parser.cpp",
+    "host/probs.cpp",
+]
+HEADERS = [
+    "gpu/dsp_math.cuh",
+    "gpu/engine_types.h",
+    "gpu/engine.h",
+    "host/parser.h",
+    "host/probs.h",
+    "host/bitreader.h",
+    "common/vp9_tables.h",
+    "common/vp9_consts.h",
+]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.isabs(c) and os.path.exists(c) or not os.path.isabs(c)):
+            return c
+    return "nvcc"
+
+
+def stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
+    deps += [os.path.join(HERE, "..", "include", h) for h in ("rv9.h", "rv9_records.h")]
+    deps.append(os.path.abspath(__file__))
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False):
+    if not force and not stale():
+        return LIB
+    os.makedirs(OUT, exist_ok=True)
+    objs = []
+    for s in SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(OUT, os.path.basename(s) + ".o")
+        cmd = [nvcc(), "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+               *ARCH, "-c", src, "-o", obj]
+        if s.endswith(".cpp"):
+            cmd[1:1] = ["-x", "cu"] if s.startswith("gpu/") else []
+        if "-Xptxas" in os.environ.get("RV9_NVCC_FLAGS", ""):
+            cmd += os.environ["RV9_NVCC_FLAGS"].split()
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    subprocess.run([nvcc(), "-shared", *ARCH, "-o", tmp, *objs, "-lcudart", "-lpthread"], check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

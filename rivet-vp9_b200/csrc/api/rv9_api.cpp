@@ -1,0 +1,163 @@
+// The C ABI of rv9.h: the reference decoder API (src/decoder/mod.rs:150-216)
+// over the host parser and the CUDA reconstruction engine.
+#include <stdlib.h>
+#include <string.h>
+
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "../../../include/rv9.h"
+#include "../gpu/engine.h"
+#include "../host/parser.h"
+
+struct rv9_decoder {
+  rv9::Parser parser;
+  rv9g::Engine engine;
+  std::string err;
+  rv9::ParsedFrame pf;
+  double parse_ms = 0;
+};
+
+static thread_local std::string g_global_err;
+
+static void fill_meta(const rv9g::DevFrame* f, rv9_frame* out) {
+  out->width = f->width;
+  out->height = f->height;
+  out->bit_depth = f->bit_depth;
+  out->chroma = f->ss_x ? (f->ss_y ? RV9_YUV420 : RV9_YUV422) : (f->ss_y ? RV9_YUV440 : RV9_YUV444);
+  out->color_space = f->color_space;
+  out->full_range = f->color_range;
+  out->render_width = f->render_w;
+  out->render_height = f->render_h;
+  size_t bps = f->bps(), off = 0;
+  for (int p = 0; p < 3; ++p) {
+    uint32_t w = p ? (f->width + f->ss_x) >> f->ss_x : f->width;
+    uint32_t h = p ? (f->height + f->ss_y) >> f->ss_y : f->height;
+    out->planes[p].offset = off;
+    out->planes[p].width = w;
+    out->planes[p].height = h;
+    off += (size_t)w * h * bps;
+  }
+  out->size = off;
+}
+
+extern "C" {
+
+rv9_decoder* rv9_decoder_new(int device) {
+  rv9_decoder* d = new rv9_decoder;
+  std::string err;
+  if (!d->engine.init(device, &err)) {
+    g_global_err = err;
+    delete d;
+    return nullptr;
+  }
+  return d;
+}
+
+void rv9_decoder_free(rv9_decoder* d) { delete d; }
+void rv9_decoder_set_threads(rv9_decoder* d, uint32_t t) { d->parser.set_threads((int)t); }
+void rv9_decoder_set_max_pixels(rv9_decoder* d, uint64_t p) { d->parser.set_max_pixels(p); }
+uint64_t rv9_decoder_frames_decoded(const rv9_decoder* d) { return d->parser.frames_decoded(); }
+const char* rv9_last_error(const rv9_decoder* d) { return d->err.c_str(); }
+const char* rv9_last_global_error(void) { return g_global_err.c_str(); }
+
+// One frame of a packet: parse, reconstruct; the shown frame (if any).
+static rv9_status decode_one(rv9_decoder* d, const uint8_t* data, size_t len, rv9g::DevFrame** shown) {
+  auto t0 = std::chrono::steady_clock::now();
+  rv9::Status st = d->parser.parse_frame(data, len, &d->pf, &d->err);
+  d->parse_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (st != rv9::ST_OK) return (rv9_status)st;
+  st = d->engine.recon(d->pf, shown, &d->err);
+  return (rv9_status)st;
+}
+
+rv9_status rv9_decode_all(rv9_decoder* d, const uint8_t* pkt, size_t len, rv9_frame* out, size_t cap,
+                          size_t* n_out) {
+  *n_out = 0;
+  if (!d || (!pkt && len)) return RV9_INVALID_INPUT;
+  std::vector<std::pair<size_t, size_t>> frames;
+  rv9::superframe_split(pkt, len, &frames);
+  for (auto& fr : frames) {
+    rv9g::DevFrame* shown = nullptr;
+    rv9_status st = decode_one(d, pkt + fr.first, fr.second, &shown);
+    if (st != RV9_OK) return st;
+    if (shown) {
+      if (*n_out < cap) {
+        rv9_frame* o = &out[*n_out];
+        fill_meta(shown, o);
+        o->data = (uint8_t*)malloc(o->size ? o->size : 1);
+        rv9::Status s2 = d->engine.download(shown, o->data, &d->err);
+        if (s2 != rv9::ST_OK) return (rv9_status)s2;
+      }
+      ++*n_out;
+    }
+  }
+  return RV9_OK;
+}
+
+rv9_status rv9_decode(rv9_decoder* d, const uint8_t* pkt, size_t len, rv9_frame* out, int* shown) {
+  *shown = 0;
+  std::vector<rv9_frame> frames(8);
+  size_t n = 0;
+  rv9_status st = rv9_decode_all(d, pkt, len, frames.data(), frames.size(), &n);
+  if (st != RV9_OK) return st;
+  size_t kept = n < frames.size() ? n : frames.size();
+  for (size_t i = 0; i + 1 < kept; ++i) rv9_frame_release(&frames[i]);
+  if (kept > 0) {
+    *out = frames[kept - 1];
+    *shown = 1;
+  }
+  return RV9_OK;
+}
+
+void rv9_frame_release(rv9_frame* f) {
+  if (!f) return;
+  free(f->data);
+  f->data = nullptr;
+  f->size = 0;
+}
+
+rv9_status rv9_decode_packets(rv9_decoder* d, const uint8_t* const* pkts, const size_t* lens, size_t n,
+                              uint8_t* out, size_t cap, size_t* n_frames, size_t* bytes) {
+  *n_frames = 0;
+  *bytes = 0;
+  std::vector<std::pair<size_t, size_t>> frames;
+  for (size_t i = 0; i < n; ++i) {
+    rv9::superframe_split(pkts[i], lens[i], &frames);
+    for (auto& fr : frames) {
+      rv9g::DevFrame* shown = nullptr;
+      rv9_status st = decode_one(d, pkts[i] + fr.first, fr.second, &shown);
+      if (st != RV9_OK) return st;
+      if (shown) {
+        size_t nb = rv9g::Engine::packed_bytes(shown);
+        if (*bytes + nb > cap) {
+          d->err = "output buffer too small";
+          return RV9_INVALID_INPUT;
+        }
+        rv9::Status s2 = d->engine.download_async(shown, out + *bytes, &d->err);
+        if (s2 != rv9::ST_OK) return (rv9_status)s2;
+        *bytes += nb;
+        ++*n_frames;
+      }
+    }
+  }
+  return (rv9_status)d->engine.sync(&d->err);
+}
+
+void rv9_decoder_stats(rv9_decoder* d, rv9_stats* out, int reset) {
+  out->device_ms = d->engine.device_ms;
+  out->parse_ms = d->parse_ms;
+  out->frames = d->engine.frames;
+  out->algorithmic_bytes = d->engine.alg_bytes;
+  out->kernel_launches = d->engine.launches;
+  if (reset) {
+    d->engine.device_ms = 0;
+    d->parse_ms = 0;
+    d->engine.frames = 0;
+    d->engine.alg_bytes = 0;
+    d->engine.launches = 0;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,453 @@
+// Per-sample arithmetic of VP9 reconstruction, written once for the CUDA
+// kernels. Every function here is __host__ __device__ so that the same code
+// can be compiled for the CPU and checked against the oracle without a GPU.
+//
+// - Inverse DCT / ADST / WHT (spec 8.7.1): the butterfly network with its
+//   intermediate rounding, compile-time sized so that the index arithmetic and
+//   the cosine constants fold away. Lanes: L32 (8 bits; 32-bit wrapping
+//   arithmetic) and L64 (10/12 bits; 64-bit values whose multiplications take
+//   the low 32 bits of the operand), matching the reference's S32 / S64
+//   (rivet-vp9 src/dsp/itx.rs:574-666).
+// - Intra predictors (spec 8.5.1.1) as closed forms: each sample computed
+//   directly from the edge arrays, so a warp predicts a block in parallel; the
+//   directional modes' copy recurrences (reference src/dsp/intra.rs:49-144)
+//   are unrolled into an index into their first row or column.
+// - Loop filter sample operations (spec 8.8.5; reference src/dsp/lf.rs:24-143)
+//   on one line of 16 samples across an edge.
+#pragma once
+#include <stdint.h>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
+#define RV9_HD __host__ __device__ __forceinline__
+
+namespace rv9g {
+
+// ---------------------------------------------------------------------------
+// Transforms.
+
+RV9_HD constexpr int32_t cos64(int angle) {
+  // cos64_lookup (spec 8.7.1.1), folded by quadrant.
+  constexpr int32_t C[33] = {16384, 16364, 16305, 16207, 16069, 15893, 15679, 15426, 15137, 14811, 14449,
+                             14053, 13623, 13160, 12665, 12140, 11585, 11003, 10394, 9760,  9102,  8423,
+                             7723,  7005,  6270,  5520,  4756,  3981,  3196,  2404,  1606,  804,   0};
+  return (angle & 127) <= 32   ? C[angle & 127]
+         : (angle & 127) <= 64 ? -C[64 - (angle & 127)]
+         : (angle & 127) <= 96 ? -C[(angle & 127) - 64]
+                               : C[128 - (angle & 127)];
+}
+RV9_HD constexpr int32_t sin64(int angle) { return cos64(angle - 32); }
+
+RV9_HD constexpr int brev(int num_bits, int x) {
+  int t = 0;
+  for (int i = 0; i < num_bits; ++i) t |= ((x >> i) & 1) << (num_bits - 1 - i);
+  return t;
+}
+
+struct L32 {
+  typedef int32_t store_t;
+  int32_t v;
+  static RV9_HD L32 zero() { return L32{0}; }
+  static RV9_HD L32 load(int32_t x) { return L32{x}; }
+  RV9_HD L32 add(L32 o) const { return L32{(int32_t)((uint32_t)v + (uint32_t)o.v)}; }
+  RV9_HD L32 sub(L32 o) const { return L32{(int32_t)((uint32_t)v - (uint32_t)o.v)}; }
+  RV9_HD L32 mul(int32_t c) const { return L32{(int32_t)((uint32_t)v * (uint32_t)c)}; }
+  RV9_HD L32 rshift(int n) const { return L32{(int32_t)((uint32_t)v + (1u << (n - 1))) >> n}; }
+  RV9_HD L32 sar(int n) const { return L32{v >> n}; }
+  // Residual clamped to +-2^16, as the reference's lanes clamp it.
+  RV9_HD int32_t residual() const { return v < -(1 << 16) ? -(1 << 16) : (v > (1 << 16) ? (1 << 16) : v); }
+};
+
+struct L64 {
+  typedef int64_t store_t;
+  int64_t v;
+  static RV9_HD L64 zero() { return L64{0}; }
+  static RV9_HD L64 load(int64_t x) { return L64{x}; }
+  RV9_HD L64 add(L64 o) const { return L64{(int64_t)((uint64_t)v + (uint64_t)o.v)}; }
+  RV9_HD L64 sub(L64 o) const { return L64{(int64_t)((uint64_t)v - (uint64_t)o.v)}; }
+  RV9_HD L64 mul(int32_t c) const { return L64{(int64_t)(int32_t)(uint32_t)(uint64_t)v * (int64_t)c}; }
+  RV9_HD L64 rshift(int n) const { return L64{(int64_t)((uint64_t)v + (1ull << (n - 1))) >> n}; }
+  RV9_HD L64 sar(int n) const { return L64{v >> n}; }
+  RV9_HD int32_t residual() const {
+    return (int32_t)(v < -(1 << 16) ? -(1 << 16) : (v > (1 << 16) ? (1 << 16) : v));
+  }
+};
+
+template <class V>
+RV9_HD V round14(V x) {
+  return x.rshift(14);
+}
+
+template <class V>
+RV9_HD void bfly(V* t, int a, int b, int angle, bool flip) {
+  const int32_t c = cos64(angle), s = sin64(angle);
+  V x = round14(t[a].mul(c).sub(t[b].mul(s)));
+  V y = round14(t[a].mul(s).add(t[b].mul(c)));
+  t[a] = flip ? y : x;
+  t[b] = flip ? x : y;
+}
+
+template <class V>
+RV9_HD void hada(V* t, int a, int b, bool flip) {
+  int p = flip ? b : a, q = flip ? a : b;
+  V x = t[p], y = t[q];
+  t[p] = x.add(y);
+  t[q] = x.sub(y);
+}
+
+template <class V>
+RV9_HD void sbfly(const V* t, V* s, int a, int b, int angle, bool flip) {
+  const int32_t c = cos64(angle), sn = sin64(angle);
+  V x = t[a].mul(c).sub(t[b].mul(sn));
+  V y = t[a].mul(sn).add(t[b].mul(c));
+  s[a] = flip ? y : x;
+  s[b] = flip ? x : y;
+}
+
+template <class V>
+RV9_HD void shada(V* t, const V* s, int a, int b) {
+  t[a] = round14(s[a].add(s[b]));
+  t[b] = round14(s[a].sub(s[b]));
+}
+
+// The inverse DCT steps of size 2^n after the recursive call (spec 8.7.1.3).
+template <int n, class V>
+RV9_HD void idct_stage(V* t) {
+  constexpr int n0 = 1 << n, n1 = n0 >> 1, n2 = n0 >> 2, n3 = n0 >> 3;
+#pragma unroll
+  for (int i = 0; i < n2; ++i) bfly(t, n1 + i, n0 - 1 - i, 32 - brev(5, n1 + i), false);
+  if (n >= 3) {
+#pragma unroll
+    for (int i = 0; i < n3; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) hada(t, n1 + 4 * i + 2 * j, n1 + 1 + 4 * i + 2 * j, j == 1);
+  }
+  if (n == 5) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        bfly(t, n0 - n + 3 - n2 * j - 4 * i, n1 + n - 4 + n2 * j + 4 * i, 28 - 16 * i + 56 * j, true);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) hada(t, n1 + n3 * j + i, n1 + n2 - 5 + n3 * j - i, (j & 1) == 1);
+  }
+  if (n >= 4) {
+    constexpr int imax = n == 5 ? 1 : 0;
+#pragma unroll
+    for (int i = 0; i <= imax; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) bfly(t, n0 - n + 2 - i - n2 * j, n1 + n - 3 + i + n2 * j, 24 + 48 * j, true);
+#pragma unroll
+    for (int i = 0; i < 2 * n - 6; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) hada(t, n1 + n2 * j + i, n1 + n2 - 1 + n2 * j - i, (j & 1) == 1);
+  }
+  if (n >= 3) {
+#pragma unroll
+    for (int i = 0; i < n3; ++i) bfly(t, n0 - n3 - 1 - i, n1 + n3 + i, 16, true);
+  }
+#pragma unroll
+  for (int i = 0; i < n1; ++i) hada(t, i, n0 - 1 - i, false);
+}
+
+template <int n, class V>
+RV9_HD void idct(V* t) {
+  constexpr int n0 = 1 << n;
+  V c[n0];
+#pragma unroll
+  for (int i = 0; i < n0; ++i) c[i] = t[i];
+#pragma unroll
+  for (int i = 0; i < n0; ++i) t[i] = c[brev(n, i)];
+  bfly(t, 0, 1, 16, true);
+  idct_stage<2>(t);
+  if (n >= 3) idct_stage<(n >= 3 ? 3 : 2)>(t);
+  if (n >= 4) idct_stage<(n >= 4 ? 4 : 2)>(t);
+  if (n >= 5) idct_stage<(n >= 5 ? 5 : 2)>(t);
+}
+
+template <int n, class V>
+RV9_HD void adst_in_perm(V* t) {
+  constexpr int n0 = 1 << n, n1 = n0 >> 1;
+  V c[n0];
+#pragma unroll
+  for (int i = 0; i < n0; ++i) c[i] = t[i];
+#pragma unroll
+  for (int i = 0; i < n1; ++i) {
+    t[2 * i] = c[n0 - 1 - 2 * i];
+    t[2 * i + 1] = c[2 * i];
+  }
+}
+
+template <int n, class V>
+RV9_HD void adst_out_perm(V* t) {
+  constexpr int n0 = 1 << n;
+  V c[n0];
+#pragma unroll
+  for (int i = 0; i < n0; ++i) c[i] = t[i];
+  if (n == 4) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      int a = (q >> 3) & 1, b = (q >> 2) & 1, cc = (q >> 1) & 1, d = q & 1;
+      t[q] = c[8 * (d ^ cc) + 4 * (cc ^ b) + 2 * (b ^ a) + a];
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      int a = (q >> 2) & 1, b = (q >> 1) & 1, cc = q & 1;
+      t[q] = c[4 * (cc ^ b) + 2 * (b ^ a) + a];
+    }
+  }
+}
+
+template <class V>
+RV9_HD void iadst4(V* t) {
+  V s0 = t[0].mul(5283), s1 = t[0].mul(9929), s2 = t[1].mul(13377);
+  V s3 = t[2].mul(15212), s4 = t[2].mul(5283), s5 = t[3].mul(9929);
+  V s6 = t[3].mul(15212);
+  V v = t[0].sub(t[2]).add(t[3]);
+  V s7 = v.mul(13377);
+  V x0 = s0.add(s3).add(s5), x1 = s1.sub(s4).sub(s6), x2 = s7, x3 = s2;
+  t[0] = round14(x0.add(x3));
+  t[1] = round14(x1.add(x3));
+  t[2] = round14(x2);
+  t[3] = round14(x0.add(x1).sub(x3));
+}
+
+template <class V>
+RV9_HD void iadst8(V* t) {
+  V s[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s[i] = V::zero();
+  adst_in_perm<3>(t);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) sbfly(t, s, 2 * i, 1 + 2 * i, 30 - 8 * i, true);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) shada(t, s, i, 4 + i);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) sbfly(t, s, 4 + 3 * i, 5 + i, 24 - 16 * i, true);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) shada(t, s, 4 + i, 6 + i);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) hada(t, i, 2 + i, false);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) bfly(t, 2 + 4 * i, 3 + 4 * i, 16, true);
+  adst_out_perm<3>(t);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) t[1 + 2 * i] = V::zero().sub(t[1 + 2 * i]);
+}
+
+template <class V>
+RV9_HD void iadst16(V* t) {
+  V s[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) s[i] = V::zero();
+  adst_in_perm<4>(t);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) sbfly(t, s, 2 * i, 1 + 2 * i, 31 - 4 * i, true);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) shada(t, s, i, 8 + i);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) sbfly(t, s, 8 + 2 * i, 9 + 2 * i, 28 - 16 * i, true);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) shada(t, s, 8 + i, 12 + i);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) hada(t, i, 4 + i, false);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) sbfly(t, s, 4 + 8 * i + 3 * j, 5 + 8 * i + j, 24 - 16 * j, true);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) shada(t, s, 4 + 8 * j + i, 6 + 8 * j + i);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) hada(t, 8 * j + i, 2 + 8 * j + i, false);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) bfly(t, 2 + 4 * j + 8 * i, 3 + 4 * j + 8 * i, 48 + 64 * (i ^ j), false);
+  adst_out_perm<4>(t);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) t[1 + 12 * j + 2 * i] = V::zero().sub(t[1 + 12 * j + 2 * i]);
+}
+
+template <class V>
+RV9_HD void iwht(V* t, int shift) {
+  V a = t[0].sar(shift), c = t[1].sar(shift), d = t[2].sar(shift), b = t[3].sar(shift);
+  a = a.add(c);
+  d = d.sub(b);
+  V e = a.sub(d).sar(1);
+  b = e.sub(b);
+  c = e.sub(c);
+  a = a.sub(b);
+  d = d.add(c);
+  t[0] = a;
+  t[1] = b;
+  t[2] = c;
+  t[3] = d;
+}
+
+// One 1D inverse transform of size 2^n: `kind` 0 DCT, 1 ADST, 2 WHT.
+template <int n, class V>
+RV9_HD void tx1d(V* t, int kind, int wht_shift) {
+  if (kind == 2) {
+    if (n == 2) iwht(t, wht_shift);
+  } else if (kind == 0) {
+    idct<n>(t);
+  } else {
+    if (n == 2) iadst4(t);
+    if (n == 3) iadst8(t);
+    if (n == 4) iadst16(t);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Intra prediction: sample (i, j) of a 2^log2 square block.
+// `above[k + 1]` is aboveRow[k] for k in -1 .. 2*size-1; `left[k]` leftCol[k].
+// `dc` is the DC_PRED value (computed once per block). Modes use the
+// specification's numbering (DC 0, V 1, H 2, D45 3, D135 4, D117 5, D153 6,
+// D207 7, D63 8, TM 9).
+
+RV9_HD int32_t r2(int32_t x, int n) { return (x + (1 << (n - 1))) >> n; }
+
+RV9_HD int32_t intra_pixel(int mode, int i, int j, int size, const int32_t* above, const int32_t* left,
+                           int32_t dc, int32_t maxv) {
+#define A(k) above[(k) + 1]
+#define L(k) left[(k)]
+  switch (mode) {
+    case 1:  // V
+      return A(j);
+    case 2:  // H
+      return L(i);
+    case 3: {  // D45
+      int k = i + j;
+      return (i + j + 2 < size * 2) ? r2(A(k) + A(k + 1) * 2 + A(k + 2), 2) : A(2 * size - 1);
+    }
+    case 4: {  // D135: dst[i][j] = dst[i-1][j-1]
+      int k = i < j ? i : j;
+      int ii = i - k, jj = j - k;
+      if (ii == 0) return jj == 0 ? r2(L(0) + 2 * A(-1) + A(0), 2) : r2(A(jj - 2) + 2 * A(jj - 1) + A(jj), 2);
+      return ii == 1 ? r2(A(-1) + 2 * L(0) + L(1), 2) : r2(L(ii - 2) + 2 * L(ii - 1) + L(ii), 2);
+    }
+    case 5: {  // D117: dst[i][j] = dst[i-2][j-1]
+      int k = (i >> 1) < j ? (i >> 1) : j;
+      int ii = i - 2 * k, jj = j - k;
+      if (ii == 0) return r2(A(jj - 1) + A(jj), 1);
+      if (ii == 1) return jj == 0 ? r2(L(0) + 2 * A(-1) + A(0), 2) : r2(A(jj - 2) + 2 * A(jj - 1) + A(jj), 2);
+      return ii == 2 ? r2(A(-1) + 2 * L(0) + L(1), 2) : r2(L(ii - 3) + 2 * L(ii - 2) + L(ii - 1), 2);
+    }
+    case 6: {  // D153: dst[i][j] = dst[i-1][j-2]
+      int k = i < (j >> 1) ? i : (j >> 1);
+      int ii = i - k, jj = j - 2 * k;
+      if (jj == 0) return ii == 0 ? r2(L(0) + A(-1), 1) : r2(L(ii - 1) + L(ii), 1);
+      if (jj == 1) {
+        if (ii == 0) return r2(L(0) + 2 * A(-1) + A(0), 2);
+        if (ii == 1) return r2(A(-1) + 2 * L(0) + L(1), 2);
+        return r2(L(ii - 2) + 2 * L(ii - 1) + L(ii), 2);
+      }
+      return r2(A(jj - 3) + 2 * A(jj - 2) + A(jj - 1), 2);
+    }
+    case 7: {  // D207: dst[i][j] = dst[i+1][j-2]; the last row is leftCol[size-1]
+      int ii = i + (j >> 1);
+      if (ii >= size - 1) return L(size - 1);
+      if ((j & 1) == 0) return r2(L(ii) + L(ii + 1), 1);
+      if (ii < size - 2) return r2(L(ii) + 2 * L(ii + 1) + L(ii + 2), 2);
+      return r2(L(size - 2) + 3 * L(size - 1), 2);
+    }
+    case 8: {  // D63
+      int k = (i >> 1) + j;
+      return (i & 1) ? r2(A(k) + A(k + 1) * 2 + A(k + 2), 2) : r2(A(k) + A(k + 1), 1);
+    }
+    case 9: {  // TM
+      int32_t v = A(j) + L(i) - A(-1);
+      return v < 0 ? 0 : (v > maxv ? maxv : v);
+    }
+    default:
+      return dc;
+  }
+#undef A
+#undef L
+}
+
+// DC_PRED's value (reference src/dsp/intra.rs:153-174) from the edge sums.
+RV9_HD int32_t intra_dc(int log2, int32_t sum_above, int32_t sum_left, bool have_left, bool have_above,
+                        int bit_depth) {
+  int size = 1 << log2;
+  if (have_left && have_above) return (sum_above + sum_left + size) >> (log2 + 1);
+  if (have_left) return (sum_left + (1 << (log2 - 1))) >> log2;
+  if (have_above) return (sum_above + (1 << (log2 - 1))) >> log2;
+  return 1 << (bit_depth - 1);
+}
+
+// ---------------------------------------------------------------------------
+// Loop filter on one line across an edge: s[0..15] are the samples at
+// offsets -8..7 from the edge (s[8] is q0). Returns nothing; modifies s.
+
+RV9_HD int iabs(int v) { return v < 0 ? -v : v; }
+RV9_HD int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+RV9_HD void lf_line(int* s, int filter_size, int limit, int blimit, int thresh, int bd) {
+  int q0 = s[8], q1 = s[9], q2 = s[10], q3 = s[11];
+  int p0 = s[7], p1 = s[6], p2 = s[5], p3 = s[4];
+  int sh = bd - 8;
+  int limit_bd = limit << sh, blimit_bd = blimit << sh;
+  if (iabs(p3 - p2) > limit_bd || iabs(p2 - p1) > limit_bd || iabs(p1 - p0) > limit_bd ||
+      iabs(q1 - q0) > limit_bd || iabs(q2 - q1) > limit_bd || iabs(q3 - q2) > limit_bd ||
+      iabs(p0 - q0) * 2 + iabs(p1 - q1) / 2 > blimit_bd)
+    return;
+  int thresh_bd = thresh << sh;
+  bool hev = iabs(p1 - p0) > thresh_bd || iabs(q1 - q0) > thresh_bd;
+  int one = 1 << sh;
+  bool flat = filter_size >= 1 && iabs(p1 - p0) <= one && iabs(q1 - q0) <= one && iabs(p2 - p0) <= one &&
+              iabs(q2 - q0) <= one && iabs(p3 - p0) <= one && iabs(q3 - q0) <= one;
+  if (filter_size == 0 || !flat) {
+    // Narrow filter (spec 8.8.5.2).
+    int lo = -(1 << (bd - 1)), hi = (1 << (bd - 1)) - 1;
+    int off = 0x80 << sh;
+    int ps1 = p1 - off, ps0 = p0 - off, qs0 = q0 - off, qs1 = q1 - off;
+    int f = hev ? iclamp(ps1 - qs1, lo, hi) : 0;
+    f = iclamp(f + 3 * (qs0 - ps0), lo, hi);
+    int f1 = iclamp(f + 4, lo, hi) >> 3, f2 = iclamp(f + 3, lo, hi) >> 3;
+    s[8] = iclamp(qs0 - f1, lo, hi) + off;
+    s[7] = iclamp(ps0 + f2, lo, hi) + off;
+    if (!hev) {
+      int g = (f1 + 1) >> 1;
+      s[9] = iclamp(qs1 - g, lo, hi) + off;
+      s[6] = iclamp(ps1 + g, lo, hi) + off;
+    }
+    return;
+  }
+  bool flat2 = false;
+  if (filter_size >= 2) {
+    flat2 = true;
+#pragma unroll
+    for (int k = 4; k < 8; ++k)
+      if (iabs(s[8 - k - 1] - p0) > one || iabs(s[8 + k] - q0) > one) flat2 = false;
+  }
+  // Wide filter (spec 8.8.5.3): a rounded sliding mean over 8 or 16 taps.
+  int log2 = (filter_size == 1 || !flat2) ? 3 : 4;
+  int n = (1 << (log2 - 1)) - 1;
+  int f[16];
+  for (int i = -n; i < n; ++i) {
+    int t = s[i + 8];
+    for (int j = -n; j <= n; ++j) {
+      int p = i + j;
+      p = p < -(n + 1) ? -(n + 1) : (p > n ? n : p);
+      t += s[p + 8];
+    }
+    f[i + 8] = (t + (1 << (log2 - 1))) >> log2;
+  }
+  for (int i = -n; i < n; ++i) s[i + 8] = f[i + 8];
+}
+
+}  // namespace rv9g

@@ -1,0 +1,746 @@
+// CUDA kernels of VP9 reconstruction for sm_100a.
+//
+// One frame is reconstructed by a short chain of launches on the decoder's
+// stream (reference process: FrameDec::replay, src/decoder/block.rs:1405-1498,
+// then loopfilter::filter_frame, src/decoder/loopfilter.rs:51-81):
+//
+//   k_zero_pad    zero the samples beyond the mode-info area (the reference
+//                 reconstructs into zeroed planes, src/decoder/pool.rs:1-6)
+//   k_lf_mi       per 8x8 loop-filter record from the block records
+//   k_intra_mark  mark the 4x4 cells of intra transform blocks pending
+//   k_inter       inter prediction: one CTA per prediction region, 8-tap
+//                 H then V passes through shared memory, scaled references,
+//                 compound averaging fused (src/dsp/inter.rs, pixel.rs)
+//   k_inter_res   inverse transform + add of inter blocks' residuals: one
+//                 warp per transform block (src/dsp/itx.rs)
+//   k_intra       intra prediction + residual as a dependency wavefront:
+//                 a persistent grid takes transform blocks in bitstream order
+//                 and each warp waits only for the 4x4 cells its edges read
+//   k_lf          loop filter as a superblock wavefront: superblock (r, c)
+//                 waits for (r, c-1) and (r-1, c+1), then filters its
+//                 vertical then horizontal edges in shared memory
+//
+// Inter prediction reads only reference frames, so it runs fully parallel
+// before the intra wavefront. Every wait is bounded: on timeout a kernel
+// records an error code, sets the abort flag and returns.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dsp_math.cuh"
+#include "engine_types.h"
+
+namespace rv9g {
+
+__constant__ int16_t c_filters[4][16][8];
+
+static constexpr int kWaitLimit = 1 << 22;  // polls before a wait gives up
+
+template <class T>
+__device__ __forceinline__ T* plane_ptr(const PlanePtr& p) {
+  return reinterpret_cast<T*>(p.data);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ---------------------------------------------------------------------------
+// Zero the samples of the SB-aligned planes outside the mode-info area.
+
+template <class T>
+__global__ void k_zero_pad(KFrame k) {
+  int plane = blockIdx.y;
+  int sx = plane ? k.ss_x : 0, sy = plane ? k.ss_y : 0;
+  int mw = (k.mi_cols * 8) >> sx, mh = (k.mi_rows * 8) >> sy;
+  int aw = (k.sb64_cols * 64) >> sx, ah = (k.sb64_rows * 64) >> sy;
+  T* d = plane_ptr<T>(k.cur[plane]);
+  int stride = k.cur[plane].stride;
+  // Right strip then bottom strip.
+  int right = (aw - mw) * mh;
+  int total = right + (ah - mh) * aw;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    int x, y;
+    if (i < right) {
+      y = i / (aw - mw);
+      x = mw + i % (aw - mw);
+    } else {
+      int j = i - right;
+      y = mh + j / aw;
+      x = j % aw;
+    }
+    d[(size_t)y * stride + x] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Loop-filter records per 8x8 (the MiInfo fields loopfilter.rs reads):
+// bits 0-5 level, 6-7 luma tx size, 8-9 chroma tx size, 10-13 block size,
+// 14 coded (intra, or not skipped).
+
+__global__ void k_lf_mi(KFrame k, int n_blocks) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_blocks) return;
+  const rv9_block& b = k.blocks[i];
+  int mode = b.y_mode;
+  int mode_type = (mode == 10 || mode == 11 || mode == 13) ? 1 : 0;  // NEARESTMV, NEARMV, NEWMV
+  int rf = b.ref_frame[0] > 0 ? b.ref_frame[0] : 0;
+  int level = k.lvl[b.segment_id][rf][mode_type];
+  int uv_tx;
+  if (b.mi_size < 3) {
+    uv_tx = 0;
+  } else {
+    // get_uv_tx_size with 4:2:0's subsampling for a pre-final profile 1 stream.
+    const uint8_t SS[13][2][2] = {{{0, 14}, {14, 14}}, {{1, 0}, {14, 14}}, {{2, 14}, {0, 14}}, {{3, 2}, {1, 0}},
+                                  {{4, 3}, {14, 1}},   {{5, 14}, {3, 2}},  {{6, 5}, {4, 3}},   {{7, 6}, {14, 4}},
+                                  {{8, 14}, {6, 5}},   {{9, 8}, {7, 6}},   {{10, 9}, {14, 7}}, {{11, 14}, {9, 8}},
+                                  {{12, 11}, {10, 9}}};
+    const uint8_t MAXTX[13] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3, 3};
+    int ux = k.legacy_uv ? 1 : k.ss_x, uy = k.legacy_uv ? 1 : k.ss_y;
+    int uv = SS[b.mi_size][ux][uy];
+    uv_tx = b.tx_size < MAXTX[uv] ? b.tx_size : MAXTX[uv];
+  }
+  bool coded = b.ref_frame[0] <= 0 || !(b.flags & RV9_BLK_SKIP);
+  uint32_t v = (uint32_t)level | ((uint32_t)b.tx_size << 6) | ((uint32_t)uv_tx << 8) | ((uint32_t)b.mi_size << 10) |
+               ((coded ? 1u : 0u) << 14);
+  const uint8_t N8W[13] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4, 4, 8, 8};
+  const uint8_t N8H[13] = {1, 1, 1, 1, 2, 1, 2, 4, 2, 4, 8, 4, 8};
+  int ye = min((int)b.mi_row + N8H[b.mi_size], k.mi_rows);
+  int xe = min((int)b.mi_col + N8W[b.mi_size], k.mi_cols);
+  for (int y = b.mi_row; y < ye; ++y)
+    for (int x = b.mi_col; x < xe; ++x) k.lf_mi[(size_t)y * k.mi_cols + x] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Intra cells: mark each intra transform block's 4x4 cells pending.
+
+__global__ void k_intra_mark(KFrame k) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k.n_intra) return;
+  const IntraItem it = k.intra[i];
+  int n = 1 << it.tx_size;  // cells per side
+  uint8_t* cells = k.cells[it.plane];
+  int cs = k.cell_stride[it.plane];
+  int cx = it.x >> 2, cy = it.y >> 2;
+  for (int y = 0; y < n; ++y)
+    for (int x = 0; x < n; ++x) cells[(size_t)(cy + y) * cs + cx + x] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Inter prediction.
+
+struct RefPos {
+  int start_x, start_y, step_x, step_y;
+};
+
+__device__ __forceinline__ int32_t q2(int32_t v) { return (v < 0 ? v - 1 : v + 1) / 2; }
+__device__ __forceinline__ int32_t q4(int32_t v) { return (v < 0 ? v - 2 : v + 2) / 4; }
+
+// Motion vector selection, clamping and scaling (reference
+// src/decoder/recon.rs:115-167, src/decoder/mod.rs:516-541).
+__device__ RefPos ref_position(const KFrame& k, const rv9_block& b, int ref_list, int plane, int x, int y,
+                               int block_idx) {
+  const int32_t(*bm)[2] = b.mv[ref_list];
+  int32_t mv0, mv1;
+  if (plane == 0 || b.mi_size >= 3) {
+    mv0 = bm[block_idx][0];
+    mv1 = bm[block_idx][1];
+  } else {
+    int usx = k.legacy_uv ? 1 : k.ss_x, usy = k.legacy_uv ? 1 : k.ss_y;
+    if (usx == 0 && usy == 0) {
+      mv0 = bm[block_idx][0];
+      mv1 = bm[block_idx][1];
+    } else if (usx == 0) {
+      mv0 = q2(bm[block_idx][0] + bm[block_idx + 2][0]);
+      mv1 = q2(bm[block_idx][1] + bm[block_idx + 2][1]);
+    } else if (usy == 0) {
+      mv0 = q2(bm[block_idx][0] + bm[block_idx + 1][0]);
+      mv1 = q2(bm[block_idx][1] + bm[block_idx + 1][1]);
+    } else {
+      mv0 = q4(bm[0][0] + bm[1][0] + bm[2][0] + bm[3][0]);
+      mv1 = q4(bm[0][1] + bm[1][1] + bm[2][1] + bm[3][1]);
+    }
+  }
+  const uint8_t N8W[13] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4, 4, 8, 8};
+  const uint8_t N8H[13] = {1, 1, 1, 1, 2, 1, 2, 4, 2, 4, 8, 4, 8};
+  int sx = plane ? k.ss_x : 0, sy = plane ? k.ss_y : 0;
+  int bh = N8H[b.mi_size], bw = N8W[b.mi_size];
+  int mi_row = b.mi_row, mi_col = b.mi_col;
+  int to_top = -((mi_row * 8) * 16) >> sy;
+  int to_bottom = (((k.mi_rows - bh - mi_row) * 8) * 16) >> sy;
+  int to_left = -((mi_col * 8) * 16) >> sx;
+  int to_right = (((k.mi_cols - bw - mi_col) * 8) * 16) >> sx;
+  int spel_left = (4 + ((bw * 8) >> sx)) << 4;
+  int spel_right = spel_left - 16;
+  int spel_top = (4 + ((bh * 8) >> sy)) << 4;
+  int spel_bottom = spel_top - 16;
+  int32_t c0 = clampi((2 * mv0) >> sy, to_top - spel_top, to_bottom + spel_bottom);
+  int32_t c1 = clampi((2 * mv1) >> sx, to_left - spel_left, to_right + spel_right);
+  int ri = b.ref_frame[ref_list] - 1;
+  int64_t xs = k.ref_xs[ri], ys = k.ref_ys[ri];
+  int64_t base_x = ((int64_t)x * xs) >> 14, base_y = ((int64_t)y * ys) >> 14;
+  int64_t luma_x = plane ? ((int64_t)x << k.ss_x) : x;
+  int64_t luma_y = plane ? ((int64_t)y << k.ss_y) : y;
+  int64_t frac_x = ((16 * luma_x * xs) >> 14) & 15;
+  int64_t frac_y = ((16 * luma_y * ys) >> 14) & 15;
+  int64_t dx = (((int64_t)c1 * xs) >> 14) + frac_x;
+  int64_t dy = (((int64_t)c0 * ys) >> 14) + frac_y;
+  RefPos p;
+  p.step_x = (int)((16 * xs) >> 14);
+  p.step_y = (int)((16 * ys) >> 14);
+  p.start_x = (int)((base_x << 4) + dx);
+  p.start_y = (int)((base_y << 4) + dy);
+  return p;
+}
+
+constexpr int kInterThreads = 128;
+constexpr int kInterTmpRows = 64 * 2 + 8;  // (h-1)*step/16 + 8 rows at steps up to 32
+
+// One prediction region per CTA: the horizontal pass over the clamped
+// reference rows into shared memory, then the vertical pass; for compound
+// blocks both predictions, then their rounded average (spec 8.5.2.3-8.5.2.5).
+template <class T>
+__global__ void __launch_bounds__(kInterThreads) k_inter(KFrame k) {
+  __shared__ uint16_t tmp[kInterTmpRows * 64];
+  __shared__ uint16_t pred[64 * 64];
+  const InterUnit u = k.units[blockIdx.x];
+  const rv9_block& b = k.blocks[u.block];
+  const int w = u.w4 * 4, h = u.h4 * 4, plane = u.plane;
+  const int maxv = (1 << k.bit_depth) - 1;
+  const bool compound = b.ref_frame[1] > 0;
+  T* dst = plane_ptr<T>(k.cur[plane]) + (size_t)u.y * k.cur[plane].stride + u.x;
+  const int dstride = k.cur[plane].stride;
+  const int filter = b.interp_filter;
+  for (int rl = 0; rl < (compound ? 2 : 1); ++rl) {
+    RefPos p = ref_position(k, b, rl, plane, u.x, u.y, u.block_idx);
+    const PlanePtr& rp = k.ref[b.ref_frame[rl] - 1][plane];
+    const T* ref = plane_ptr<const T>(rp);
+    const int last_x = rp.width - 1, last_y = rp.height - 1, rstride = rp.stride;
+    const int ih = (((h - 1) * p.step_y + 15) >> 4) + 8;
+    const int y0 = (p.start_y >> 4) - 3;
+    for (int i = threadIdx.x; i < ih * w; i += kInterThreads) {
+      int r = i / w, c = i - r * w;
+      int ry = clampi(y0 + r, 0, last_y);
+      const T* src = ref + (size_t)ry * rstride;
+      int pos = p.start_x + p.step_x * c;
+      int base = (pos >> 4) - 3;
+      const int16_t* f = c_filters[filter][pos & 15];
+      int32_t sum = 0;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)src[clampi(base + t, 0, last_x)];
+      tmp[r * 64 + c] = (uint16_t)clampi((sum + 64) >> 7, 0, maxv);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < h * w; i += kInterThreads) {
+      int r = i / w, c = i - r * w;
+      int pos = (p.start_y & 15) + p.step_y * r;
+      int base = pos >> 4;
+      const int16_t* f = c_filters[filter][pos & 15];
+      int32_t sum = 0;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)tmp[(base + t) * 64 + c];
+      int v = clampi((sum + 64) >> 7, 0, maxv);
+      if (!compound)
+        dst[(size_t)r * dstride + c] = (T)v;
+      else if (rl == 0)
+        pred[r * 64 + c] = (uint16_t)v;
+      else
+        dst[(size_t)r * dstride + c] = (T)((pred[r * 64 + c] + v + 1) >> 1);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Inverse transform + add, one warp per transform block.
+
+template <class V>
+struct Scratch {
+  typename V::store_t s[32 * 33];
+};
+
+// Dequantise the recorded coefficients of `t` into the warp's scratch (zeroed
+// first) and return the mask of rows holding a nonzero value (reference
+// src/decoder/recon.rs:242-264).
+template <class V>
+__device__ uint32_t load_coefs(const KFrame& k, const rv9_tok& t, int seg, typename V::store_t* s, int lane) {
+  const int n = 2 + t.tx_size, n0 = 1 << n, sp = n0 + 1;
+  for (int i = lane; i < n0 * sp; i += 32) s[i] = 0;
+  __syncwarp();
+  const int pt = t.plane ? 1 : 0;
+  const int64_t dcq = k.dc_q[seg][pt], acq = k.ac_q[seg][pt];
+  uint32_t rows = 0;
+  for (int i = lane; i < t.n_coef; i += 32) {
+    uint32_t w = k.coefs[t.coef_start + i];
+    int pos = RV9_COEF_POS(w);
+    int64_t v = RV9_COEF_VAL(w);
+    int64_t dq = v * (pos == 0 ? dcq : acq);
+    if (t.tx_size == 3) dq /= 2;
+    dq = dq < INT32_MIN ? INT32_MIN : (dq > INT32_MAX ? INT32_MAX : dq);
+    int r = pos >> n, c = pos & (n0 - 1);
+    s[r * sp + c] = (typename V::store_t)(int32_t)dq;
+    rows |= 1u << r;
+  }
+  rows = __reduce_or_sync(0xffffffffu, rows);
+  __syncwarp();
+  return rows;
+}
+
+// The 2D transform of the scratch block added to dst (reference
+// inverse_2d_add, src/dsp/itx.rs:519-570): rows by lanes, then columns.
+template <class V, int n, class T>
+__device__ void itx_add(typename V::store_t* s, uint32_t rows, int tx_type, bool lossless, T* dst, int dstride,
+                        int maxv, int lane) {
+  constexpr int n0 = 1 << n, sp = n0 + 1;
+  const int row_kind = lossless ? 2 : ((tx_type == 0 || tx_type == 1) ? 0 : 1);
+  const int col_kind = lossless ? 2 : ((tx_type == 0 || tx_type == 2) ? 0 : 1);
+  if (lane < n0 && ((rows >> lane) & 1)) {
+    V t[n0];
+#pragma unroll
+    for (int q = 0; q < n0; ++q) t[q] = V::load(s[lane * sp + q]);
+    tx1d<n>(t, row_kind, 2);
+#pragma unroll
+    for (int q = 0; q < n0; ++q) s[lane * sp + q] = t[q].v;
+  }
+  __syncwarp();
+  if (lane < n0) {
+    V t[n0];
+#pragma unroll
+    for (int i = 0; i < n0; ++i) t[i] = V::load(s[i * sp + lane]);
+    tx1d<n>(t, col_kind, 0);
+    constexpr int shift = (n + 2) < 6 ? (n + 2) : 6;
+#pragma unroll
+    for (int i = 0; i < n0; ++i) {
+      V r = lossless ? t[i] : t[i].rshift(shift);
+      T* px = dst + (size_t)i * dstride + lane;
+      *px = (T)clampi((int)*px + r.residual(), 0, maxv);
+    }
+  }
+  __syncwarp();
+}
+
+// A transform block's residual added to dst (the prediction), by one warp.
+template <class V, class T>
+__device__ void residual_add(const KFrame& k, const rv9_tok& t, int seg, T* dst, int dstride,
+                             typename V::store_t* s, int lane) {
+  const int maxv = (1 << k.bit_depth) - 1;
+  const int n = 2 + t.tx_size, n0 = 1 << n;
+  if (t.eob == 1 && t.tx_type == 0 && !k.lossless) {
+    // Only the DC coefficient: every sample gets the same residual (the
+    // reference's dc_only_value, src/dsp/itx.rs:684-694; exact for the
+    // 64-bit lane too, whose products here fit 32 bits).
+    int pt = t.plane ? 1 : 0;
+    int32_t dc = 0;
+    if (t.n_coef > 0) {
+      uint32_t w = k.coefs[t.coef_start];
+      int64_t dq = (int64_t)RV9_COEF_VAL(w) * k.dc_q[seg][pt];
+      if (t.tx_size == 3) dq /= 2;
+      dq = dq < INT32_MIN ? INT32_MIN : (dq > INT32_MAX ? INT32_MAX : dq);
+      dc = (int32_t)dq;
+    }
+    int shift = (n + 2) < 6 ? (n + 2) : 6;
+    V v = V::load(dc).mul(11585).rshift(14);
+    V w2 = V::load((int32_t)v.v).mul(11585).rshift(14);
+    // The 64-bit lane multiplies the low 32 bits: v fits them.
+    if (sizeof(typename V::store_t) == 4) w2 = v.mul(11585).rshift(14);
+    int res = w2.rshift(shift).residual();
+    for (int i = lane; i < n0 * n0; i += 32) {
+      int r = i >> n, c = i & (n0 - 1);
+      T* px = dst + (size_t)r * dstride + c;
+      *px = (T)clampi((int)*px + res, 0, maxv);
+    }
+    __syncwarp();
+    return;
+  }
+  uint32_t rows = load_coefs<V>(k, t, seg, s, lane);
+  switch (t.tx_size) {
+    case 0: itx_add<V, 2>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
+    case 1: itx_add<V, 3>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
+    case 2: itx_add<V, 4>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
+    default: itx_add<V, 5>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
+  }
+}
+
+constexpr int kResWarps = 4;
+
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kResWarps) k_inter_res(KFrame k) {
+  __shared__ Scratch<V> sc[kResWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kResWarps + warp;
+  if (i >= k.n_res) return;
+  const ResItem it = k.res[i];
+  const rv9_tok& t = k.toks[it.tok];
+  const rv9_block& b = k.blocks[it.block];
+  const PlanePtr& pp = k.cur[t.plane];
+  T* dst = plane_ptr<T>(pp) + (size_t)t.y * pp.stride + t.x;
+  residual_add<V, T>(k, t, b.segment_id, dst, pp.stride, sc[warp].s, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Intra wavefront.
+
+constexpr int kIntraWarps = 4;
+
+template <class V>
+struct IntraSmem {
+  typename V::store_t s[32 * 33];
+  int32_t pred[32 * 32];
+  int32_t above[66];
+  int32_t left[32];
+};
+
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  IntraSmem<V>* sm = reinterpret_cast<IntraSmem<V>*>(smem_raw) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const int maxv = (1 << k.bit_depth) - 1;
+  volatile int32_t* err = k.error;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(&k.counters[0], 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= k.n_intra) return;
+    const IntraItem it = k.intra[idx];
+    const int plane = it.plane, log2 = it.tx_size + 2, size = 1 << log2;
+    const int sx = plane ? k.ss_x : 0, sy = plane ? k.ss_y : 0;
+    const int max_x = ((k.mi_cols * 8) >> sx) - 1, max_y = ((k.mi_rows * 8) >> sy) - 1;
+    const bool have_left = it.flags & 1, have_above = it.flags & 2;
+    const bool not_on_right = it.flags & 4;
+    const int x = it.x, y = it.y;
+    // Wait for the cells the edges read: row y-1 and column x-1.
+    {
+      const uint8_t* cells = k.cells[plane];
+      const int cs = k.cell_stride[plane];
+      int ax1 = min(x + ((not_on_right && it.tx_size == 0) ? 2 * size : size) - 1, max_x);
+      int ax0 = have_left ? x - 1 : x;
+      int na = have_above ? ((ax1 >> 2) - (ax0 >> 2) + 1) : 0;
+      int ly1 = min(y + size - 1, max_y);
+      int nl = have_left ? ((ly1 >> 2) - (y >> 2) + 1) : 0;
+      const volatile uint8_t* cell = nullptr;
+      if (lane < na)
+        cell = cells + (size_t)((y - 1) >> 2) * cs + (ax0 >> 2) + lane;
+      else if (lane < na + nl)
+        cell = cells + (size_t)((y >> 2) + lane - na) * cs + ((x - 1) >> 2);
+      int polls = 0;
+      for (;;) {
+        bool pending = cell != nullptr && *cell != 0;
+        if (!__any_sync(0xffffffffu, pending)) break;
+        if (__any_sync(0xffffffffu, *err != 0)) return;
+        if (++polls > kWaitLimit) {
+          if (lane == 0) atomicCAS(k.error, 0, 1);
+          return;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    // Edges (reference src/decoder/recon.rs:42-89).
+    const T* buf = plane_ptr<const T>(k.cur[plane]);
+    const int stride = k.cur[plane].stride;
+    const int base = 1 << (k.bit_depth - 1);
+    if (have_above) {
+      const T* row = buf + (size_t)(y - 1) * stride;
+      for (int i = lane; i < 2 * size; i += 32) {
+        int v;
+        if (i < size || (not_on_right && it.tx_size == 0))
+          v = __ldcg(row + min(max_x, x + i));
+        else
+          v = __ldcg(row + min(max_x, x + size - 1));
+        sm->above[1 + i] = v;
+      }
+      if (lane == 0) sm->above[0] = have_left ? (int)__ldcg(row + min(max_x, x - 1)) : base + 1;
+    } else {
+      for (int i = lane; i <= 2 * size; i += 32) sm->above[i] = base - 1;
+    }
+    for (int i = lane; i < size; i += 32)
+      sm->left[i] = have_left ? (int)__ldcg(buf + (size_t)min(max_y, y + i) * stride + x - 1) : base + 1;
+    __syncwarp();
+    int32_t dc = 0;
+    if (it.mode == 0) {
+      int32_t sa = 0, sl = 0;
+      for (int i = lane; i < size; i += 32) {
+        sa += sm->above[1 + i];
+        sl += sm->left[i];
+      }
+      sa = __reduce_add_sync(0xffffffffu, sa);
+      sl = __reduce_add_sync(0xffffffffu, sl);
+      dc = intra_dc(log2, sa, sl, have_left, have_above, k.bit_depth);
+    }
+    for (int i = lane; i < size * size; i += 32) {
+      int r = i >> log2, c = i & (size - 1);
+      sm->pred[i] = intra_pixel(it.mode, r, c, size, sm->above, sm->left, dc, maxv);
+    }
+    __syncwarp();
+    if (it.tok != NO_TOK) {
+      const rv9_tok& t = k.toks[it.tok];
+      residual_add<V, int32_t>(k, t, k.blocks[it.block].segment_id, sm->pred, size, sm->s, lane);
+    }
+    T* dst = plane_ptr<T>(k.cur[plane]) + (size_t)y * stride + x;
+    for (int i = lane; i < size * size; i += 32) {
+      int r = i >> log2, c = i & (size - 1);
+      dst[(size_t)r * stride + c] = (T)sm->pred[i];
+    }
+    __threadfence();
+    __syncwarp();
+    {
+      uint8_t* cells = k.cells[plane];
+      const int cs = k.cell_stride[plane];
+      int nc = size >> 2;
+      for (int i = lane; i < nc * nc; i += 32) {
+        int cy = i / nc, cx = i - cy * nc;
+        ((volatile uint8_t*)cells)[(size_t)((y >> 2) + cy) * cs + (x >> 2) + cx] = 0;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Loop filter wavefront.
+
+constexpr int kLfThreads = 192;
+constexpr int kLfW = 80;   // smem row pitch: 8 left + 64 + 8 of slack
+constexpr int kLfH = 72;   // 8 above + 64
+
+struct LfEdge {
+  int8_t fs;
+  uint8_t limit, blimit, thresh;
+};
+
+// The filtering of one (edge, run) of one pass of one plane of a superblock
+// (reference superblock(), src/decoder/loopfilter.rs:466-620, one entry).
+__device__ LfEdge lf_entry(const KFrame& k, int plane, int pass, int row, int col, int ed, int rn) {
+  LfEdge e{-1, 0, 0, 0};
+  const int sub_x = plane ? k.ss_x : 0, sub_y = plane ? k.ss_y : 0;
+  const int sub = pass == 0 ? sub_x : sub_y;
+  auto at = [&](int e_, int r_, int* x, int* y) {
+    if (pass == 0) {
+      *x = col * 8 + e_ * (4 << sub_x);
+      *y = row * 8 + ((4 * r_) << sub_y);
+    } else {
+      *x = col * 8 + ((4 * r_) << sub_x);
+      *y = row * 8 + e_ * (4 << sub_y);
+    }
+  };
+  int ca = ed >> 1, cb = rn >> 1;
+  int x, y;
+  at(2 * ca, 2 * cb, &x, &y);
+  if (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows) return e;
+  int loop_col = ((x >> 3) >> sub_x) << sub_x;
+  int loop_row = ((y >> 3) >> sub_y) << sub_y;
+  uint32_t m = k.lf_mi[(size_t)loop_row * k.mi_cols + loop_col];
+  int l = m & 63;
+  if (l == 0) return e;
+  int tx_sz = plane ? ((m >> 8) & 3) : ((m >> 6) & 3);
+  int mi_size = (m >> 10) & 15;
+  bool coded = (m >> 14) & 1;
+  const uint8_t N8W[13] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4, 4, 8, 8};
+  const uint8_t N8H[13] = {1, 1, 1, 1, 2, 1, 2, 4, 2, 4, 8, 4, 8};
+  int sb_size = sub == 0 ? mi_size : (mi_size > 6 ? mi_size : 6);
+  int block_mask = pass == 0 ? 8 * N8W[sb_size] - 1 : 8 * N8H[sb_size] - 1;
+  at(ed, 2 * cb, &x, &y);
+  if ((pass == 0 && x == 0) || (pass == 1 && y == 0)) return e;
+  int across = pass == 0 ? x : y;
+  bool is_block_edge = (across & block_mask) == 0;
+  bool tx_edge = (ed & ((1 << tx_sz) - 1)) == 0;
+  if (!is_block_edge && !(tx_edge && coded)) return e;
+  bool is_32_edge = ed % 8 == 0;
+  int base_size = (tx_sz == 0 && is_32_edge) ? 1 : (tx_sz < 2 ? tx_sz : 2);
+  int filter_size = base_size;
+  if ((pass == 0 && sub_x == 1 && base_size == 2 && (x >> 3) == k.mi_cols - 1) ||
+      (pass == 1 && sub_y == 1 && base_size == 2 && (y >> 3) == k.mi_rows - 1))
+    filter_size = 1;
+  at(ed, rn, &x, &y);
+  if ((rn & 1) && (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows)) return e;
+  bool is_tx_edge = tx_edge;
+  if (pass == 1 && sub_x == 1 && (k.mi_cols & 1) && (ed & 1) && (x + 8) >= k.mi_cols * 8) is_tx_edge = false;
+  if (!(is_block_edge || (is_tx_edge && coded))) return e;
+  e.fs = (int8_t)filter_size;
+  e.limit = k.lf_limit[l];
+  e.blimit = k.lf_blimit[l];
+  e.thresh = k.lf_thresh[l];
+  return e;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
+  __shared__ int16_t px[3][kLfH][kLfW];
+  __shared__ LfEdge edges[3][2][16][16];
+  __shared__ int ticket;
+  __shared__ int abort_flag;
+  const int n_sb = k.sb64_cols * k.sb64_rows;
+  for (;;) {
+    if (threadIdx.x == 0) ticket = atomicAdd(&k.counters[1], 1);
+    __syncthreads();
+    const int t = ticket;
+    __syncthreads();
+    if (t >= n_sb) return;
+    const int sr = t / k.sb64_cols, sc = t - sr * k.sb64_cols;
+    const int row = sr * 8, col = sc * 8;
+    // Edge decisions (independent of samples): before waiting.
+    for (int i = threadIdx.x; i < 3 * 2 * 256; i += kLfThreads) {
+      int plane = i / 512, pass = (i >> 8) & 1, ed = (i >> 4) & 15, rn = i & 15;
+      edges[plane][pass][ed][rn] = lf_entry(k, plane, pass, row, col, ed, rn);
+    }
+    // Wait for (r, c-1) and (r-1, c+1) (or (r-1, c) at the last column).
+    if (threadIdx.x == 0) {
+      abort_flag = 0;
+      const volatile uint32_t* done = k.sb_done;
+      int polls = 0;
+      int deps[2] = {sc > 0 ? t - 1 : -1, sr > 0 ? (t - k.sb64_cols + (sc + 1 < k.sb64_cols ? 1 : 0)) : -1};
+      for (int d = 0; d < 2 && !abort_flag; ++d) {
+        if (deps[d] < 0) continue;
+        while (done[deps[d]] != k.epoch) {
+          if (*(volatile int32_t*)k.error || ++polls > kWaitLimit) {
+            atomicCAS(k.error, 0, 2);
+            abort_flag = 1;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (abort_flag) return;
+    // Load the region: rows y0-8 .. y0+63, columns x0-8 .. x0+63 per plane.
+    int rows_p[3], cols_p[3], x0s[3], y0s[3];
+    for (int p = 0; p < 3; ++p) {
+      int sxp = p ? k.ss_x : 0, syp = p ? k.ss_y : 0;
+      rows_p[p] = 64 >> syp;
+      cols_p[p] = 64 >> sxp;
+      x0s[p] = (col * 8) >> sxp;
+      y0s[p] = (row * 8) >> syp;
+    }
+    for (int p = 0; p < 3; ++p) {
+      const T* src = plane_ptr<const T>(k.cur[p]);
+      const int stride = k.cur[p].stride;
+      const int nr = rows_p[p] + 8, nc = cols_p[p] + 8;
+      for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
+        int r = i / nc, c = i - r * nc;
+        int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + c;
+        if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) px[p][r][c] = (int16_t)__ldcg(src + (size_t)gy * stride + gx);
+      }
+    }
+    __syncthreads();
+    const int bd = k.bit_depth;
+    // Vertical edges, left to right, one thread per sample row.
+    {
+      const int total = rows_p[0] + rows_p[1] + rows_p[2];
+      for (int task = threadIdx.x; task < total; task += kLfThreads) {
+        int p = task < rows_p[0] ? 0 : (task < rows_p[0] + rows_p[1] ? 1 : 2);
+        int r = task - (p == 0 ? 0 : (p == 1 ? rows_p[0] : rows_p[0] + rows_p[1]));
+        int n_edges = 16 >> (p ? k.ss_x : 0);
+        int16_t* line = &px[p][8 + r][0];
+        for (int ed = 0; ed < n_edges; ++ed) {
+          LfEdge e = edges[p][0][ed][r >> 2];
+          if (e.fs < 0) continue;
+          int s[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) s[q] = line[4 * ed + q];
+          lf_line(s, e.fs, e.limit, e.blimit, e.thresh, bd);
+#pragma unroll
+          for (int q = 1; q < 15; ++q) line[4 * ed + q] = (int16_t)s[q];
+        }
+      }
+    }
+    __syncthreads();
+    // Horizontal edges, top to bottom, one thread per sample column.
+    {
+      const int total = cols_p[0] + cols_p[1] + cols_p[2];
+      for (int task = threadIdx.x; task < total; task += kLfThreads) {
+        int p = task < cols_p[0] ? 0 : (task < cols_p[0] + cols_p[1] ? 1 : 2);
+        int c = task - (p == 0 ? 0 : (p == 1 ? cols_p[0] : cols_p[0] + cols_p[1]));
+        int n_edges = 16 >> (p ? k.ss_y : 0);
+        for (int ed = 0; ed < n_edges; ++ed) {
+          LfEdge e = edges[p][1][ed][c >> 2];
+          if (e.fs < 0) continue;
+          int s[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < kLfH) ? px[p][4 * ed + q][8 + c] : 0;
+          lf_line(s, e.fs, e.limit, e.blimit, e.thresh, bd);
+#pragma unroll
+          for (int q = 1; q < 15; ++q)
+            if (4 * ed + q < kLfH) px[p][4 * ed + q][8 + c] = (int16_t)s[q];
+        }
+      }
+    }
+    __syncthreads();
+    for (int p = 0; p < 3; ++p) {
+      T* dst = plane_ptr<T>(k.cur[p]);
+      const int stride = k.cur[p].stride;
+      const int nr = rows_p[p] + 8, nc = cols_p[p] + 8;
+      for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
+        int r = i / nc, c = i - r * nc;
+        int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + c;
+        if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) __stcg(dst + (size_t)gy * stride + gx, (T)px[p][r][c]);
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) *(volatile uint32_t*)&k.sb_done[t] = k.epoch;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch of one frame's chain.
+
+struct LaunchCounts {
+  int n_blocks;
+};
+
+cudaError_t upload_filters(const int16_t* f) { return cudaMemcpyToSymbol(c_filters, f, sizeof(int16_t) * 4 * 16 * 8); }
+
+template <class T, class V>
+static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches) {
+  int L = 0;
+  {
+    int aw = k.sb64_cols * 64, ah = k.sb64_rows * 64;
+    if (k.mi_cols * 8 < aw || k.mi_rows * 8 < ah) {
+      k_zero_pad<T><<<dim3(64, 3), 256, 0, s>>>(k);
+      ++L;
+    }
+  }
+  if (k.lf_on && n_blocks > 0) {
+    k_lf_mi<<<(n_blocks + 127) / 128, 128, 0, s>>>(k, n_blocks);
+    ++L;
+  }
+  if (k.n_intra > 0) {
+    k_intra_mark<<<(k.n_intra + 127) / 128, 128, 0, s>>>(k);
+    ++L;
+  }
+  if (k.n_units > 0) {
+    k_inter<T><<<k.n_units, kInterThreads, 0, s>>>(k);
+    ++L;
+  }
+  if (k.n_res > 0) {
+    k_inter_res<T, V><<<(k.n_res + kResWarps - 1) / kResWarps, 32 * kResWarps, 0, s>>>(k);
+    ++L;
+  }
+  if (k.n_intra > 0) {
+    size_t smem = sizeof(IntraSmem<V>) * kIntraWarps;
+    static bool attr_set = false;
+    if (!attr_set) {
+      cudaFuncSetAttribute(k_intra<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr_set = true;
+    }
+    int want = (k.n_intra + kIntraWarps - 1) / kIntraWarps;
+    int grid = want < n_sm * 4 ? want : n_sm * 4;
+    k_intra<T, V><<<grid, 32 * kIntraWarps, smem, s>>>(k);
+    ++L;
+  }
+  if (k.lf_on) {
+    int n_sb = k.sb64_cols * k.sb64_rows;
+    int grid = n_sb < n_sm * 4 ? n_sb : n_sm * 4;
+    k_lf<T><<<grid, kLfThreads, 0, s>>>(k);
+    ++L;
+  }
+  *launches += L;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches) {
+  if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches);
+  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches);
+}
+
+}  // namespace rv9g

@@ -1,0 +1,213 @@
+"""Python binding of the B200 VP9 decoder (ctypes over librv9.so).
+
+Mirrors the reference crate's decoder API (rivet-vp9 src/decoder/mod.rs:150-216
+and src/frame.rs:115-229):
+
+    dec = rv9.Decoder()
+    for packet in packets:
+        frame = dec.decode(packet)        # the last frame the packet shows, or None
+        frames = dec.decode_all(packet)   # every frame it shows
+
+Errors are raised as the reference's error kinds: BitstreamError,
+UnsupportedError, InvalidInputError; device failures as DeviceError.
+The library runs reconstruction on the GPU only: importing works anywhere,
+but Decoder() raises DeviceError when librv9.so or a usable CUDA device is
+missing.
+"""
+import ctypes
+import os
+
+from . import containers  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "_build", "librv9.so")
+
+RV9_OK, RV9_BITSTREAM, RV9_UNSUPPORTED, RV9_INVALID_INPUT, RV9_DEVICE = range(5)
+CHROMA_NAMES = {0: "Yuv420", 1: "Yuv422", 2: "Yuv440", 3: "Yuv444"}
+
+
+class Rv9Error(Exception):
+    pass
+
+
+class BitstreamError(Rv9Error):
+    pass
+
+
+class UnsupportedError(Rv9Error):
+    pass
+
+
+class InvalidInputError(Rv9Error):
+    pass
+
+
+class DeviceError(Rv9Error):
+    pass
+
+
+_ERRORS = {RV9_BITSTREAM: BitstreamError, RV9_UNSUPPORTED: UnsupportedError,
+           RV9_INVALID_INPUT: InvalidInputError, RV9_DEVICE: DeviceError}
+
+
+class CPlane(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_size_t), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32)]
+
+
+class CFrame(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("bit_depth", ctypes.c_uint32),
+                ("chroma", ctypes.c_uint32), ("color_space", ctypes.c_uint32), ("full_range", ctypes.c_uint32),
+                ("render_width", ctypes.c_uint32), ("render_height", ctypes.c_uint32),
+                ("data", ctypes.POINTER(ctypes.c_uint8)), ("size", ctypes.c_size_t), ("planes", CPlane * 3)]
+
+
+class CStats(ctypes.Structure):
+    _fields_ = [("device_ms", ctypes.c_double), ("parse_ms", ctypes.c_double), ("frames", ctypes.c_uint64),
+                ("algorithmic_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64)]
+
+
+# Every symbol include/rv9.h declares.
+EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv9_decoder_set_max_pixels",
+           "rv9_decoder_frames_decoded", "rv9_last_error", "rv9_last_global_error", "rv9_decode_all",
+           "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats")
+
+_lib = None
+
+
+def load_library(path=None):
+    """Loads librv9.so (the CUDA build); raises DeviceError if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise DeviceError(f"{p} is not built: run rivet-vp9_b200/build.py (the decoder has no CPU path)")
+    lib = ctypes.CDLL(p)
+    vp = ctypes.c_void_p
+    lib.rv9_decoder_new.restype = vp
+    lib.rv9_decoder_new.argtypes = [ctypes.c_int]
+    lib.rv9_decoder_free.argtypes = [vp]
+    lib.rv9_decoder_set_threads.argtypes = [vp, ctypes.c_uint32]
+    lib.rv9_decoder_set_max_pixels.argtypes = [vp, ctypes.c_uint64]
+    lib.rv9_decoder_frames_decoded.restype = ctypes.c_uint64
+    lib.rv9_decoder_frames_decoded.argtypes = [vp]
+    lib.rv9_last_error.restype = ctypes.c_char_p
+    lib.rv9_last_error.argtypes = [vp]
+    lib.rv9_last_global_error.restype = ctypes.c_char_p
+    lib.rv9_decode_all.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(CFrame), ctypes.c_size_t,
+                                   ctypes.POINTER(ctypes.c_size_t)]
+    lib.rv9_decode.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(CFrame),
+                               ctypes.POINTER(ctypes.c_int)]
+    lib.rv9_frame_release.argtypes = [ctypes.POINTER(CFrame)]
+    lib.rv9_decode_packets.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.c_size_t, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.POINTER(ctypes.c_size_t)]
+    lib.rv9_decoder_stats.argtypes = [vp, ctypes.POINTER(CStats), ctypes.c_int]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class Plane:
+    __slots__ = ("offset", "width", "height")
+
+    def __init__(self, offset, width, height):
+        self.offset, self.width, self.height = offset, width, height
+
+
+class Frame:
+    """A decoded frame in the reference's layout: Y, U, V packed (stride ==
+    width), one byte per sample at 8 bits, little-endian uint16 above."""
+
+    def __init__(self, c: CFrame):
+        self.width, self.height, self.bit_depth = c.width, c.height, c.bit_depth
+        self.chroma = CHROMA_NAMES.get(c.chroma, str(c.chroma))
+        self.color_space, self.full_range = c.color_space, bool(c.full_range)
+        self.render_width, self.render_height = c.render_width, c.render_height
+        self.data = ctypes.string_at(c.data, c.size) if c.size else b""
+        self.planes = [Plane(p.offset, p.width, p.height) for p in c.planes]
+
+    def bytes_per_sample(self):
+        return 2 if self.bit_depth > 8 else 1
+
+    def plane(self, i):
+        p = self.planes[i]
+        n = p.width * p.height * self.bytes_per_sample()
+        return self.data[p.offset:p.offset + n]
+
+    def packed(self):
+        return self.data
+
+
+def _raise(lib, dec, st):
+    msg = lib.rv9_last_error(dec).decode(errors="replace") if dec else ""
+    raise _ERRORS.get(st, Rv9Error)(msg or f"status {st}")
+
+
+class Decoder:
+    """A VP9 decoder whose reconstruction runs on CUDA device `device`."""
+
+    def __init__(self, device=-1, lib_path=None):
+        self._lib = load_library(lib_path)
+        self._dec = self._lib.rv9_decoder_new(device)
+        if not self._dec:
+            raise DeviceError(self._lib.rv9_last_global_error().decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "_dec", None):
+            self._lib.rv9_decoder_free(self._dec)
+            self._dec = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_threads(self, n):
+        self._lib.rv9_decoder_set_threads(self._dec, n)
+
+    def set_max_pixels(self, n):
+        self._lib.rv9_decoder_set_max_pixels(self._dec, n)
+
+    def frames_decoded(self):
+        return self._lib.rv9_decoder_frames_decoded(self._dec)
+
+    def decode_all(self, packet: bytes):
+        cap = 16
+        frames = (CFrame * cap)()
+        n = ctypes.c_size_t()
+        st = self._lib.rv9_decode_all(self._dec, packet, len(packet), frames, cap, ctypes.byref(n))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        out = []
+        for i in range(min(n.value, cap)):
+            out.append(Frame(frames[i]))
+            self._lib.rv9_frame_release(ctypes.byref(frames[i]))
+        return out
+
+    def decode(self, packet: bytes):
+        frames = self.decode_all(packet)
+        return frames[-1] if frames else None
+
+    def decode_packets(self, packets, out_buffer, out_ptr=None):
+        """Decodes a sequence of packets with parsing overlapped with the
+        device work; shown frames are written packed into `out_buffer` (a
+        writable buffer, e.g. pinned memory). Returns (frames, bytes)."""
+        n = len(packets)
+        arr = (ctypes.c_char_p * n)(*packets)
+        lens = (ctypes.c_size_t * n)(*[len(p) for p in packets])
+        nf, nb = ctypes.c_size_t(), ctypes.c_size_t()
+        if out_ptr is None:
+            out_ptr = ctypes.addressof((ctypes.c_char * len(out_buffer)).from_buffer(out_buffer))
+        st = self._lib.rv9_decode_packets(self._dec, arr, lens, n, out_ptr, len(out_buffer),
+                                          ctypes.byref(nf), ctypes.byref(nb))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        return nf.value, nb.value
+
+    def stats(self, reset=False):
+        s = CStats()
+        self._lib.rv9_decoder_stats(self._dec, ctypes.byref(s), 1 if reset else 0)
+        return {"device_ms": s.device_ms, "parse_ms": s.parse_ms, "frames": s.frames,
+                "algorithmic_bytes": s.algorithmic_bytes, "kernel_launches": s.kernel_launches}
