@@ -1154,3 +1154,30 @@ void rv9o_test_lf(uint16_t* buf, int filter_size, int limit, int blimit, int thr
 }
 
 }  // extern "C"
+
+// The oracle's loop filter over SB-aligned u16 planes, with the mode info of
+// the given blocks.
+extern "C" void rv9o_test_lf_frame(const rv9_frame_desc* d, const rv9_block* blocks, int n_blocks, uint16_t* y,
+                                   uint16_t* u, uint16_t* v) {
+  oracle::Picture pic;
+  int w = d->sb64_cols * 64, h = d->sb64_rows * 64;
+  uint16_t* src[3] = {y, u, v};
+  for (int p = 0; p < 3; ++p) {
+    int pw = p ? w >> d->ss_x : w, ph = p ? h >> d->ss_y : h;
+    pic.planes[p].data.assign(src[p], src[p] + (size_t)pw * ph);
+    pic.planes[p].stride = pw;
+    pic.planes[p].height = ph;
+  }
+  oracle::FrameRecon fr(*d, pic);
+  std::vector<oracle::MiLf> mi((size_t)d->mi_rows * d->mi_cols);
+  for (int i = 0; i < n_blocks; ++i) {
+    const rv9_block& b = blocks[i];
+    oracle::MiLf m{b.mi_size, (uint8_t)((b.flags & RV9_BLK_SKIP) ? 1 : 0), b.tx_size, b.y_mode, b.segment_id,
+                   b.ref_frame[0]};
+    uint32_t bh = vp9t_num_8x8_high[b.mi_size], bw = vp9t_num_8x8_wide[b.mi_size];
+    for (uint32_t yy = b.mi_row; yy < std::min(b.mi_row + bh, d->mi_rows); ++yy)
+      for (uint32_t xx = b.mi_col; xx < std::min(b.mi_col + bw, d->mi_cols); ++xx) mi[(size_t)yy * d->mi_cols + xx] = m;
+  }
+  fr.filter_frame(mi);
+  for (int p = 0; p < 3; ++p) std::copy(pic.planes[p].data.begin(), pic.planes[p].data.end(), src[p]);
+}

@@ -396,6 +396,27 @@ RV9_HD int32_t intra_dc(int log2, int32_t sum_above, int32_t sum_left, bool have
 RV9_HD int iabs(int v) { return v < 0 ? -v : v; }
 RV9_HD int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// The wide filter (spec 8.8.5.3): a rounded sliding mean over 2^log2 taps of
+// the samples at -(n+1) .. n (n = 2^(log2-1) - 1), replacing -n .. n-1. All
+// indices are compile-time constants so the line stays in registers.
+template <int LOG2>
+RV9_HD void lf_wide(int* s) {
+  constexpr int n = (1 << (LOG2 - 1)) - 1;
+  int f[16];
+#pragma unroll
+  for (int i = -n; i < n; ++i) {
+    int t = s[i + 8];
+#pragma unroll
+    for (int j = -n; j <= n; ++j) {
+      const int p = (i + j) < -(n + 1) ? -(n + 1) : ((i + j) > n ? n : (i + j));
+      t += s[p + 8];
+    }
+    f[i + 8] = (t + (1 << (LOG2 - 1))) >> LOG2;
+  }
+#pragma unroll
+  for (int i = -n; i < n; ++i) s[i + 8] = f[i + 8];
+}
+
 RV9_HD void lf_line(int* s, int filter_size, int limit, int blimit, int thresh, int bd) {
   int q0 = s[8], q1 = s[9], q2 = s[10], q3 = s[11];
   int p0 = s[7], p1 = s[6], p2 = s[5], p3 = s[4];
@@ -427,27 +448,159 @@ RV9_HD void lf_line(int* s, int filter_size, int limit, int blimit, int thresh, 
     }
     return;
   }
-  bool flat2 = false;
-  if (filter_size >= 2) {
-    flat2 = true;
+  bool flat2 = filter_size >= 2;
 #pragma unroll
-    for (int k = 4; k < 8; ++k)
-      if (iabs(s[8 - k - 1] - p0) > one || iabs(s[8 + k] - q0) > one) flat2 = false;
+  for (int k = 4; k < 8; ++k)
+    if (iabs(s[8 - k - 1] - p0) > one || iabs(s[8 + k] - q0) > one) flat2 = false;
+  if (filter_size == 1 || !flat2)
+    lf_wide<3>(s);
+  else
+    lf_wide<4>(s);
+}
+
+// ---------------------------------------------------------------------------
+// Loop filter edge decisions (reference superblock(),
+// src/decoder/loopfilter.rs:466-620), one (edge, run) entry at a time.
+
+// Per 8x8 loop-filter record: bits 0-5 level, 6-7 luma tx size, 8-9 chroma tx
+// size, 10-13 block size, 14 coded (intra, or not skipped).
+RV9_HD uint32_t lf_pack(int level, int tx_y, int tx_uv, int mi_size, bool coded) {
+  return (uint32_t)level | ((uint32_t)tx_y << 6) | ((uint32_t)tx_uv << 8) | ((uint32_t)mi_size << 10) |
+         ((coded ? 1u : 0u) << 14);
+}
+
+struct LfParams {
+  int mi_cols, mi_rows, ss_x, ss_y;
+  const uint32_t* lf_mi;
+  const uint8_t* limit;   // [64] by level
+  const uint8_t* blimit;
+  const uint8_t* thresh;
+};
+
+struct LfEdge {
+  int8_t fs;
+  uint8_t limit, blimit, thresh;
+};
+
+RV9_HD void lf_at(int pass, int sub_x, int sub_y, int row, int col, int e, int r, int* x, int* y) {
+  if (pass == 0) {
+    *x = col * 8 + e * (4 << sub_x);
+    *y = row * 8 + ((4 * r) << sub_y);
+  } else {
+    *x = col * 8 + ((4 * r) << sub_x);
+    *y = row * 8 + e * (4 << sub_y);
   }
-  // Wide filter (spec 8.8.5.3): a rounded sliding mean over 8 or 16 taps.
-  int log2 = (filter_size == 1 || !flat2) ? 3 : 4;
-  int n = (1 << (log2 - 1)) - 1;
-  int f[16];
-  for (int i = -n; i < n; ++i) {
-    int t = s[i + 8];
-    for (int j = -n; j <= n; ++j) {
-      int p = i + j;
-      p = p < -(n + 1) ? -(n + 1) : (p > n ? n : p);
-      t += s[p + 8];
-    }
-    f[i + 8] = (t + (1 << (log2 - 1))) >> log2;
+}
+
+// The filter of edge `ed`, run `rn` of pass `pass` (0 vertical, 1 horizontal)
+// of plane `plane` in the superblock at mode-info (row, col).
+RV9_HD LfEdge lf_edge_entry(const LfParams& k, int plane, int pass, int row, int col, int ed, int rn) {
+  LfEdge e{-1, 0, 0, 0};
+  const int sub_x = plane ? k.ss_x : 0, sub_y = plane ? k.ss_y : 0;
+  const int sub = pass == 0 ? sub_x : sub_y;
+  int ca = ed >> 1, cb = rn >> 1;
+  int x, y;
+  lf_at(pass, sub_x, sub_y, row, col, 2 * ca, 2 * cb, &x, &y);
+  if (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows) return e;
+  int loop_col = ((x >> 3) >> sub_x) << sub_x;
+  int loop_row = ((y >> 3) >> sub_y) << sub_y;
+  uint32_t m = k.lf_mi[(size_t)loop_row * k.mi_cols + loop_col];
+  int l = m & 63;
+  if (l == 0) return e;
+  int tx_sz = plane ? ((m >> 8) & 3) : ((m >> 6) & 3);
+  int mi_size = (m >> 10) & 15;
+  bool coded = (m >> 14) & 1;
+  // num_8x8 wide / high by block size, as 2-bit fields of a constant.
+  int w8 = 1 << ((0x3ea5400u >> (2 * mi_size)) & 3);
+  int h8 = 1 << ((0x3b99100u >> (2 * mi_size)) & 3);
+  int sb_size = sub == 0 ? mi_size : (mi_size > 6 ? mi_size : 6);
+  if (sb_size != mi_size) {
+    w8 = 1 << ((0x3ea5400u >> (2 * sb_size)) & 3);
+    h8 = 1 << ((0x3b99100u >> (2 * sb_size)) & 3);
   }
-  for (int i = -n; i < n; ++i) s[i + 8] = f[i + 8];
+  int block_mask = pass == 0 ? 8 * w8 - 1 : 8 * h8 - 1;
+  lf_at(pass, sub_x, sub_y, row, col, ed, 2 * cb, &x, &y);
+  if ((pass == 0 && x == 0) || (pass == 1 && y == 0)) return e;
+  int across = pass == 0 ? x : y;
+  bool is_block_edge = (across & block_mask) == 0;
+  bool tx_edge = (ed & ((1 << tx_sz) - 1)) == 0;
+  if (!is_block_edge && !(tx_edge && coded)) return e;
+  bool is_32_edge = ed % 8 == 0;
+  int base_size = (tx_sz == 0 && is_32_edge) ? 1 : (tx_sz < 2 ? tx_sz : 2);
+  int filter_size = base_size;
+  if ((pass == 0 && sub_x == 1 && base_size == 2 && (x >> 3) == k.mi_cols - 1) ||
+      (pass == 1 && sub_y == 1 && base_size == 2 && (y >> 3) == k.mi_rows - 1))
+    filter_size = 1;
+  lf_at(pass, sub_x, sub_y, row, col, ed, rn, &x, &y);
+  if ((rn & 1) && (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows)) return e;
+  bool is_tx_edge = tx_edge;
+  if (pass == 1 && sub_x == 1 && (k.mi_cols & 1) && (ed & 1) && (x + 8) >= k.mi_cols * 8) is_tx_edge = false;
+  if (!(is_block_edge || (is_tx_edge && coded))) return e;
+  e.fs = (int8_t)filter_size;
+  e.limit = k.limit[l];
+  e.blimit = k.blimit[l];
+  e.thresh = k.thresh[l];
+  return e;
+}
+
+// The loop-filter record of a block (the MiInfo fields the filter reads).
+// `lvl` is LvlLookup[segment][ref][mode type] (8.8.1).
+RV9_HD uint32_t lf_block_record(int mi_size, int tx_size, int flags, int segment_id, int y_mode, int ref0,
+                                const uint8_t (*lvl)[4][2], int legacy_uv, int ss_x, int ss_y) {
+  int mode_type = (y_mode == 10 || y_mode == 11 || y_mode == 13) ? 1 : 0;  // NEARESTMV, NEARMV, NEWMV
+  int rf = ref0 > 0 ? ref0 : 0;
+  int level = lvl[segment_id][rf][mode_type];
+  int uv_tx = 0;
+  if (mi_size >= 3) {
+    // get_uv_tx_size: the chroma block's largest transform, with 4:2:0's
+    // subsampling for a pre-final profile 1 stream.
+    int ux = legacy_uv ? 1 : ss_x, uy = legacy_uv ? 1 : ss_y;
+    // Chroma block width / height log2 in 4-sample units.
+    int bw = ((0x3ea5400u >> (2 * mi_size)) & 3) + 1 - ux;  // log2(8x8 units) + 1 = log2(4x4 units)
+    int bh = ((0x3b99100u >> (2 * mi_size)) & 3) + 1 - uy;
+    int m = bw < bh ? bw : bh;  // largest square transform inside: log2 in 4-sample units
+    if (m > 3) m = 3;
+    uv_tx = tx_size < m ? tx_size : m;
+  }
+  bool coded = ref0 <= 0 || !(flags & 1);
+  return lf_pack(level, tx_size, uv_tx, mi_size, coded);
+}
+
+// Vertical edges of one sample row of a superblock, left to right. `line`
+// holds the row from 8 samples left of the superblock; `e` the plane's
+// vertical-pass entries [edge][run].
+RV9_HD void lf_vertical_row(int16_t* line, const LfEdge (*e)[16], int n_edges, int run, int bd) {
+  for (int ed = 0; ed < n_edges; ++ed) {
+    LfEdge f = e[ed][run];
+    if (f.fs < 0) continue;
+    int16_t* w = line + 4 * ed;
+    int s[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) s[q] = w[q];
+    lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+#pragma unroll
+    for (int q = 1; q < 15; ++q) w[q] = (int16_t)s[q];
+  }
+}
+
+// Horizontal edges of one sample column, top to bottom. `col` points at the
+// column's sample 8 rows above the superblock; `pitch` is the row pitch;
+// `rows` the rows available from there.
+RV9_HD void lf_horizontal_col(int16_t* col, int pitch, int rows, const LfEdge (*e)[16], int n_edges, int run,
+                              int bd) {
+  for (int ed = 0; ed < n_edges; ++ed) {
+    LfEdge f = e[ed][run];
+    if (f.fs < 0) continue;
+    int16_t* w = col + 4 * ed * pitch;
+    const int avail = rows - 4 * ed;
+    int s[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) s[q] = q < avail ? w[q * pitch] : 0;
+    lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+#pragma unroll
+    for (int q = 1; q < 15; ++q)
+      if (q < avail) w[q * pitch] = (int16_t)s[q];
+  }
 }
 
 }  // namespace rv9g

@@ -79,31 +79,11 @@ __global__ void k_lf_mi(KFrame k, int n_blocks) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_blocks) return;
   const rv9_block& b = k.blocks[i];
-  int mode = b.y_mode;
-  int mode_type = (mode == 10 || mode == 11 || mode == 13) ? 1 : 0;  // NEARESTMV, NEARMV, NEWMV
-  int rf = b.ref_frame[0] > 0 ? b.ref_frame[0] : 0;
-  int level = k.lvl[b.segment_id][rf][mode_type];
-  int uv_tx;
-  if (b.mi_size < 3) {
-    uv_tx = 0;
-  } else {
-    // get_uv_tx_size with 4:2:0's subsampling for a pre-final profile 1 stream.
-    const uint8_t SS[13][2][2] = {{{0, 14}, {14, 14}}, {{1, 0}, {14, 14}}, {{2, 14}, {0, 14}}, {{3, 2}, {1, 0}},
-                                  {{4, 3}, {14, 1}},   {{5, 14}, {3, 2}},  {{6, 5}, {4, 3}},   {{7, 6}, {14, 4}},
-                                  {{8, 14}, {6, 5}},   {{9, 8}, {7, 6}},   {{10, 9}, {14, 7}}, {{11, 14}, {9, 8}},
-                                  {{12, 11}, {10, 9}}};
-    const uint8_t MAXTX[13] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3, 3};
-    int ux = k.legacy_uv ? 1 : k.ss_x, uy = k.legacy_uv ? 1 : k.ss_y;
-    int uv = SS[b.mi_size][ux][uy];
-    uv_tx = b.tx_size < MAXTX[uv] ? b.tx_size : MAXTX[uv];
-  }
-  bool coded = b.ref_frame[0] <= 0 || !(b.flags & RV9_BLK_SKIP);
-  uint32_t v = (uint32_t)level | ((uint32_t)b.tx_size << 6) | ((uint32_t)uv_tx << 8) | ((uint32_t)b.mi_size << 10) |
-               ((coded ? 1u : 0u) << 14);
-  const uint8_t N8W[13] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4, 4, 8, 8};
-  const uint8_t N8H[13] = {1, 1, 1, 1, 2, 1, 2, 4, 2, 4, 8, 4, 8};
-  int ye = min((int)b.mi_row + N8H[b.mi_size], k.mi_rows);
-  int xe = min((int)b.mi_col + N8W[b.mi_size], k.mi_cols);
+  uint32_t v = lf_block_record(b.mi_size, b.tx_size, (b.flags & RV9_BLK_SKIP) ? 1 : 0, b.segment_id, b.y_mode,
+                               b.ref_frame[0], k.lvl, k.legacy_uv, k.ss_x, k.ss_y);
+  int w8 = 1 << ((0x3ea5400u >> (2 * b.mi_size)) & 3), h8 = 1 << ((0x3b99100u >> (2 * b.mi_size)) & 3);
+  int ye = min((int)b.mi_row + h8, k.mi_rows);
+  int xe = min((int)b.mi_col + w8, k.mi_cols);
   for (int y = b.mi_row; y < ye; ++y)
     for (int x = b.mi_col; x < xe; ++x) k.lf_mi[(size_t)y * k.mi_cols + x] = v;
 }
@@ -501,66 +481,6 @@ constexpr int kLfThreads = 192;
 constexpr int kLfW = 80;   // smem row pitch: 8 left + 64 + 8 of slack
 constexpr int kLfH = 72;   // 8 above + 64
 
-struct LfEdge {
-  int8_t fs;
-  uint8_t limit, blimit, thresh;
-};
-
-// The filtering of one (edge, run) of one pass of one plane of a superblock
-// (reference superblock(), src/decoder/loopfilter.rs:466-620, one entry).
-__device__ LfEdge lf_entry(const KFrame& k, int plane, int pass, int row, int col, int ed, int rn) {
-  LfEdge e{-1, 0, 0, 0};
-  const int sub_x = plane ? k.ss_x : 0, sub_y = plane ? k.ss_y : 0;
-  const int sub = pass == 0 ? sub_x : sub_y;
-  auto at = [&](int e_, int r_, int* x, int* y) {
-    if (pass == 0) {
-      *x = col * 8 + e_ * (4 << sub_x);
-      *y = row * 8 + ((4 * r_) << sub_y);
-    } else {
-      *x = col * 8 + ((4 * r_) << sub_x);
-      *y = row * 8 + e_ * (4 << sub_y);
-    }
-  };
-  int ca = ed >> 1, cb = rn >> 1;
-  int x, y;
-  at(2 * ca, 2 * cb, &x, &y);
-  if (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows) return e;
-  int loop_col = ((x >> 3) >> sub_x) << sub_x;
-  int loop_row = ((y >> 3) >> sub_y) << sub_y;
-  uint32_t m = k.lf_mi[(size_t)loop_row * k.mi_cols + loop_col];
-  int l = m & 63;
-  if (l == 0) return e;
-  int tx_sz = plane ? ((m >> 8) & 3) : ((m >> 6) & 3);
-  int mi_size = (m >> 10) & 15;
-  bool coded = (m >> 14) & 1;
-  const uint8_t N8W[13] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4, 4, 8, 8};
-  const uint8_t N8H[13] = {1, 1, 1, 1, 2, 1, 2, 4, 2, 4, 8, 4, 8};
-  int sb_size = sub == 0 ? mi_size : (mi_size > 6 ? mi_size : 6);
-  int block_mask = pass == 0 ? 8 * N8W[sb_size] - 1 : 8 * N8H[sb_size] - 1;
-  at(ed, 2 * cb, &x, &y);
-  if ((pass == 0 && x == 0) || (pass == 1 && y == 0)) return e;
-  int across = pass == 0 ? x : y;
-  bool is_block_edge = (across & block_mask) == 0;
-  bool tx_edge = (ed & ((1 << tx_sz) - 1)) == 0;
-  if (!is_block_edge && !(tx_edge && coded)) return e;
-  bool is_32_edge = ed % 8 == 0;
-  int base_size = (tx_sz == 0 && is_32_edge) ? 1 : (tx_sz < 2 ? tx_sz : 2);
-  int filter_size = base_size;
-  if ((pass == 0 && sub_x == 1 && base_size == 2 && (x >> 3) == k.mi_cols - 1) ||
-      (pass == 1 && sub_y == 1 && base_size == 2 && (y >> 3) == k.mi_rows - 1))
-    filter_size = 1;
-  at(ed, rn, &x, &y);
-  if ((rn & 1) && (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows)) return e;
-  bool is_tx_edge = tx_edge;
-  if (pass == 1 && sub_x == 1 && (k.mi_cols & 1) && (ed & 1) && (x + 8) >= k.mi_cols * 8) is_tx_edge = false;
-  if (!(is_block_edge || (is_tx_edge && coded))) return e;
-  e.fs = (int8_t)filter_size;
-  e.limit = k.lf_limit[l];
-  e.blimit = k.lf_blimit[l];
-  e.thresh = k.lf_thresh[l];
-  return e;
-}
-
 template <class T>
 __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
   __shared__ int16_t px[3][kLfH][kLfW];
@@ -576,10 +496,11 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
     if (t >= n_sb) return;
     const int sr = t / k.sb64_cols, sc = t - sr * k.sb64_cols;
     const int row = sr * 8, col = sc * 8;
+    const LfParams P{k.mi_cols, k.mi_rows, k.ss_x, k.ss_y, k.lf_mi, k.lf_limit, k.lf_blimit, k.lf_thresh};
     // Edge decisions (independent of samples): before waiting.
     for (int i = threadIdx.x; i < 3 * 2 * 256; i += kLfThreads) {
       int plane = i / 512, pass = (i >> 8) & 1, ed = (i >> 4) & 15, rn = i & 15;
-      edges[plane][pass][ed][rn] = lf_entry(k, plane, pass, row, col, ed, rn);
+      edges[plane][pass][ed][rn] = lf_edge_entry(P, plane, pass, row, col, ed, rn);
     }
     // Wait for (r, c-1) and (r-1, c+1) (or (r-1, c) at the last column).
     if (threadIdx.x == 0) {
@@ -630,17 +551,7 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
         int p = task < rows_p[0] ? 0 : (task < rows_p[0] + rows_p[1] ? 1 : 2);
         int r = task - (p == 0 ? 0 : (p == 1 ? rows_p[0] : rows_p[0] + rows_p[1]));
         int n_edges = 16 >> (p ? k.ss_x : 0);
-        int16_t* line = &px[p][8 + r][0];
-        for (int ed = 0; ed < n_edges; ++ed) {
-          LfEdge e = edges[p][0][ed][r >> 2];
-          if (e.fs < 0) continue;
-          int s[16];
-#pragma unroll
-          for (int q = 0; q < 16; ++q) s[q] = line[4 * ed + q];
-          lf_line(s, e.fs, e.limit, e.blimit, e.thresh, bd);
-#pragma unroll
-          for (int q = 1; q < 15; ++q) line[4 * ed + q] = (int16_t)s[q];
-        }
+        lf_vertical_row(&px[p][8 + r][0], edges[p][0], n_edges, r >> 2, bd);
       }
     }
     __syncthreads();
@@ -651,17 +562,7 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
         int p = task < cols_p[0] ? 0 : (task < cols_p[0] + cols_p[1] ? 1 : 2);
         int c = task - (p == 0 ? 0 : (p == 1 ? cols_p[0] : cols_p[0] + cols_p[1]));
         int n_edges = 16 >> (p ? k.ss_y : 0);
-        for (int ed = 0; ed < n_edges; ++ed) {
-          LfEdge e = edges[p][1][ed][c >> 2];
-          if (e.fs < 0) continue;
-          int s[16];
-#pragma unroll
-          for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < kLfH) ? px[p][4 * ed + q][8 + c] : 0;
-          lf_line(s, e.fs, e.limit, e.blimit, e.thresh, bd);
-#pragma unroll
-          for (int q = 1; q < 15; ++q)
-            if (4 * ed + q < kLfH) px[p][4 * ed + q][8 + c] = (int16_t)s[q];
-        }
+        lf_horizontal_col(&px[p][0][8 + c], kLfW, kLfH, edges[p][1], n_edges, c >> 2, bd);
       }
     }
     __syncthreads();

@@ -5,6 +5,11 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
+#include <vector>
+
+#include "../../include/rv9_records.h"
+
 #include "../../rivet-vp9_b200/csrc/gpu/dsp_math.cuh"
 
 using namespace rv9g;
@@ -94,3 +99,91 @@ void shim_lf(uint16_t* buf, int filter_size, int limit, int blimit, int thresh, 
 }
 
 }  // extern "C"
+
+// The loop-filter kernel's superblock procedure, run over the superblocks in
+// raster order: per superblock, the region from 8 samples above and left is
+// copied to a tile, the edge entries are decided, vertical edges filter one
+// row at a time, horizontal edges one column at a time, and the tile is
+// written back. `planes` are SB-aligned with the given strides.
+extern "C" void shim_lf_frame(const rv9_frame_desc* d, const rv9_block* blocks, int n_blocks, uint16_t* planes0,
+                              uint16_t* planes1, uint16_t* planes2) {
+  uint16_t* planes[3] = {planes0, planes1, planes2};
+  int aw = d->sb64_cols * 64, ah = d->sb64_rows * 64;
+  int stride[3] = {aw, aw >> d->ss_x, aw >> d->ss_x};
+  // LvlLookup and limits (8.8.1).
+  uint8_t lvl[8][4][2];
+  uint8_t lim[64], blim[64], thr[64];
+  int n_shift = d->lf_level >> 5;
+  for (int seg = 0; seg < 8; ++seg) {
+    int lvl_seg = d->lf_level;
+    if (d->seg.enabled && d->seg.feature_enabled[seg][1]) {
+      int data = d->seg.feature_data[seg][1];
+      lvl_seg = d->seg.abs_or_delta_update ? data : data + d->lf_level;
+      lvl_seg = lvl_seg < 0 ? 0 : (lvl_seg > 63 ? 63 : lvl_seg);
+    }
+    for (int rf = 0; rf < 4; ++rf)
+      for (int mode = 0; mode < 2; ++mode) {
+        int v = lvl_seg;
+        if (d->lf_delta_enabled) {
+          v = lvl_seg + d->lf_ref_deltas[rf] * (1 << n_shift);
+          if (rf > 0) v += d->lf_mode_deltas[mode] * (1 << n_shift);
+        }
+        lvl[seg][rf][mode] = (uint8_t)(v < 0 ? 0 : (v > 63 ? 63 : v));
+      }
+  }
+  int shift = d->lf_sharpness > 4 ? 2 : (d->lf_sharpness > 0 ? 1 : 0);
+  for (int l = 0; l < 64; ++l) {
+    int limit = l >> shift;
+    if (d->lf_sharpness > 0 && limit > 9 - d->lf_sharpness) limit = 9 - d->lf_sharpness;
+    if (limit < 1) limit = 1;
+    lim[l] = (uint8_t)limit;
+    blim[l] = (uint8_t)(2 * (l + 2) + limit);
+    thr[l] = (uint8_t)(l >> 4);
+  }
+  std::vector<uint32_t> lf_mi((size_t)d->mi_rows * d->mi_cols);
+  for (int i = 0; i < n_blocks; ++i) {
+    const rv9_block& b = blocks[i];
+    uint32_t v = lf_block_record(b.mi_size, b.tx_size, (b.flags & RV9_BLK_SKIP) ? 1 : 0, b.segment_id, b.y_mode,
+                                 b.ref_frame[0], lvl, d->legacy_uv, d->ss_x, d->ss_y);
+    int w8 = 1 << ((0x3ea5400u >> (2 * b.mi_size)) & 3), h8 = 1 << ((0x3b99100u >> (2 * b.mi_size)) & 3);
+    for (int y = b.mi_row; y < (int)std::min<uint32_t>(b.mi_row + h8, d->mi_rows); ++y)
+      for (int x = b.mi_col; x < (int)std::min<uint32_t>(b.mi_col + w8, d->mi_cols); ++x)
+        lf_mi[(size_t)y * d->mi_cols + x] = v;
+  }
+  LfParams P{(int)d->mi_cols, (int)d->mi_rows, d->ss_x, d->ss_y, lf_mi.data(), lim, blim, thr};
+  static int16_t px[3][72][80];
+  static LfEdge edges[3][2][16][16];
+  for (int sr = 0; sr < (int)d->sb64_rows; ++sr)
+    for (int sc = 0; sc < (int)d->sb64_cols; ++sc) {
+      int row = sr * 8, col = sc * 8;
+      for (int i = 0; i < 3 * 2 * 256; ++i) {
+        int plane = i / 512, pass = (i >> 8) & 1, ed = (i >> 4) & 15, rn = i & 15;
+        edges[plane][pass][ed][rn] = lf_edge_entry(P, plane, pass, row, col, ed, rn);
+      }
+      int rows_p[3], cols_p[3], x0s[3], y0s[3];
+      for (int p = 0; p < 3; ++p) {
+        int sxp = p ? d->ss_x : 0, syp = p ? d->ss_y : 0;
+        rows_p[p] = 64 >> syp;
+        cols_p[p] = 64 >> sxp;
+        x0s[p] = (col * 8) >> sxp;
+        y0s[p] = (row * 8) >> syp;
+        for (int r = 0; r < rows_p[p] + 8; ++r)
+          for (int c = 0; c < cols_p[p] + 8; ++c) {
+            int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + c;
+            if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) px[p][r][c] = (int16_t)planes[p][(size_t)gy * stride[p] + gx];
+          }
+      }
+      for (int p = 0; p < 3; ++p)
+        for (int r = 0; r < rows_p[p]; ++r)
+          lf_vertical_row(&px[p][8 + r][0], edges[p][0], 16 >> (p ? d->ss_x : 0), r >> 2, d->bit_depth);
+      for (int p = 0; p < 3; ++p)
+        for (int c = 0; c < cols_p[p]; ++c)
+          lf_horizontal_col(&px[p][0][8 + c], 80, 72, edges[p][1], 16 >> (p ? d->ss_y : 0), c >> 2, d->bit_depth);
+      for (int p = 0; p < 3; ++p)
+        for (int r = 0; r < rows_p[p] + 8; ++r)
+          for (int c = 0; c < cols_p[p] + 8; ++c) {
+            int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + c;
+            if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) planes[p][(size_t)gy * stride[p] + gx] = (uint16_t)px[p][r][c];
+          }
+    }
+}

@@ -109,3 +109,59 @@ def test_loop_filter_lines(libs):
         o.rv9o_test_lf(P(a), fs, limit, blimit, thresh, bd)
         s.shim_lf(P(b), fs, limit, blimit, thresh, bd)
         assert np.array_equal(a, b), (fs, bd)
+
+
+def _lf_case(libs, rng, w, h, ss_x, ss_y, bd):
+    from records_ctypes import FrameDesc, Block, random_blocks
+    o, s = libs
+    d = FrameDesc()
+    d.width, d.height = w, h
+    d.mi_cols, d.mi_rows = (w + 7) >> 3, (h + 7) >> 3
+    d.sb64_cols, d.sb64_rows = (d.mi_cols + 7) >> 3, (d.mi_rows + 7) >> 3
+    d.ss_x, d.ss_y, d.bit_depth = ss_x, ss_y, bd
+    d.lf_level = int(rng.integers(1, 64))
+    d.lf_sharpness = int(rng.integers(0, 8))
+    d.lf_delta_enabled = int(rng.integers(0, 2))
+    for i, v in enumerate(rng.integers(-15, 16, 4)):
+        d.lf_ref_deltas[i] = int(v)
+    for i, v in enumerate(rng.integers(-15, 16, 2)):
+        d.lf_mode_deltas[i] = int(v)
+    d.seg.enabled = int(rng.integers(0, 2))
+    for sgi in range(8):
+        d.seg.feature_enabled[sgi][1] = int(rng.integers(0, 2))
+        d.seg.feature_data[sgi][1] = int(rng.integers(-63, 64))
+    d.seg.abs_or_delta_update = int(rng.integers(0, 2))
+    blocks = random_blocks(rng, d.mi_rows, d.mi_cols, ss_x, ss_y)
+    arr = (Block * len(blocks))(*blocks)
+    aw, ah = d.sb64_cols * 64, d.sb64_rows * 64
+    planes = []
+    for p in range(3):
+        pw, ph = (aw >> ss_x, ah >> ss_y) if p else (aw, ah)
+        yy, xx = np.mgrid[0:ph, 0:pw]
+        base = (xx * 3 + yy * 2 + rng.integers(0, 64)) % (1 << bd)
+        noise = rng.integers(-3, 4, (ph, pw)) << (bd - 8)
+        blocky = ((xx // 8 + yy // 8) % 2) * int(rng.integers(0, 24)) << (bd - 8)
+        planes.append(np.clip(base // 4 + noise + blocky, 0, (1 << bd) - 1).astype(np.uint16))
+    a = [pl.copy() for pl in planes]
+    b = [pl.copy() for pl in planes]
+    o.rv9o_test_lf_frame(ctypes.byref(d), arr, len(blocks), P(a[0]), P(a[1]), P(a[2]))
+    s.shim_lf_frame(ctypes.byref(d), arr, len(blocks), P(b[0]), P(b[1]), P(b[2]))
+    changed = sum(int((a[p] != planes[p]).sum()) for p in range(3))
+    for p in range(3):
+        assert np.array_equal(a[p], b[p]), (w, h, ss_x, ss_y, bd, p, np.argwhere(a[p] != b[p])[:4].tolist())
+    return changed
+
+
+def test_loop_filter_frames(libs):
+    """The loop-filter kernel's superblock procedure (edge decisions, row and
+    column passes, tile copy) against the oracle's filter_frame, on random
+    block layouts and levels, every chroma format, odd sizes."""
+    rng = np.random.default_rng(17)
+    changed = 0
+    sizes = [(66, 66), (130, 132), (226, 226), (8, 8), (200, 120), (352, 288), (72, 40)]
+    for i in range(40):
+        w, h = sizes[i % len(sizes)]
+        ss = [(1, 1), (1, 0), (0, 1), (0, 0)][i % 4]
+        bd = [8, 10, 12][i % 3]
+        changed += _lf_case(libs, rng, w, h, ss[0], ss[1], bd)
+    assert changed > 0
