@@ -28,6 +28,7 @@ HEADERS = [
     "gpu/engine_types.h",
     "gpu/engine.h",
     "host/parser.h",
+    "host/syntax.h",
     "host/probs.h",
     "host/bitreader.h",
     "common/vp9_tables.h",
@@ -51,6 +52,29 @@ def stale():
     deps += [os.path.join(HERE, "..", "include", h) for h in ("rv9.h", "rv9_records.h")]
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps)
+
+
+ENC_LIB = os.path.join(OUT, "librv9enc.so")
+ENC_SOURCES = ["encoder/encoder.cpp", "host/probs.cpp"]
+ENC_HEADERS = ["encoder/recon_host.h", "host/syntax.h", "host/parser.h", "host/probs.h", "gpu/dsp_math.cuh",
+               "common/vp9_tables.h", "common/vp9_consts.h"]
+
+
+def build_encoder(force=False, verbose=False):
+    """The stream generator (host CPU code): _build/librv9enc.so."""
+    deps = [os.path.join(CSRC, s) for s in ENC_SOURCES + ENC_HEADERS]
+    deps.append(os.path.join(HERE, "..", "include", "rv9_encoder.h"))
+    if not force and os.path.exists(ENC_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(ENC_LIB) for d in deps):
+        return ENC_LIB
+    os.makedirs(OUT, exist_ok=True)
+    tmp = ENC_LIB + ".tmp"
+    cmd = ["g++", "-std=c++17", "-O3", "-fPIC", "-shared", "-o", tmp] + [os.path.join(CSRC, s) for s in ENC_SOURCES]
+    cmd += ["-lpthread"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, ENC_LIB)
+    return ENC_LIB
 
 
 def build(force=False, verbose=False):
@@ -79,3 +103,4 @@ def build(force=False, verbose=False):
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build_encoder(force="--force" in sys.argv, verbose=True))
