@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""Benchmark: bit-exact decoded Mpixels/s of the B200 VP9 reconstruction engine.
+
+Workload (one GPU): the single-stream GPU reconstruction configuration —
+1920x1080 profile 0 8-bit 4:2:0 synthetic video (2D sine gradient panned by
+(+3,+2) px/frame, 12 moving 32x24 rectangles, uniform noise +-6), encoded by
+this repository's stream generator with 4 tile columns at base_q_idx 40 and
+80, 60 frames each. A step decodes both streams (120 frames).
+
+  value   reconstruction with the streams' records resident in HBM
+          (rv9_sequence_run: every kernel, no host work, no copies), CUDA
+          events on the engine's stream, max over ranks.
+  e2e     the same metric through the public C ABI (rv9_decode_packets) from
+          host packets: host parsing, record upload from pinned memory,
+          kernels, and the decoded frames copied back to pinned host memory.
+  roofline  the kernel with the most device time: algorithmic bytes per
+          launch / average launch time (CUDA events around each launch),
+          against the measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (restated scalar decoder) on a bounded sample.
+
+`--impl reference` times the reference's CPU decoder path instead: the Rust
+crate cannot be built here (no toolchain), so its restatement (the oracle)
+runs with all host threads on the same workload.
+
+Multi-GPU: one process per GPU (torchrun); each rank decodes its own copy of
+the streams (independent streams, no collective in the data path); value is
+the sum of all ranks' samples over the slowest rank's time.
+"""
+import argparse
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "rivet-vp9_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+STREAMS = [
+    dict(name="1080p_q40", width=1920, height=1080, frames=60, q=40, seed=0),
+    dict(name="1080p_q80", width=1920, height=1080, frames=60, q=80, seed=1),
+]
+METRIC = "decoded Mpixels/s (bit-exact, 1080p 8-bit 4:2:0, 4 tile columns, q40+q80)"
+STREAM_DIR = os.path.join(PKG, "_build", "streams")
+
+
+def stream_packets(spec):
+    """Packets of a workload stream (generated once, cached under _build)."""
+    from rv9 import containers, streams
+    path = os.path.join(STREAM_DIR, spec["name"] + ".ivf")
+    if not os.path.exists(path):
+        cfg = streams.config(spec["width"], spec["height"], spec["frames"], spec["q"], bit_depth=8, chroma=(1, 1),
+                             tile_cols_log2=2, golden_interval=8, seed=spec["seed"], pan=(3, 2), rectangles=12,
+                             noise=6)
+        pk = streams.generate(cfg)
+        os.makedirs(STREAM_DIR, exist_ok=True)
+        with open(path[:-4] + ".last.md5", "w") as f:
+            f.write(hashlib.md5(streams.last_reconstruction()).hexdigest())
+        tmp = path + f".tmp{os.getpid()}"
+        with open(tmp, "wb") as f:
+            f.write(containers.ivf_write(pk, spec["width"], spec["height"]))
+        os.replace(tmp, path)
+    with open(path, "rb") as f:
+        return containers.ivf_packets(f.read())
+
+
+def dist_setup(backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary."""
+    p = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def cpu_baseline(packets_list, frames):
+    """The oracle (single thread) on the first `frames` frames of each stream."""
+    import oracle
+    samples, secs = 0, 0.0
+    for pk in packets_list:
+        dec = oracle.OracleDecoder(threads=1)
+        t = time.perf_counter()
+        for p in pk[:frames]:
+            for fr in dec.decode_all(p):
+                samples += fr.width * fr.height
+        secs += time.perf_counter() - t
+    return samples / secs / 1e6, secs
+
+
+def run_gpu(args, world, rank, local):
+    import torch
+    import rv9
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    packets = [stream_packets(s) for s in STREAMS]
+    if args.frames:
+        packets = [pk[:args.frames] for pk in packets]
+    dec = rv9.Decoder(device=local)
+    # Consistency: the public decode path reproduces the generator's closed-
+    # loop reconstruction of the last frame (bit-exact).
+    seqs = [dec.load_sequence(pk) for pk in packets]
+    luma_per_step = sum(s.luma_samples for s in seqs)
+    bytes_per_step = sum(s.algorithmic_bytes for s in seqs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(per_kernel):
+        ms = 0.0
+        for s in seqs:
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            ms += s.run(per_kernel=per_kernel)
+        return ms
+
+    for _ in range(args.warmup):
+        step(False)
+    dec.kernel_stats(reset=True)
+    launches0 = dec.stats()["kernel_launches"]
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    ms_total = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ms_total += step(True)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    dist_barrier(world)
+    clocks = sampler.stop() if sampler else None
+    launches = dec.stats()["kernel_launches"] - launches0
+    ks = dec.kernel_stats(reset=True)
+    ms_max = dist_max(ms_total, world, dev)
+    value = luma_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+    # Roofline of the kernel with the most device time.
+    top = max(ks.items(), key=lambda kv: kv[1]["ms"])
+    name, st = top
+    peak, peak_kind = measured_peaks()
+    achieved = (st["algorithmic_bytes"] / max(st["launches"], 1)) / (st["ms"] / max(st["launches"], 1) / 1e3) / 1e9
+    traffic = ncu_traffic().get(name)
+    kernels = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                   "share": round(v["ms"] / max(sum(x["ms"] for x in ks.values()), 1e-9), 4),
+                   "GBps": round(v["algorithmic_bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in ks.items()}
+    # End to end through the public API.
+    frame_bytes = 1920 * 1080 * 3 // 2
+    cap = max(len(pk) for pk in packets) * frame_bytes + (1 << 20)
+    host_out = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = sum(s.record_bytes for s in seqs)
+    d2h = 0
+    e2e_secs = 0.0
+    last_md5 = None
+    for i in range(e2e_steps + 1):
+        torch.cuda.synchronize(dev)
+        dist_barrier(world)
+        t = time.perf_counter()
+        n_out = 0
+        for pk in packets:
+            nf, nb = dec.decode_packets_to(pk, host_out.data_ptr(), cap)
+            n_out += nb
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t
+        if i > 0:  # the first pass warms the frame pool
+            e2e_secs += dt
+        d2h = n_out
+        last_md5 = hashlib.md5(bytes(host_out[nb - frame_bytes: nb].numpy())).hexdigest()
+    e2e_secs = dist_max(e2e_secs, world, dev)
+    e2e_value = luma_per_step * e2e_steps * world / e2e_secs / 1e6
+    # Bit-exactness of what was timed: the last frame of the q80 stream from
+    # the public API, from the device-resident replay (slot 0 after the timed
+    # runs), and from the generator's closed-loop reconstruction.
+    replay_md5 = hashlib.md5(dec.download_slot(0, frame_bytes)).hexdigest()
+    gen_md5_path = os.path.join(STREAM_DIR, STREAMS[-1]["name"] + ".last.md5")
+    gen_md5 = open(gen_md5_path).read().strip() if os.path.exists(gen_md5_path) else None
+    check = {"e2e_equals_replay": last_md5 == replay_md5,
+             "equals_generator_reconstruction": (gen_md5 == last_md5) if gen_md5 else None}
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu_val, cpu_secs = cpu_baseline(packets, 8)
+        cpu = {"value": round(cpu_val, 2), "unit": "Mpixels/s", "cores": 1, "kind": "port",
+               "sample": f"first 8 frames of each stream (16 x 1080p), single thread, {cpu_secs:.1f} s; "
+                         "restated scalar C++, not the reference's SIMD build"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mpixels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator + encoder)",
+            "config": {"workload": "1080p 8-bit 4:2:0, 4 tile columns, q40 + q80, 2 x 60 frames per step",
+                       "width": 1920, "height": 1080, "frames_per_step": sum(s.frames for s in seqs),
+                       "streams_per_gpu": len(seqs), "l2": "flushed between sequences (256 MiB write)",
+                       "parallelism": f"replicas x{world}", "records_resident_bytes": h2d},
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mpixels/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": traffic},
+            "algorithmic_GBps_all_kernels": round(bytes_per_step * args.steps / (ms_total / 1e3) / 1e9, 1),
+            "kernels": kernels, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+            "bit_exact_check": check, "wall_s_timed": round(wall, 3),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU decoder path (its restatement) with all host threads."""
+    if rank != 0:
+        return
+    import oracle
+    packets = [stream_packets(s) for s in STREAMS]
+    cores = os.cpu_count() or 1
+    per = max(1, cores // len(packets))
+    frames = 12  # per stream per step: a bounded sample of the workload
+
+    def decode(pk, out, i):
+        dec = oracle.OracleDecoder(threads=per)
+        n = 0
+        for p in pk[:frames]:
+            for fr in dec.decode_all(p):
+                n += fr.width * fr.height
+        out[i] = n
+
+    def step():
+        out = [0] * len(packets)
+        th = [threading.Thread(target=decode, args=(pk, out, i)) for i, pk in enumerate(packets)]
+        t = time.perf_counter()
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        return sum(out), time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        step()
+    samples, secs = 0, 0.0
+    for _ in range(args.steps):
+        n, dt = step()
+        samples += n
+        secs += dt
+    value = samples / secs / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "Mpixels/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator + encoder)",
+        "config": {"workload": "1080p 8-bit 4:2:0, 4 tile columns, q40 + q80", "width": 1920, "height": 1080,
+                   "sample": f"first {frames} frames of each of the 2 streams per step", "parallelism": "host threads"},
+        "e2e": {"value": round(value, 2), "unit": "Mpixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": round(value, 2), "unit": "Mpixels/s", "cores": min(cores, per * len(packets)),
+                         "kind": "port",
+                         "sample": f"first {frames} frames of both streams per step, the streams decoded "
+                                   f"concurrently, {per} tile threads each; the reference crate (Rust) cannot be "
+                                   "built here, so its C++ restatement runs"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="rv9", choices=["rv9", "reference"])
+    ap.add_argument("--frames", type=int, default=0, help="frames per stream (0: all; fewer for profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        world, rank, _ = dist_setup("gloo")
+        run_reference(args, world, rank)
+    else:
+        world, rank, local = dist_setup("nccl")
+        run_gpu(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

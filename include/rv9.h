@@ -115,6 +115,38 @@ typedef struct rv9_stats {
 } rv9_stats;
 void rv9_decoder_stats(rv9_decoder* dec, rv9_stats* out, int reset);
 
+/* ---- Device-resident replay (the reconstruction engine on its own) ----
+ *
+ * A sequence is a stream's packets parsed on the host, with their records
+ * and work lists copied to device memory once; rv9_sequence_run then
+ * reconstructs every frame from those records (all kernels, no host work,
+ * no copies), starting from empty reference slots. This measures the
+ * reconstruction path with its inputs resident in HBM. */
+typedef struct rv9_sequence rv9_sequence;
+rv9_status rv9_sequence_load(rv9_decoder* dec, const uint8_t* const* packets, const size_t* lens, size_t n,
+                             rv9_sequence** out);
+/* Reconstructs the sequence; *device_ms receives the CUDA-event time of the
+ * run on the decoder's stream. With per_kernel, each launch is bracketed by
+ * events for rv9_kernel_stats. */
+rv9_status rv9_sequence_run(rv9_decoder* dec, rv9_sequence* seq, int per_kernel, double* device_ms);
+uint32_t rv9_sequence_frames(const rv9_sequence* seq);
+uint64_t rv9_sequence_luma_samples(const rv9_sequence* seq);     /* visible luma of shown frames */
+uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* seq); /* per run */
+uint64_t rv9_sequence_record_bytes(const rv9_sequence* seq);      /* device bytes held */
+void rv9_sequence_free(rv9_decoder* dec, rv9_sequence* seq);
+
+/* The frame in reference slot `slot` (0..7), packed like rv9_frame data. */
+rv9_status rv9_decoder_download_slot(rv9_decoder* dec, int slot, uint8_t* out, size_t cap, size_t* bytes);
+
+typedef struct rv9_kernel_stat {
+  char name[24];
+  uint64_t launches;
+  double ms;                  /* summed CUDA-event durations */
+  uint64_t algorithmic_bytes; /* summed over the launches */
+} rv9_kernel_stat;
+/* Per-kernel timing of the per_kernel sequence runs; returns the count. */
+size_t rv9_kernel_stats(rv9_decoder* dec, rv9_kernel_stat* out, size_t cap, int reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,5 +1,6 @@
 // The C ABI of rv9.h: the reference decoder API (src/decoder/mod.rs:150-216)
 // over the host parser and the CUDA reconstruction engine.
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -87,7 +88,8 @@ rv9_status rv9_decode_all(rv9_decoder* d, const uint8_t* pkt, size_t len, rv9_fr
         rv9_frame* o = &out[*n_out];
         fill_meta(shown, o);
         o->data = (uint8_t*)malloc(o->size ? o->size : 1);
-        rv9::Status s2 = d->engine.download(shown, o->data, &d->err);
+        rv9::Status s2 = d->engine.download_async(shown, o->data, &d->err);
+        if (s2 == rv9::ST_OK) s2 = d->engine.sync(&d->err);
         if (s2 != rv9::ST_OK) return (rv9_status)s2;
       }
       ++*n_out;
@@ -143,6 +145,84 @@ rv9_status rv9_decode_packets(rv9_decoder* d, const uint8_t* const* pkts, const 
     }
   }
   return (rv9_status)d->engine.sync(&d->err);
+}
+
+struct rv9_sequence {
+  rv9g::Sequence seq;
+};
+
+rv9_status rv9_sequence_load(rv9_decoder* d, const uint8_t* const* pkts, const size_t* lens, size_t n,
+                             rv9_sequence** out) {
+  *out = nullptr;
+  rv9::Parser parser;  // a fresh stream
+  parser.set_threads(0);
+  std::vector<rv9::ParsedFrame> frames;
+  std::vector<std::pair<size_t, size_t>> split;
+  for (size_t i = 0; i < n; ++i) {
+    rv9::superframe_split(pkts[i], lens[i], &split);
+    for (auto& fr : split) {
+      frames.emplace_back();
+      rv9::Status st = parser.parse_frame(pkts[i] + fr.first, fr.second, &frames.back(), &d->err);
+      if (st != rv9::ST_OK) return (rv9_status)st;
+    }
+  }
+  rv9_sequence* s = new rv9_sequence;
+  rv9::Status st = d->engine.sequence_load(frames, &s->seq, &d->err);
+  if (st != rv9::ST_OK) {
+    delete s;
+    return (rv9_status)st;
+  }
+  *out = s;
+  return RV9_OK;
+}
+
+rv9_status rv9_sequence_run(rv9_decoder* d, rv9_sequence* s, int per_kernel, double* device_ms) {
+  float ms = 0;
+  rv9::Status st = d->engine.sequence_run(s->seq, per_kernel != 0, &ms, &d->err);
+  *device_ms = ms;
+  return (rv9_status)st;
+}
+
+uint32_t rv9_sequence_frames(const rv9_sequence* s) { return (uint32_t)s->seq.frames.size(); }
+uint64_t rv9_sequence_luma_samples(const rv9_sequence* s) { return s->seq.luma_samples; }
+uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* s) {
+  uint64_t b = 0;
+  for (const auto& f : s->seq.frames) b += f.total_bytes;
+  return b;
+}
+uint64_t rv9_sequence_record_bytes(const rv9_sequence* s) { return s->seq.bytes; }
+
+void rv9_sequence_free(rv9_decoder* d, rv9_sequence* s) {
+  if (!s) return;
+  d->engine.sequence_free(&s->seq);
+  delete s;
+}
+
+rv9_status rv9_decoder_download_slot(rv9_decoder* d, int slot, uint8_t* out, size_t cap, size_t* bytes) {
+  *bytes = 0;
+  if (slot < 0 || slot > 7 || !d->engine.slot(slot)) return RV9_INVALID_INPUT;
+  rv9g::DevFrame* f = d->engine.slot(slot);
+  size_t nb = rv9g::Engine::packed_bytes(f);
+  if (nb > cap) return RV9_INVALID_INPUT;
+  rv9::Status st = d->engine.download_async(f, out, &d->err);
+  if (st == rv9::ST_OK) st = d->engine.sync(&d->err);
+  *bytes = nb;
+  return (rv9_status)st;
+}
+
+size_t rv9_kernel_stats(rv9_decoder* d, rv9_kernel_stat* out, size_t cap, int reset) {
+  size_t n = 0;
+  for (int k = 0; k < rv9g::K_COUNT; ++k) {
+    if (n < cap) {
+      snprintf(out[n].name, sizeof out[n].name, "%s", rv9g::kKernelNames[k]);
+      out[n].launches = d->engine.kstats[k].launches;
+      out[n].ms = d->engine.kstats[k].ms;
+      out[n].algorithmic_bytes = d->engine.kstats[k].bytes;
+    }
+    ++n;
+    if (reset) d->engine.kstats[k] = rv9g::KernelStat();
+  }
+  return n;
 }
 
 void rv9_decoder_stats(rv9_decoder* d, rv9_stats* out, int reset) {

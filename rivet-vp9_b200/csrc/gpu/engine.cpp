@@ -16,27 +16,36 @@
 namespace rv9g {
 using namespace vp9;
 
-#define CK(call)                                           \
-  do {                                                     \
-    cudaError_t e_ = (call);                               \
-    if (e_ != cudaSuccess) {                               \
+const char* const kKernelNames[K_COUNT] = {"k_zero_pad", "k_lf_mi", "k_intra_mark", "k_inter",
+                                           "k_inter_res", "k_intra", "k_lf"};
+
+#define CK(call)                                                 \
+  do {                                                           \
+    cudaError_t e_ = (call);                                     \
+    if (e_ != cudaSuccess) {                                     \
       *err = std::string(#call) + ": " + cudaGetErrorString(e_); \
-      return rv9::ST_DEVICE;                               \
-    }                                                      \
+      return rv9::ST_DEVICE;                                     \
+    }                                                            \
   } while (0)
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (DevFrame* f : pool_) {
-    if (f->ready) cudaEventDestroy(f->ready);
     cudaFree(f->base);
     delete f;
   }
-  cudaFree(d_scratch_);
-  cudaFreeHost(h_scratch_);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(d_stage_[i]);
+    cudaFreeHost(h_stage_[i]);
+    if (stage_ev_[i]) cudaEventDestroy(stage_ev_[i]);
+  }
   cudaFree(d_lf_mi_);
   cudaFree(d_sb_done_);
   cudaFree(d_counters_);
+  cudaFreeHost(h_error_);
+  for (cudaEvent_t e : kev_) cudaEventDestroy(e);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -65,10 +74,13 @@ bool Engine::init(int device, std::string* err) {
   n_sm_ = prop.multiProcessorCount;
   if ((e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreate(&ev0_)) != cudaSuccess || (e = cudaEventCreate(&ev1_)) != cudaSuccess ||
-      (e = cudaMalloc(&d_counters_, 64)) != cudaSuccess) {
+      (e = cudaEventCreateWithFlags(&stage_ev_[0], cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&stage_ev_[1], cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaMalloc(&d_counters_, 64)) != cudaSuccess || (e = cudaMallocHost(&h_error_, 64)) != cudaSuccess) {
     *err = cudaGetErrorString(e);
     return false;
   }
+  *h_error_ = 0;
   int16_t f[4][16][8];
   for (int a = 0; a < 4; ++a)
     for (int b = 0; b < 16; ++b)
@@ -88,8 +100,10 @@ size_t Engine::packed_bytes(const DevFrame* f) {
 
 DevFrame* Engine::alloc_frame(const rv9_frame_desc& d) {
   uint32_t aw = d.sb64_cols * 64, ah = d.sb64_rows * 64;
+  // A frame no slot holds is free: every use of it is queued on the stream
+  // before the work that overwrites it.
   for (DevFrame* f : pool_) {
-    if (f->refs == 0 && !f->busy && f->aw == aw && f->ah == ah && f->ss_x == d.ss_x && f->ss_y == d.ss_y &&
+    if (f->refs == 0 && f->aw == aw && f->ah == ah && f->ss_x == d.ss_x && f->ss_y == d.ss_y &&
         f->bit_depth == d.bit_depth)
       return f;
   }
@@ -107,12 +121,12 @@ DevFrame* Engine::alloc_frame(const rv9_frame_desc& d) {
     f->stride[p] = w;
     f->pheight[p] = h;
     plane_off[p] = off;
-    off += ((size_t)w * h * bps + 255) & ~(size_t)255;
+    off += align256((size_t)w * h * bps);
   }
   for (int p = 0; p < 3; ++p) {
     f->cell_stride[p] = f->stride[p] / 4;
     cell_off[p] = off;
-    off += ((size_t)f->cell_stride[p] * (f->pheight[p] / 4) + 255) & ~(size_t)255;
+    off += align256((size_t)f->cell_stride[p] * (f->pheight[p] / 4));
   }
   f->bytes = off;
   if (cudaMalloc(&f->base, off) != cudaSuccess) {
@@ -124,30 +138,15 @@ DevFrame* Engine::alloc_frame(const rv9_frame_desc& d) {
     f->cells[p] = (uint8_t*)f->base + cell_off[p];
   }
   cudaMemsetAsync(f->base, 0, off, stream_);
-  cudaEventCreateWithFlags(&f->ready, cudaEventDisableTiming);
   pool_.push_back(f);
   return f;
 }
 
-void Engine::release_ref(DevFrame* f) {
-  if (f) --f->refs;
-}
-
-bool Engine::ensure_scratch(size_t bytes, std::string* err) {
-  if (bytes <= scratch_cap_) return true;
-  size_t cap = std::max(bytes, scratch_cap_ * 3 / 2);
-  cudaStreamSynchronize(stream_);
-  cudaFree(d_scratch_);
-  cudaFreeHost(h_scratch_);
-  d_scratch_ = nullptr;
-  h_scratch_ = nullptr;
-  scratch_cap_ = 0;
-  if (cudaMalloc(&d_scratch_, cap) != cudaSuccess || cudaMallocHost(&h_scratch_, cap) != cudaSuccess) {
-    *err = "out of memory for frame records";
-    return false;
+void Engine::reset_slots() {
+  for (int i = 0; i < 8; ++i) {
+    if (slots_[i]) --slots_[i]->refs;
+    slots_[i] = nullptr;
   }
-  scratch_cap_ = cap;
-  return true;
 }
 
 static int uv_tx_size(const rv9_frame_desc& d, const rv9_block& b) {
@@ -157,15 +156,37 @@ static int uv_tx_size(const rv9_frame_desc& d, const rv9_block& b) {
   return std::min<int>(b.tx_size, MAX_TXSIZE_LOOKUP[uv]);
 }
 
-// The work lists: the prediction regions and residuals of inter blocks, and
-// the intra transform blocks in bitstream order (replay's loop structure).
-void Engine::build_work(const rv9::ParsedFrame& pf) {
+template <class T>
+static size_t put(std::vector<uint8_t>* out, const T* data, size_t n) {
+  size_t off = align256(out->size());
+  out->resize(off + n * sizeof(T));
+  if (n) memcpy(out->data() + off, data, n * sizeof(T));
+  return off;
+}
+
+// The work lists (the prediction regions and residuals of inter blocks, and
+// the intra transform blocks in bitstream order, replay's loop structure) and
+// the frame's staged bytes, appended to `out`. Algorithmic bytes per kernel:
+// inter 1 sample per predicted sample and reference plus the output; a
+// residual its coefficient words plus reading and writing its samples; intra
+// its samples out plus (3 n + 1) edge samples plus its coefficients; the loop
+// filter reading and writing the mode-info area once; all at 1 byte per
+// sample at 8 bits, 2 above.
+void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<uint8_t>* out) {
   const rv9_frame_desc& d = pf.desc;
+  fw->desc = d;
+  fw->show_existing = pf.show_existing;
+  fw->show_slot = pf.show_slot;
+  fw->show_frame = pf.show_frame;
+  fw->refresh_mask = pf.refresh_mask;
+  for (int i = 0; i < 3; ++i) fw->ref_slot[i] = pf.ref_slot[i];
+  memset(fw->kbytes, 0, sizeof fw->kbytes);
+  fw->total_bytes = 0;
+  if (pf.show_existing) return;
   units_.clear();
   res_.clear();
   intra_.clear();
-  const size_t bps = d.bit_depth > 8 ? 2 : 1;
-  uint64_t ref_bytes = 0;
+  const uint64_t bps = d.bit_depth > 8 ? 2 : 1;
   for (uint32_t bi = 0; bi < pf.blocks.size(); ++bi) {
     const rv9_block& b = pf.blocks[bi];
     const bool is_inter = b.flags & RV9_BLK_INTER;
@@ -190,7 +211,7 @@ void Engine::build_work(const rv9::ParsedFrame& pf) {
           units_.push_back(
               InterUnit{bi, (uint16_t)base_x, (uint16_t)base_y, (uint8_t)plane, (uint8_t)n4w, (uint8_t)n4h, 0});
         }
-        ref_bytes += (uint64_t)n4w * n4h * 16 * bps * nrefs;
+        fw->kbytes[K_INTER] += (uint64_t)n4w * n4h * 16 * bps * (nrefs + 1);
       }
       int max_x = (int)((d.mi_cols * 8) >> sx), max_y = (int)((d.mi_rows * 8) >> sy);
       int block_idx = 0;
@@ -203,38 +224,94 @@ void Engine::build_work(const rv9::ParsedFrame& pf) {
               t = tok++;
               if (pf.toks[t].eob == 0) t = NO_TOK;
             }
+            const uint64_t n0 = 4u << tx_sz;
+            const uint64_t coef_bytes = t != NO_TOK ? sizeof(rv9_tok) + 4ull * pf.toks[t].n_coef : 0;
             if (is_inter) {
-              if (t != NO_TOK) res_.push_back(ResItem{t, bi});
+              if (t != NO_TOK) {
+                res_.push_back(ResItem{t, bi});
+                fw->kbytes[K_INTER_RES] += coef_bytes + 2 * n0 * n0 * bps;
+              }
             } else {
               int mode = plane ? b.uv_mode : (b.mi_size >= BLOCK_8X8 ? b.y_mode : b.sub_modes[block_idx]);
               uint8_t fl = (uint8_t)((avail_l || x > 0 ? 1 : 0) | (avail_u || y > 0 ? 2 : 0) | (x + step < n4w ? 4 : 0));
               intra_.push_back(IntraItem{bi, t, (uint16_t)start_x, (uint16_t)start_y, (uint8_t)plane, (uint8_t)tx_sz,
                                          (uint8_t)mode, fl});
+              fw->kbytes[K_INTRA] += (n0 * n0 + 3 * n0 + 1) * bps + coef_bytes;
             }
           }
           ++block_idx;
         }
     }
   }
-  uint64_t out_bytes = (uint64_t)d.mi_cols * 8 * d.mi_rows * 8 * bps;
-  out_bytes += 2 * (((uint64_t)d.mi_cols * 8) >> d.ss_x) * (((uint64_t)d.mi_rows * 8) >> d.ss_y) * bps;
-  uint64_t rec_bytes = pf.blocks.size() * sizeof(rv9_block) + pf.toks.size() * sizeof(rv9_tok) + pf.coefs.size() * 4;
-  alg_bytes += out_bytes + ref_bytes + rec_bytes;
+  const uint64_t mi_w = (uint64_t)d.mi_cols * 8, mi_h = (uint64_t)d.mi_rows * 8;
+  const uint64_t area = (mi_w * mi_h + 2 * (mi_w >> d.ss_x) * (mi_h >> d.ss_y)) * bps;
+  if (d.lf_level) {
+    fw->kbytes[K_LF] = 2 * area;
+    fw->kbytes[K_LF_MI] = pf.blocks.size() * sizeof(rv9_block) + (uint64_t)d.mi_cols * d.mi_rows * 4;
+  }
+  fw->kbytes[K_INTRA_MARK] = intra_.size() * sizeof(IntraItem);
+  // The frame's algorithmic bytes: records read once, reference samples
+  // predicted from, and the reconstructed samples written once.
+  uint64_t ref_bytes = fw->kbytes[K_INTER];
+  for (const InterUnit& u : units_) ref_bytes -= (uint64_t)u.w4 * u.h4 * 16 * bps;  // minus the outputs
+  fw->total_bytes = pf.blocks.size() * sizeof(rv9_block) + pf.toks.size() * sizeof(rv9_tok) +
+                    pf.coefs.size() * 4 + ref_bytes + area;
+  size_t base = align256(out->size());
+  out->resize(base);
+  fw->o_blocks = put(out, pf.blocks.data(), pf.blocks.size());
+  fw->o_toks = put(out, pf.toks.data(), pf.toks.size());
+  fw->o_coefs = put(out, pf.coefs.data(), pf.coefs.size());
+  fw->o_units = put(out, units_.data(), units_.size());
+  fw->o_res = put(out, res_.data(), res_.size());
+  fw->o_intra = put(out, intra_.data(), intra_.size());
+  out->resize(align256(out->size()));
+  fw->bytes = out->size() - base;
+  fw->n_blocks = (uint32_t)pf.blocks.size();
+  fw->n_toks = (uint32_t)pf.toks.size();
+  fw->n_coefs = (uint32_t)pf.coefs.size();
+  fw->n_units = (uint32_t)units_.size();
+  fw->n_res = (uint32_t)res_.size();
+  fw->n_intra = (uint32_t)intra_.size();
 }
 
-static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+void Engine::hook(void* ctx, int kernel, int phase) {
+  Engine* e = (Engine*)ctx;
+  if (e->kev_used_ == e->kev_.size()) {
+    cudaEvent_t ev;
+    cudaEventCreate(&ev);
+    e->kev_.push_back(ev);
+    e->kev_kernel_.push_back(0);
+  }
+  size_t i = e->kev_used_++;
+  e->kev_kernel_[i] = kernel;
+  cudaEventRecord(e->kev_[i], e->stream_);
+  if (phase == 0 && e->cur_fw_) e->kstats[kernel].bytes += e->cur_fw_->kbytes[kernel];
+}
 
-rv9::Status Engine::recon(rv9::ParsedFrame& pf, DevFrame** shown, std::string* err) {
+void Engine::collect_kernel_events() {
+  cudaStreamSynchronize(stream_);
+  for (size_t i = 0; i + 1 < kev_used_; i += 2) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, kev_[i], kev_[i + 1]);
+    KernelStat& s = kstats[kev_kernel_[i]];
+    s.ms += ms;
+    s.launches += 1;
+  }
+  kev_used_ = 0;
+}
+
+rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
+                              std::string* err) {
   *shown = nullptr;
-  if (pf.show_existing) {
-    *shown = slots_[pf.show_slot];
+  if (fw.show_existing) {
+    *shown = slots_[fw.show_slot];
     if (!*shown) {
       *err = "show_existing_frame of an empty slot";
       return rv9::ST_BITSTREAM;
     }
     return rv9::ST_OK;
   }
-  const rv9_frame_desc& d = pf.desc;
+  const rv9_frame_desc& d = fw.desc;
   DevFrame* cur = alloc_frame(d);
   if (!cur) {
     *err = "out of device memory for a frame";
@@ -246,43 +323,25 @@ rv9::Status Engine::recon(rv9::ParsedFrame& pf, DevFrame** shown, std::string* e
   cur->color_range = d.color_range;
   cur->render_w = d.render_width;
   cur->render_h = d.render_height;
-  build_work(pf);
-  // Stage records and work lists in one pinned buffer, one copy.
-  size_t o_blocks = 0;
-  size_t o_toks = align256(o_blocks + pf.blocks.size() * sizeof(rv9_block));
-  size_t o_coefs = align256(o_toks + pf.toks.size() * sizeof(rv9_tok));
-  size_t o_units = align256(o_coefs + pf.coefs.size() * 4);
-  size_t o_res = align256(o_units + units_.size() * sizeof(InterUnit));
-  size_t o_intra = align256(o_res + res_.size() * sizeof(ResItem));
-  size_t total = align256(o_intra + intra_.size() * sizeof(IntraItem));
-  if (!ensure_scratch(total, err)) return rv9::ST_DEVICE;
-  memcpy(h_scratch_ + o_blocks, pf.blocks.data(), pf.blocks.size() * sizeof(rv9_block));
-  memcpy(h_scratch_ + o_toks, pf.toks.data(), pf.toks.size() * sizeof(rv9_tok));
-  memcpy(h_scratch_ + o_coefs, pf.coefs.data(), pf.coefs.size() * 4);
-  memcpy(h_scratch_ + o_units, units_.data(), units_.size() * sizeof(InterUnit));
-  memcpy(h_scratch_ + o_res, res_.data(), res_.size() * sizeof(ResItem));
-  memcpy(h_scratch_ + o_intra, intra_.data(), intra_.size() * sizeof(IntraItem));
-  CK(cudaMemcpyAsync(d_scratch_, h_scratch_, total, cudaMemcpyHostToDevice, stream_));
-  // Loop filter scratch.
   size_t mi_len = (size_t)d.mi_cols * d.mi_rows;
   if (mi_len > lf_mi_cap_) {
+    CK(cudaStreamSynchronize(stream_));
     cudaFree(d_lf_mi_);
     CK(cudaMalloc(&d_lf_mi_, mi_len * 4));
     lf_mi_cap_ = mi_len;
   }
   size_t n_sb = (size_t)d.sb64_cols * d.sb64_rows;
   if (n_sb > sb_cap_) {
+    CK(cudaStreamSynchronize(stream_));
     cudaFree(d_sb_done_);
     CK(cudaMalloc(&d_sb_done_, n_sb * 4));
     CK(cudaMemsetAsync(d_sb_done_, 0, n_sb * 4, stream_));
     sb_cap_ = n_sb;
   }
-  ++epoch_;
-  if (epoch_ == 0) {
+  if (++epoch_ == 0) {
     CK(cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_));
     epoch_ = 1;
   }
-  // The frame's kernel arguments.
   KFrame k;
   memset(&k, 0, sizeof k);
   for (int p = 0; p < 3; ++p) {
@@ -295,7 +354,7 @@ rv9::Status Engine::recon(rv9::ParsedFrame& pf, DevFrame** shown, std::string* e
   }
   if (!d.frame_is_intra) {
     for (int i = 0; i < 3; ++i) {
-      DevFrame* r = slots_[pf.ref_slot[i]];
+      DevFrame* r = slots_[fw.ref_slot[i]];
       if (!r) {
         *err = "reference to an empty slot";
         return rv9::ST_BITSTREAM;
@@ -324,30 +383,29 @@ rv9::Status Engine::recon(rv9::ParsedFrame& pf, DevFrame** shown, std::string* e
   k.legacy_uv = d.legacy_uv;
   // Quantiser per segment (reference qindex + reconstruct's lookups).
   int bd_idx = (d.bit_depth - 8) >> 1;
+  auto cq = [](int v) { return std::min(std::max(v, 0), 255); };
   for (int seg = 0; seg < 8; ++seg) {
     int q = d.base_q_idx;
     if (d.seg.enabled && d.seg.feature_enabled[seg][SEG_LVL_ALT_Q]) {
       int data = d.seg.feature_data[seg][SEG_LVL_ALT_Q];
       if (!d.seg.abs_or_delta_update) data += d.base_q_idx;
-      q = std::min(std::max(data, 0), 255);
+      q = cq(data);
     }
-    auto cq = [](int v) { return std::min(std::max(v, 0), 255); };
     k.dc_q[seg][0] = vp9t_dc_qlookup[bd_idx][cq(q + d.delta_q_y_dc)];
     k.ac_q[seg][0] = vp9t_ac_qlookup[bd_idx][cq(q)];
     k.dc_q[seg][1] = vp9t_dc_qlookup[bd_idx][cq(q + d.delta_q_uv_dc)];
     k.ac_q[seg][1] = vp9t_ac_qlookup[bd_idx][cq(q + d.delta_q_uv_ac)];
   }
-  k.blocks = (const rv9_block*)(d_scratch_ + o_blocks);
-  k.toks = (const rv9_tok*)(d_scratch_ + o_toks);
-  k.coefs = (const uint32_t*)(d_scratch_ + o_coefs);
-  k.units = (const InterUnit*)(d_scratch_ + o_units);
-  k.n_units = (int32_t)units_.size();
-  k.res = (const ResItem*)(d_scratch_ + o_res);
-  k.n_res = (int32_t)res_.size();
-  k.intra = (const IntraItem*)(d_scratch_ + o_intra);
-  k.n_intra = (int32_t)intra_.size();
-  // Loop filter levels and limits (8.8.1; reference loopfilter.rs:15-47,
-  // 135-170).
+  k.blocks = (const rv9_block*)(d_base + fw.o_blocks);
+  k.toks = (const rv9_tok*)(d_base + fw.o_toks);
+  k.coefs = (const uint32_t*)(d_base + fw.o_coefs);
+  k.units = (const InterUnit*)(d_base + fw.o_units);
+  k.n_units = (int32_t)fw.n_units;
+  k.res = (const ResItem*)(d_base + fw.o_res);
+  k.n_res = (int32_t)fw.n_res;
+  k.intra = (const IntraItem*)(d_base + fw.o_intra);
+  k.n_intra = (int32_t)fw.n_intra;
+  // Loop filter levels and limits (8.8.1).
   k.lf_on = d.lf_level != 0;
   if (k.lf_on) {
     int n_shift = d.lf_level >> 5;
@@ -384,38 +442,52 @@ rv9::Status Engine::recon(rv9::ParsedFrame& pf, DevFrame** shown, std::string* e
   k.counters = d_counters_;
   k.error = d_counters_ + 2;
   CK(cudaMemsetAsync(d_counters_, 0, 8, stream_));
-  CK(cudaEventRecord(ev0_, stream_));
   int L = 0;
-  CK(launch_frame(k, (int)pf.blocks.size(), stream_, n_sm_, &L));
-  CK(cudaEventRecord(ev1_, stream_));
+  cur_fw_ = &fw;
+  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this));
+  cur_fw_ = nullptr;
+  // The device's error word, read at the next sync.
+  CK(cudaMemcpyAsync(h_error_ + 1, d_counters_ + 2, 4, cudaMemcpyDeviceToHost, stream_));
   launches += L;
   ++frames;
-  // The staging buffer is reused by the next frame: wait for the copy (the
-  // kernels keep running).
-  CK(cudaEventSynchronize(ev0_));
-  // Device time of the previous frames' kernels is accumulated lazily.
-  float ms = 0;
-  CK(cudaEventSynchronize(ev1_));
-  CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
-  device_ms += ms;
-  int32_t dev_err = 0;
-  CK(cudaMemcpy(&dev_err, d_counters_ + 2, 4, cudaMemcpyDeviceToHost));
-  if (dev_err) {
-    *err = dev_err == 1 ? "intra wavefront wait timed out" : "loop filter wait timed out";
-    // Leave the cell maps consistent for the next frame.
-    cudaMemsetAsync(cur->base, 0, cur->bytes, stream_);
-    cudaMemsetAsync(d_counters_, 0, 64, stream_);
-    return rv9::ST_DEVICE;
-  }
+  alg_bytes += fw.total_bytes;
   // Reference update (8.10 step 1).
   for (int i = 0; i < 8; ++i)
-    if ((pf.refresh_mask >> i) & 1) {
-      release_ref(slots_[i]);
+    if ((fw.refresh_mask >> i) & 1) {
+      if (slots_[i]) --slots_[i]->refs;
       slots_[i] = cur;
       ++cur->refs;
     }
-  if (pf.show_frame) *shown = cur;
+  if (fw.show_frame) *shown = cur;
   return rv9::ST_OK;
+}
+
+rv9::Status Engine::recon(const rv9::ParsedFrame& pf, DevFrame** shown, std::string* err) {
+  FrameWork fw;
+  host_work_.clear();
+  build_work(pf, &fw, &host_work_);
+  if (pf.show_existing) return run_frame(fw, nullptr, false, shown, err);
+  // Stage the bytes in the pinned buffer of this turn (its previous copy
+  // done), one copy to the device.
+  int s = stage_;
+  stage_ ^= 1;
+  CK(cudaEventSynchronize(stage_ev_[s]));
+  if (fw.bytes > stage_cap_[s]) {
+    size_t cap = std::max(fw.bytes, stage_cap_[s] * 3 / 2);
+    CK(cudaStreamSynchronize(stream_));
+    cudaFree(d_stage_[s]);
+    cudaFreeHost(h_stage_[s]);
+    d_stage_[s] = nullptr;
+    h_stage_[s] = nullptr;
+    stage_cap_[s] = 0;
+    CK(cudaMalloc(&d_stage_[s], cap));
+    CK(cudaMallocHost(&h_stage_[s], cap));
+    stage_cap_[s] = cap;
+  }
+  memcpy(h_stage_[s], host_work_.data(), fw.bytes);
+  CK(cudaMemcpyAsync(d_stage_[s], h_stage_[s], fw.bytes, cudaMemcpyHostToDevice, stream_));
+  CK(cudaEventRecord(stage_ev_[s], stream_));
+  return run_frame(fw, d_stage_[s], false, shown, err);
 }
 
 rv9::Status Engine::download_async(DevFrame* f, uint8_t* dst, std::string* err) {
@@ -431,15 +503,64 @@ rv9::Status Engine::download_async(DevFrame* f, uint8_t* dst, std::string* err) 
   return rv9::ST_OK;
 }
 
-rv9::Status Engine::download(DevFrame* f, uint8_t* dst, std::string* err) {
-  rv9::Status st = download_async(f, dst, err);
-  if (st != rv9::ST_OK) return st;
-  return sync(err);
-}
-
 rv9::Status Engine::sync(std::string* err) {
   CK(cudaStreamSynchronize(stream_));
+  if (h_error_[1]) {
+    int code = h_error_[1];
+    h_error_[1] = 0;
+    *err = code == 1 ? "intra wavefront wait timed out" : "loop filter wait timed out";
+    // Leave the cell maps and counters consistent for what follows.
+    for (DevFrame* f : pool_) cudaMemsetAsync(f->cells[0], 0, (uint8_t*)f->base + f->bytes - f->cells[0], stream_);
+    cudaMemsetAsync(d_counters_, 0, 64, stream_);
+    cudaStreamSynchronize(stream_);
+    return rv9::ST_DEVICE;
+  }
   return rv9::ST_OK;
+}
+
+rv9::Status Engine::sequence_load(const std::vector<rv9::ParsedFrame>& frames, Sequence* seq, std::string* err) {
+  std::vector<uint8_t> host;
+  seq->frames.resize(frames.size());
+  seq->luma_samples = 0;
+  for (size_t i = 0; i < frames.size(); ++i) {
+    build_work(frames[i], &seq->frames[i], &host);
+    const rv9::ParsedFrame& pf = frames[i];
+    if (pf.show_existing || pf.show_frame) {
+      // Visible luma of the shown frame (show_existing shows a slot of the
+      // same stream: the size of the frame last shown is a fair stand-in).
+      seq->luma_samples += pf.show_existing ? 0 : (uint64_t)pf.desc.width * pf.desc.height;
+    }
+  }
+  seq->bytes = host.size();
+  CK(cudaMalloc(&seq->d_data, std::max<size_t>(host.size(), 256)));
+  CK(cudaMemcpy(seq->d_data, host.data(), host.size(), cudaMemcpyHostToDevice));
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::sequence_run(const Sequence& seq, bool per_kernel, float* ms, std::string* err) {
+  reset_slots();
+  CK(cudaEventRecord(ev0_, stream_));
+  for (const FrameWork& fw : seq.frames) {
+    DevFrame* shown = nullptr;
+    rv9::Status st = run_frame(fw, seq.d_data, per_kernel, &shown, err);
+    if (st != rv9::ST_OK) return st;
+  }
+  CK(cudaEventRecord(ev1_, stream_));
+  rv9::Status st = sync(err);
+  if (st != rv9::ST_OK) return st;
+  CK(cudaEventElapsedTime(ms, ev0_, ev1_));
+  device_ms += *ms;
+  if (per_kernel) collect_kernel_events();
+  return rv9::ST_OK;
+}
+
+void Engine::sequence_free(Sequence* seq) {
+  if (seq->d_data) {
+    cudaStreamSynchronize(stream_);
+    cudaFree(seq->d_data);
+  }
+  seq->d_data = nullptr;
+  seq->frames.clear();
 }
 
 }  // namespace rv9g

@@ -13,7 +13,15 @@
 
 namespace rv9g {
 
-cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches);
+// Kernels of a frame, for per-kernel timing and byte accounting.
+enum KernelId { K_ZERO_PAD = 0, K_LF_MI, K_INTRA_MARK, K_INTER, K_INTER_RES, K_INTRA, K_LF, K_COUNT };
+extern const char* const kKernelNames[K_COUNT];
+
+// Called around each launch when timing per kernel: phase 0 before, 1 after.
+typedef void (*LaunchHook)(void* ctx, int kernel, int phase);
+
+cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
+                         void* hook_ctx);
 cudaError_t upload_filters(const int16_t* f);
 
 // A decoded frame in device memory: three SB-aligned planes of 1 byte per
@@ -28,17 +36,38 @@ struct DevFrame {
   int32_t pheight[3] = {0, 0, 0};  // SB-aligned rows
   uint8_t* cells[3] = {nullptr, nullptr, nullptr};
   int32_t cell_stride[3] = {0, 0, 0};
-  int refs = 0;             // reference slots holding it
-  bool busy = false;        // being reconstructed or copied out
-  // Output metadata.
+  int refs = 0;  // reference slots holding it
   uint8_t color_space = 1, color_range = 0;
   uint32_t render_w = 0, render_h = 0;
-  cudaEvent_t ready = nullptr;  // recorded when reconstruction is enqueued
   size_t bps() const { return bit_depth > 8 ? 2 : 1; }
 };
 
-struct HostFrameOut {
-  DevFrame* f;
+// One frame's work, staged in a byte buffer (host, then device): the records
+// and the work lists built from them, at the given offsets.
+struct FrameWork {
+  rv9_frame_desc desc;
+  bool show_existing = false, show_frame = false;
+  int show_slot = 0;
+  uint8_t refresh_mask = 0;
+  int ref_slot[3] = {0, 0, 0};
+  uint32_t n_blocks = 0, n_toks = 0, n_coefs = 0, n_units = 0, n_res = 0, n_intra = 0;
+  size_t o_blocks = 0, o_toks = 0, o_coefs = 0, o_units = 0, o_res = 0, o_intra = 0, bytes = 0;
+  uint64_t kbytes[K_COUNT] = {0};  // algorithmic bytes per kernel
+  uint64_t total_bytes = 0;        // algorithmic bytes of the frame
+};
+
+// Parsed frames resident in device memory, for repeated reconstruction.
+struct Sequence {
+  std::vector<FrameWork> frames;
+  uint8_t* d_data = nullptr;
+  size_t bytes = 0;
+  uint64_t luma_samples = 0;  // visible, shown frames
+};
+
+struct KernelStat {
+  uint64_t launches = 0;
+  double ms = 0;
+  uint64_t bytes = 0;
 };
 
 class Engine {
@@ -46,46 +75,66 @@ class Engine {
   Engine() = default;
   ~Engine();
   bool init(int device, std::string* err);
-  // Reconstructs a parsed frame (or handles show_existing); returns the frame
-  // to show (or null) — valid until the next call.
-  rv9::Status recon(rv9::ParsedFrame& pf, DevFrame** shown, std::string* err);
+  // Reconstructs a parsed frame (or handles show_existing); the frame to show
+  // (or null) stays valid until the next call. Work is queued; errors of the
+  // device waits surface at the next sync().
+  rv9::Status recon(const rv9::ParsedFrame& pf, DevFrame** shown, std::string* err);
   // Copies the visible planes of `f`, packed (the reference Frame layout),
-  // into host memory `dst` (pinned or not) on the engine's stream; waits.
-  rv9::Status download(DevFrame* f, uint8_t* dst, std::string* err);
-  // Enqueues the packed copy of `f` into `dst` without waiting.
+  // into host memory `dst` on the engine's stream (queued).
   rv9::Status download_async(DevFrame* f, uint8_t* dst, std::string* err);
   rv9::Status sync(std::string* err);
   static size_t packed_bytes(const DevFrame* f);
 
+  // Device-resident sequences.
+  rv9::Status sequence_load(const std::vector<rv9::ParsedFrame>& frames, Sequence* seq, std::string* err);
+  // Reconstructs every frame of `seq` from scratch (empty slots first);
+  // returns the CUDA-event time of the whole run.
+  rv9::Status sequence_run(const Sequence& seq, bool per_kernel, float* ms, std::string* err);
+  void sequence_free(Sequence* seq);
+  DevFrame* slot(int i) const { return slots_[i]; }
+
   // Stats.
   double device_ms = 0;
   uint64_t frames = 0, alg_bytes = 0, launches = 0;
+  KernelStat kstats[K_COUNT];
   cudaStream_t stream() const { return stream_; }
 
  private:
   DevFrame* alloc_frame(const rv9_frame_desc& d);
-  void release_ref(DevFrame* f);
-  bool ensure_scratch(size_t bytes, std::string* err);
-  void build_work(const rv9::ParsedFrame& pf);
+  void build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<uint8_t>* out);
+  rv9::Status run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
+                        std::string* err);
+  void reset_slots();
+  static void hook(void* ctx, int kernel, int phase);
+  void collect_kernel_events();
 
   int device_ = 0;
   int n_sm_ = 148;
   cudaStream_t stream_ = nullptr;
   std::vector<DevFrame*> pool_;
   DevFrame* slots_[8] = {nullptr};
-  // Device scratch for one frame's records and work lists, and its pinned
-  // host staging copy.
-  uint8_t* d_scratch_ = nullptr;
-  uint8_t* h_scratch_ = nullptr;
-  size_t scratch_cap_ = 0;
+  // Record staging for recon(): pinned host buffers (double-buffered) and
+  // device buffers.
+  std::vector<uint8_t> host_work_;
+  uint8_t* h_stage_[2] = {nullptr, nullptr};
+  uint8_t* d_stage_[2] = {nullptr, nullptr};
+  size_t stage_cap_[2] = {0, 0};
+  cudaEvent_t stage_ev_[2] = {nullptr, nullptr};
+  int stage_ = 0;
   uint32_t* d_lf_mi_ = nullptr;
   size_t lf_mi_cap_ = 0;
   uint32_t* d_sb_done_ = nullptr;
   size_t sb_cap_ = 0;
   int32_t* d_counters_ = nullptr;  // [0] intra, [1] lf, [2] error
+  int32_t* h_error_ = nullptr;     // pinned copy of the error word
   uint32_t epoch_ = 0;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
-  // Work lists of the current frame.
+  // Per-kernel timing.
+  std::vector<cudaEvent_t> kev_;
+  std::vector<int> kev_kernel_;
+  size_t kev_used_ = 0;
+  const FrameWork* cur_fw_ = nullptr;
+  // Work lists of the frame being built.
   std::vector<InterUnit> units_;
   std::vector<ResItem> res_;
   std::vector<IntraItem> intra_;

@@ -27,6 +27,7 @@
 #include <stdint.h>
 
 #include "dsp_math.cuh"
+#include "engine.h"
 #include "engine_types.h"
 
 namespace rv9g {
@@ -585,36 +586,46 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
 // ---------------------------------------------------------------------------
 // Host-side launch of one frame's chain.
 
-struct LaunchCounts {
-  int n_blocks;
-};
-
 cudaError_t upload_filters(const int16_t* f) { return cudaMemcpyToSymbol(c_filters, f, sizeof(int16_t) * 4 * 16 * 8); }
 
 template <class T, class V>
-static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches) {
+static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches,
+                                  LaunchHook hook, void* hctx) {
   int L = 0;
+  auto mark = [&](int id, int phase) {
+    if (hook) hook(hctx, id, phase);
+  };
   {
     int aw = k.sb64_cols * 64, ah = k.sb64_rows * 64;
     if (k.mi_cols * 8 < aw || k.mi_rows * 8 < ah) {
+      mark(K_ZERO_PAD, 0);
       k_zero_pad<T><<<dim3(64, 3), 256, 0, s>>>(k);
+      mark(K_ZERO_PAD, 1);
       ++L;
     }
   }
   if (k.lf_on && n_blocks > 0) {
+    mark(K_LF_MI, 0);
     k_lf_mi<<<(n_blocks + 127) / 128, 128, 0, s>>>(k, n_blocks);
+    mark(K_LF_MI, 1);
     ++L;
   }
   if (k.n_intra > 0) {
+    mark(K_INTRA_MARK, 0);
     k_intra_mark<<<(k.n_intra + 127) / 128, 128, 0, s>>>(k);
+    mark(K_INTRA_MARK, 1);
     ++L;
   }
   if (k.n_units > 0) {
+    mark(K_INTER, 0);
     k_inter<T><<<k.n_units, kInterThreads, 0, s>>>(k);
+    mark(K_INTER, 1);
     ++L;
   }
   if (k.n_res > 0) {
+    mark(K_INTER_RES, 0);
     k_inter_res<T, V><<<(k.n_res + kResWarps - 1) / kResWarps, 32 * kResWarps, 0, s>>>(k);
+    mark(K_INTER_RES, 1);
     ++L;
   }
   if (k.n_intra > 0) {
@@ -626,22 +637,27 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
     }
     int want = (k.n_intra + kIntraWarps - 1) / kIntraWarps;
     int grid = want < n_sm * 4 ? want : n_sm * 4;
+    mark(K_INTRA, 0);
     k_intra<T, V><<<grid, 32 * kIntraWarps, smem, s>>>(k);
+    mark(K_INTRA, 1);
     ++L;
   }
   if (k.lf_on) {
     int n_sb = k.sb64_cols * k.sb64_rows;
     int grid = n_sb < n_sm * 4 ? n_sb : n_sm * 4;
+    mark(K_LF, 0);
     k_lf<T><<<grid, kLfThreads, 0, s>>>(k);
+    mark(K_LF, 1);
     ++L;
   }
   *launches += L;
   return cudaGetLastError();
 }
 
-cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches) {
-  if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches);
-  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches);
+cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
+                         void* hook_ctx) {
+  if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx);
+  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx);
 }
 
 }  // namespace rv9g

@@ -69,7 +69,14 @@ class CStats(ctypes.Structure):
 # Every symbol include/rv9.h declares.
 EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv9_decoder_set_max_pixels",
            "rv9_decoder_frames_decoded", "rv9_last_error", "rv9_last_global_error", "rv9_decode_all",
-           "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats")
+           "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
+           "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
+           "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_decoder_download_slot", "rv9_kernel_stats")
+
+
+class CKernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
+                ("algorithmic_bytes", ctypes.c_uint64)]
 
 _lib = None
 
@@ -103,9 +110,47 @@ def load_library(path=None):
                                        ctypes.c_size_t, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
                                        ctypes.POINTER(ctypes.c_size_t)]
     lib.rv9_decoder_stats.argtypes = [vp, ctypes.POINTER(CStats), ctypes.c_int]
+    lib.rv9_sequence_load.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t),
+                                      ctypes.c_size_t, ctypes.POINTER(vp)]
+    lib.rv9_sequence_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
+        getattr(lib, name).restype = ctypes.c_uint64
+        getattr(lib, name).argtypes = [vp]
+    lib.rv9_sequence_frames.restype = ctypes.c_uint32
+    lib.rv9_sequence_frames.argtypes = [vp]
+    lib.rv9_sequence_free.argtypes = [vp, vp]
+    lib.rv9_decoder_download_slot.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+    lib.rv9_kernel_stats.restype = ctypes.c_size_t
+    lib.rv9_kernel_stats.argtypes = [vp, ctypes.POINTER(CKernelStat), ctypes.c_size_t, ctypes.c_int]
     if path is None:
         _lib = lib
     return lib
+
+
+class Sequence:
+    """Parsed frames whose records are resident in device memory."""
+
+    def __init__(self, dec, handle):
+        self._dec, self._h = dec, handle
+        L = dec._lib
+        self.frames = L.rv9_sequence_frames(handle)
+        self.luma_samples = L.rv9_sequence_luma_samples(handle)
+        self.algorithmic_bytes = L.rv9_sequence_algorithmic_bytes(handle)
+        self.record_bytes = L.rv9_sequence_record_bytes(handle)
+
+    def run(self, per_kernel=False):
+        """Reconstructs every frame on the device; returns the CUDA-event
+        milliseconds of the run."""
+        ms = ctypes.c_double()
+        st = self._dec._lib.rv9_sequence_run(self._dec._dec, self._h, 1 if per_kernel else 0, ctypes.byref(ms))
+        if st != RV9_OK:
+            _raise(self._dec._lib, self._dec._dec, st)
+        return ms.value
+
+    def free(self):
+        if self._h:
+            self._dec._lib.rv9_sequence_free(self._dec._dec, self._h)
+            self._h = None
 
 
 class Plane:
@@ -205,6 +250,44 @@ class Decoder:
         if st != RV9_OK:
             _raise(self._lib, self._dec, st)
         return nf.value, nb.value
+
+    def decode_packets_to(self, packets, out_ptr, cap):
+        """decode_packets into `cap` bytes of memory at address `out_ptr`
+        (e.g. pinned host memory). Returns (frames, bytes)."""
+        n = len(packets)
+        arr = (ctypes.c_char_p * n)(*packets)
+        lens = (ctypes.c_size_t * n)(*[len(p) for p in packets])
+        nf, nb = ctypes.c_size_t(), ctypes.c_size_t()
+        st = self._lib.rv9_decode_packets(self._dec, arr, lens, n, out_ptr, cap, ctypes.byref(nf), ctypes.byref(nb))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        return nf.value, nb.value
+
+    def load_sequence(self, packets):
+        """Parses `packets` (one stream from its start) and keeps their records
+        in device memory for run_sequence."""
+        n = len(packets)
+        arr = (ctypes.c_char_p * n)(*packets)
+        lens = (ctypes.c_size_t * n)(*[len(p) for p in packets])
+        seq = ctypes.c_void_p()
+        st = self._lib.rv9_sequence_load(self._dec, arr, lens, n, ctypes.byref(seq))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        return Sequence(self, seq)
+
+    def download_slot(self, slot, cap):
+        buf = ctypes.create_string_buffer(cap)
+        n = ctypes.c_size_t()
+        st = self._lib.rv9_decoder_download_slot(self._dec, slot, buf, cap, ctypes.byref(n))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        return buf.raw[:n.value]
+
+    def kernel_stats(self, reset=False):
+        arr = (CKernelStat * 16)()
+        n = self._lib.rv9_kernel_stats(self._dec, arr, 16, 1 if reset else 0)
+        return {a.name.decode(): {"launches": a.launches, "ms": a.ms, "algorithmic_bytes": a.algorithmic_bytes}
+                for a in arr[:min(n, 16)]}
 
     def stats(self, reset=False):
         s = CStats()
