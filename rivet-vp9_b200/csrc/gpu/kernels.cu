@@ -479,16 +479,128 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
 // Loop filter wavefront.
 
 constexpr int kLfThreads = 192;
-constexpr int kLfW = 80;   // smem row pitch: 8 left + 64 + 8 of slack
+constexpr int kLfW = 80;   // tile row pitch (int16): 8 left + 64 + 8 of slack
 constexpr int kLfH = 72;   // 8 above + 64
 
+// Eight samples at a time between a plane (8-sample aligned) and the tile.
+template <class T>
+struct Chunk;
+template <>
+struct Chunk<uint8_t> {
+  static __device__ __forceinline__ void load(const uint8_t* g, int16_t* t) {
+    uint2 v = __ldcg(reinterpret_cast<const uint2*>(g));
+    int4 o;
+    o.x = (int)(v.x & 0xff) | (int)((v.x >> 8) & 0xff) << 16;
+    o.y = (int)((v.x >> 16) & 0xff) | (int)(v.x >> 24) << 16;
+    o.z = (int)(v.y & 0xff) | (int)((v.y >> 8) & 0xff) << 16;
+    o.w = (int)((v.y >> 16) & 0xff) | (int)(v.y >> 24) << 16;
+    *reinterpret_cast<int4*>(t) = o;
+  }
+  static __device__ __forceinline__ void store(uint8_t* g, const int16_t* t) {
+    int4 o = *reinterpret_cast<const int4*>(t);
+    uint2 v;
+    v.x = (uint32_t)(o.x & 0xff) | (uint32_t)((o.x >> 16) & 0xff) << 8 | (uint32_t)(o.y & 0xff) << 16 |
+          (uint32_t)((o.y >> 16) & 0xff) << 24;
+    v.y = (uint32_t)(o.z & 0xff) | (uint32_t)((o.z >> 16) & 0xff) << 8 | (uint32_t)(o.w & 0xff) << 16 |
+          (uint32_t)((o.w >> 16) & 0xff) << 24;
+    __stcg(reinterpret_cast<uint2*>(g), v);
+  }
+};
+template <>
+struct Chunk<uint16_t> {
+  static __device__ __forceinline__ void load(const uint16_t* g, int16_t* t) {
+    *reinterpret_cast<int4*>(t) = __ldcg(reinterpret_cast<const int4*>(g));
+  }
+  static __device__ __forceinline__ void store(uint16_t* g, const int16_t* t) {
+    __stcg(reinterpret_cast<int4*>(g), *reinterpret_cast<const int4*>(t));
+  }
+};
+
+// Vertical edges of one sample row held in registers (the row from 8 samples
+// left of the superblock), left to right.
+__device__ __forceinline__ void lf_row_regs(int16_t* line, const LfEdge (*e)[16], int n_edges, int run, int bd) {
+  int v[72];
+#pragma unroll
+  for (int q = 0; q < 72; q += 8) {
+    int4 w = *reinterpret_cast<const int4*>(line + q);
+    v[q] = (int16_t)(w.x & 0xffff); v[q + 1] = w.x >> 16;
+    v[q + 2] = (int16_t)(w.y & 0xffff); v[q + 3] = w.y >> 16;
+    v[q + 4] = (int16_t)(w.z & 0xffff); v[q + 5] = w.z >> 16;
+    v[q + 6] = (int16_t)(w.w & 0xffff); v[q + 7] = w.w >> 16;
+  }
+#pragma unroll
+  for (int ed = 0; ed < 16; ++ed) {
+    if (ed < n_edges) {
+      LfEdge f = e[ed][run];
+      if (f.fs >= 0) {
+        int* sw = &v[4 * ed];
+        if (4 * ed + 16 <= 72) {
+          lf_line(sw, f.fs, f.limit, f.blimit, f.thresh, bd);
+        } else {
+          // The last edges' windows reach past the tile: only p3..q3 matter.
+          int s[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < 72) ? v[4 * ed + q] : 0;
+          lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            if (4 * ed + q < 72) v[4 * ed + q] = s[q];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 72; q += 8) {
+    int4 w;
+    w.x = (v[q] & 0xffff) | (v[q + 1] << 16);
+    w.y = (v[q + 2] & 0xffff) | (v[q + 3] << 16);
+    w.z = (v[q + 4] & 0xffff) | (v[q + 5] << 16);
+    w.w = (v[q + 6] & 0xffff) | (v[q + 7] << 16);
+    *reinterpret_cast<int4*>(line + q) = w;
+  }
+}
+
+// Horizontal edges of one sample column held in registers (from 8 rows above
+// the superblock), top to bottom.
+__device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16], int n_edges, int run, int bd) {
+  int v[72];
+#pragma unroll
+  for (int q = 0; q < 72; ++q) v[q] = col[q * kLfW];
+#pragma unroll
+  for (int ed = 0; ed < 16; ++ed) {
+    if (ed < n_edges) {
+      LfEdge f = e[ed][run];
+      if (f.fs >= 0) {
+        if (4 * ed + 16 <= 72) {
+          lf_line(&v[4 * ed], f.fs, f.limit, f.blimit, f.thresh, bd);
+        } else {
+          int s[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < 72) ? v[4 * ed + q] : 0;
+          lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            if (4 * ed + q < 72) v[4 * ed + q] = s[q];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 72; ++q) col[q * kLfW] = (int16_t)v[q];
+}
+
+// One superblock (all three planes) per ticket, tickets in raster order.
+// The 64x64 interior of a superblock is untouched by the filtering of earlier
+// superblocks, so it is loaded before waiting; only the strips 8 samples
+// left and above (filtered by (r, c-1) and the row above) are loaded after.
 template <class T>
 __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
-  __shared__ int16_t px[3][kLfH][kLfW];
+  __shared__ __align__(16) int16_t px[3][kLfH][kLfW];
   __shared__ LfEdge edges[3][2][16][16];
   __shared__ int ticket;
   __shared__ int abort_flag;
   const int n_sb = k.sb64_cols * k.sb64_rows;
+  const int bd = k.bit_depth;
   for (;;) {
     if (threadIdx.x == 0) ticket = atomicAdd(&k.counters[1], 1);
     __syncthreads();
@@ -498,10 +610,29 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
     const int sr = t / k.sb64_cols, sc = t - sr * k.sb64_cols;
     const int row = sr * 8, col = sc * 8;
     const LfParams P{k.mi_cols, k.mi_rows, k.ss_x, k.ss_y, k.lf_mi, k.lf_limit, k.lf_blimit, k.lf_thresh};
-    // Edge decisions (independent of samples): before waiting.
+    int nch[3], nrw[3], x0s[3], y0s[3];
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const int sxp = p ? k.ss_x : 0, syp = p ? k.ss_y : 0;
+      nch[p] = (64 >> sxp) / 8 + 1;  // 8-sample chunks per tile row, the left strip included
+      nrw[p] = (64 >> syp) + 8;
+      x0s[p] = (col * 8) >> sxp;
+      y0s[p] = (row * 8) >> syp;
+    }
+    // Edge decisions, and the interior (tile rows >= 8, chunks >= 1).
     for (int i = threadIdx.x; i < 3 * 2 * 256; i += kLfThreads) {
       int plane = i / 512, pass = (i >> 8) & 1, ed = (i >> 4) & 15, rn = i & 15;
       edges[plane][pass][ed][rn] = lf_edge_entry(P, plane, pass, row, col, ed, rn);
+    }
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const T* src = plane_ptr<const T>(k.cur[p]);
+      const int stride = k.cur[p].stride;
+      const int nc = nch[p] - 1, nr = nrw[p] - 8;
+      for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
+        int r = i / nc, c = i - r * nc;
+        Chunk<T>::load(src + (size_t)(y0s[p] + r) * stride + x0s[p] + 8 * c, &px[p][8 + r][8 + 8 * c]);
+      }
     }
     // Wait for (r, c-1) and (r-1, c+1) (or (r-1, c) at the last column).
     if (threadIdx.x == 0) {
@@ -517,64 +648,67 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
             abort_flag = 1;
             break;
           }
-          __nanosleep(64);
+          if (polls > 64) __nanosleep(32);
         }
       }
       __threadfence();
     }
     __syncthreads();
     if (abort_flag) return;
-    // Load the region: rows y0-8 .. y0+63, columns x0-8 .. x0+63 per plane.
-    int rows_p[3], cols_p[3], x0s[3], y0s[3];
-    for (int p = 0; p < 3; ++p) {
-      int sxp = p ? k.ss_x : 0, syp = p ? k.ss_y : 0;
-      rows_p[p] = 64 >> syp;
-      cols_p[p] = 64 >> sxp;
-      x0s[p] = (col * 8) >> sxp;
-      y0s[p] = (row * 8) >> syp;
-    }
+    // The strips: left (tile rows >= 8, chunk 0) and top (rows < 8, chunks >= 1).
+#pragma unroll
     for (int p = 0; p < 3; ++p) {
       const T* src = plane_ptr<const T>(k.cur[p]);
       const int stride = k.cur[p].stride;
-      const int nr = rows_p[p] + 8, nc = cols_p[p] + 8;
-      for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
-        int r = i / nc, c = i - r * nc;
-        int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + c;
-        if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) px[p][r][c] = (int16_t)__ldcg(src + (size_t)gy * stride + gx);
+      const int nl = sc > 0 ? nrw[p] - 8 : 0;
+      const int nt = sr > 0 ? 8 * (nch[p] - 1) : 0;
+      for (int i = threadIdx.x; i < nl + nt; i += kLfThreads) {
+        int r, c;
+        if (i < nl) {
+          r = 8 + i;
+          c = 0;
+        } else {
+          int j = i - nl;
+          r = j / (nch[p] - 1);
+          c = 1 + j - r * (nch[p] - 1);
+        }
+        Chunk<T>::load(src + (size_t)(y0s[p] - 8 + r) * stride + x0s[p] - 8 + 8 * c, &px[p][r][8 * c]);
       }
     }
     __syncthreads();
-    const int bd = k.bit_depth;
-    // Vertical edges, left to right, one thread per sample row.
+    // Vertical edges, one thread per sample row.
     {
-      const int total = rows_p[0] + rows_p[1] + rows_p[2];
+      const int r0 = nrw[0] - 8, r1 = nrw[1] - 8;
+      const int total = r0 + 2 * r1;
       for (int task = threadIdx.x; task < total; task += kLfThreads) {
-        int p = task < rows_p[0] ? 0 : (task < rows_p[0] + rows_p[1] ? 1 : 2);
-        int r = task - (p == 0 ? 0 : (p == 1 ? rows_p[0] : rows_p[0] + rows_p[1]));
-        int n_edges = 16 >> (p ? k.ss_x : 0);
-        lf_vertical_row(&px[p][8 + r][0], edges[p][0], n_edges, r >> 2, bd);
+        int p = task < r0 ? 0 : (task < r0 + r1 ? 1 : 2);
+        int r = task - (p == 0 ? 0 : (p == 1 ? r0 : r0 + r1));
+        lf_row_regs(&px[p][8 + r][0], edges[p][0], 16 >> (p ? k.ss_x : 0), r >> 2, bd);
       }
     }
     __syncthreads();
-    // Horizontal edges, top to bottom, one thread per sample column.
+    // Horizontal edges, one thread per sample column.
     {
-      const int total = cols_p[0] + cols_p[1] + cols_p[2];
+      const int c0 = 8 * (nch[0] - 1), c1 = 8 * (nch[1] - 1);
+      const int total = c0 + 2 * c1;
       for (int task = threadIdx.x; task < total; task += kLfThreads) {
-        int p = task < cols_p[0] ? 0 : (task < cols_p[0] + cols_p[1] ? 1 : 2);
-        int c = task - (p == 0 ? 0 : (p == 1 ? cols_p[0] : cols_p[0] + cols_p[1]));
-        int n_edges = 16 >> (p ? k.ss_y : 0);
-        lf_horizontal_col(&px[p][0][8 + c], kLfW, kLfH, edges[p][1], n_edges, c >> 2, bd);
+        int p = task < c0 ? 0 : (task < c0 + c1 ? 1 : 2);
+        int c = task - (p == 0 ? 0 : (p == 1 ? c0 : c0 + c1));
+        lf_col_regs(&px[p][0][8 + c], edges[p][1], 16 >> (p ? k.ss_y : 0), c >> 2, bd);
       }
     }
     __syncthreads();
+    // Write back everything but the corner, 8 samples at a time.
+#pragma unroll
     for (int p = 0; p < 3; ++p) {
       T* dst = plane_ptr<T>(k.cur[p]);
       const int stride = k.cur[p].stride;
-      const int nr = rows_p[p] + 8, nc = cols_p[p] + 8;
+      const int nc = nch[p], nr = nrw[p];
       for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
         int r = i / nc, c = i - r * nc;
-        int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + c;
-        if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) __stcg(dst + (size_t)gy * stride + gx, (T)px[p][r][c]);
+        int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + 8 * c;
+        if ((r >= 8 || c >= 1) && gy >= 0 && gx >= 0)
+          Chunk<T>::store(dst + (size_t)gy * stride + gx, &px[p][r][8 * c]);
       }
     }
     __threadfence();
