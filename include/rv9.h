@@ -129,6 +129,34 @@ rv9_status rv9_sequence_load(rv9_decoder* dec, const uint8_t* const* packets, co
  * run on the decoder's stream. With per_kernel, each launch is bracketed by
  * events for rv9_kernel_stats. */
 rv9_status rv9_sequence_run(rv9_decoder* dec, rv9_sequence* seq, int per_kernel, double* device_ms);
+/* rv9_sequence_run without allocating. No counterpart in the reference
+ * (whose decoder has no device and no replay): this entry point exists for
+ * callers that must not allocate device memory while they decode — a
+ * serving loop whose HBM is already reserved by its admission budget (a
+ * cudaMalloc there can fail or take memory another stream was promised), or
+ * a latency-bound loop that cannot take the device-wide synchronisation
+ * cudaMalloc and cudaFree imply.
+ *
+ * It reconstructs the sequence exactly as rv9_sequence_run does (per_kernel
+ * off), with two differences. The wavefront scratch (tickets, error word,
+ * superblock done flags, per-8x8 loop-filter records) is a fixed static
+ * device array of 1 MiB, not an allocation: a sequence with a frame needing
+ * more (256 bytes + 4 per 64x64 superblock, rounded up to 256, + 4 per 8x8
+ * block; e.g. 4096x2304 needs 0.57 MiB, 8192x4096 does not fit) is refused
+ * with RV9_INVALID_INPUT before anything runs. And every frame buffer comes
+ * from the decoder's pool: when the pool lacks a frame the run would take
+ * (call rv9_sequence_run on the sequence once first to fill it), the call
+ * returns RV9_INVALID_INPUT before anything runs.
+ *
+ * The first call on a device looks the array's address up with
+ * cudaGetSymbolAddress; make that first call before any CUDA stream capture
+ * begins. The counters and done flags must start at zero for each frame: the
+ * call clears them with cudaMemsetAsync on the decoder's stream before each
+ * frame; the loop-filter records are rewritten whole by each frame. All
+ * calls on one device share the one array, so calls that overlap in time on
+ * the same device (two decoders, or two host threads) race on it and must be
+ * serialised by the caller. */
+rv9_status rv9_sequence_run_noalloc(rv9_decoder* dec, rv9_sequence* seq, double* device_ms);
 uint32_t rv9_sequence_frames(const rv9_sequence* seq);
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* seq);     /* visible luma of shown frames */
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* seq); /* per run */

@@ -183,6 +183,14 @@ rv9_status rv9_sequence_run(rv9_decoder* d, rv9_sequence* s, int per_kernel, dou
   return (rv9_status)st;
 }
 
+rv9_status rv9_sequence_run_noalloc(rv9_decoder* d, rv9_sequence* s, double* device_ms) {
+  if (!d || !s || !device_ms) return RV9_INVALID_INPUT;
+  float ms = 0;
+  rv9::Status st = d->engine.sequence_run_fixed(s->seq, &ms, &d->err);
+  *device_ms = ms;
+  return (rv9_status)st;
+}
+
 uint32_t rv9_sequence_frames(const rv9_sequence* s) { return (uint32_t)s->seq.frames.size(); }
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* s) { return s->seq.luma_samples; }
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* s) {

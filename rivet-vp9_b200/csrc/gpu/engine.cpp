@@ -107,6 +107,7 @@ DevFrame* Engine::alloc_frame(const rv9_frame_desc& d) {
         f->bit_depth == d.bit_depth)
       return f;
   }
+  if (fixed_) return nullptr;  // sequence_run_fixed allocates nothing
   DevFrame* f = new DevFrame;
   f->aw = aw;
   f->ah = ah;
@@ -324,21 +325,26 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   cur->render_w = d.render_width;
   cur->render_h = d.render_height;
   size_t mi_len = (size_t)d.mi_cols * d.mi_rows;
-  if (mi_len > lf_mi_cap_) {
+  if (fixed_) {
+    // Already checked against the array's size; zero the counters and the
+    // done flags (flags then compare against epoch 1).
+    size_t flags = align256((size_t)d.sb64_cols * d.sb64_rows * 4);
+    CK(cudaMemsetAsync(fixed_, 0, 256 + flags, stream_));
+  } else if (mi_len > lf_mi_cap_) {
     CK(cudaStreamSynchronize(stream_));
     cudaFree(d_lf_mi_);
     CK(cudaMalloc(&d_lf_mi_, mi_len * 4));
     lf_mi_cap_ = mi_len;
   }
   size_t n_sb = (size_t)d.sb64_cols * d.sb64_rows;
-  if (n_sb > sb_cap_) {
+  if (!fixed_ && n_sb > sb_cap_) {
     CK(cudaStreamSynchronize(stream_));
     cudaFree(d_sb_done_);
     CK(cudaMalloc(&d_sb_done_, n_sb * 4));
     CK(cudaMemsetAsync(d_sb_done_, 0, n_sb * 4, stream_));
     sb_cap_ = n_sb;
   }
-  if (++epoch_ == 0) {
+  if (!fixed_ && ++epoch_ == 0) {
     CK(cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_));
     epoch_ = 1;
   }
@@ -436,18 +442,27 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
       k.lf_thresh[l] = (uint8_t)(l >> 4);
     }
   }
-  k.lf_mi = d_lf_mi_;
-  k.sb_done = d_sb_done_;
-  k.epoch = epoch_;
-  k.counters = d_counters_;
-  k.error = d_counters_ + 2;
-  CK(cudaMemsetAsync(d_counters_, 0, 8, stream_));
+  if (fixed_) {
+    size_t flags = align256(n_sb * 4);
+    k.counters = (int32_t*)fixed_;
+    k.error = k.counters + 2;
+    k.sb_done = (uint32_t*)(fixed_ + 256);
+    k.lf_mi = (uint32_t*)(fixed_ + 256 + flags);
+    k.epoch = 1;
+  } else {
+    k.lf_mi = d_lf_mi_;
+    k.sb_done = d_sb_done_;
+    k.epoch = epoch_;
+    k.counters = d_counters_;
+    k.error = d_counters_ + 2;
+    CK(cudaMemsetAsync(d_counters_, 0, 8, stream_));
+  }
   int L = 0;
   cur_fw_ = &fw;
   CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this));
   cur_fw_ = nullptr;
   // The device's error word, read at the next sync.
-  CK(cudaMemcpyAsync(h_error_ + 1, d_counters_ + 2, 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(h_error_ + 1, k.error, 4, cudaMemcpyDeviceToHost, stream_));
   launches += L;
   ++frames;
   alg_bytes += fw.total_bytes;
@@ -552,6 +567,90 @@ rv9::Status Engine::sequence_run(const Sequence& seq, bool per_kernel, float* ms
   device_ms += *ms;
   if (per_kernel) collect_kernel_events();
   return rv9::ST_OK;
+}
+
+size_t fixed_scratch_need(uint32_t mi_cols, uint32_t mi_rows, uint32_t sb64_cols, uint32_t sb64_rows) {
+  return 256 + align256((size_t)sb64_cols * sb64_rows * 4) + (size_t)mi_cols * mi_rows * 4;
+}
+
+// Replays alloc_frame's choices over the sequence with reference counts only:
+// true when every frame the run takes is already in the pool.
+bool Engine::pool_covers(const Sequence& seq) {
+  DevFrame* sim_slots[8] = {nullptr};
+  for (DevFrame* f : pool_) f->sim_refs = 0;
+  for (const FrameWork& fw : seq.frames) {
+    if (fw.show_existing) continue;
+    const rv9_frame_desc& d = fw.desc;
+    uint32_t aw = d.sb64_cols * 64, ah = d.sb64_rows * 64;
+    DevFrame* cur = nullptr;
+    for (DevFrame* f : pool_) {
+      if (f->sim_refs == 0 && f->aw == aw && f->ah == ah && f->ss_x == d.ss_x && f->ss_y == d.ss_y &&
+          f->bit_depth == d.bit_depth) {
+        cur = f;
+        break;
+      }
+    }
+    if (!cur) return false;
+    for (int i = 0; i < 8; ++i)
+      if ((fw.refresh_mask >> i) & 1) {
+        if (sim_slots[i]) --sim_slots[i]->sim_refs;
+        sim_slots[i] = cur;
+        ++cur->sim_refs;
+      }
+  }
+  return true;
+}
+
+rv9::Status Engine::sequence_run_fixed(const Sequence& seq, float* ms, std::string* err) {
+  for (const FrameWork& fw : seq.frames) {
+    if (fw.show_existing) continue;
+    const rv9_frame_desc& d = fw.desc;
+    if (fixed_scratch_need(d.mi_cols, d.mi_rows, d.sb64_cols, d.sb64_rows) > kFixedScratchBytes) {
+      *err = "frame too large for the fixed scratch array (1 MiB: 256 + 4 per superblock + 4 per 8x8 block)";
+      return rv9::ST_INVALID_INPUT;
+    }
+  }
+  int prev = -1;
+  CK(cudaGetDevice(&prev));
+  if (prev != device_) CK(cudaSetDevice(device_));
+  void* scratch = nullptr;
+  cudaError_t rc = fixed_scratch_address(device_, &scratch);
+  rv9::Status st = rv9::ST_OK;
+  if (rc != cudaSuccess) {
+    *err = std::string("cudaGetSymbolAddress of the fixed scratch: ") + cudaGetErrorString(rc);
+    st = rv9::ST_DEVICE;
+  } else {
+    // Slots are emptied first, as in sequence_run; the pool is checked
+    // against the frames the run will take.
+    reset_slots();
+    if (!pool_covers(seq)) {
+      *err = "the frame pool lacks frames this sequence needs (allocating nothing, it reuses the frames an "
+             "earlier rv9_sequence_run of the sequence left in the pool)";
+      st = rv9::ST_INVALID_INPUT;
+    }
+  }
+  if (st == rv9::ST_OK) {
+    fixed_ = (uint8_t*)scratch;
+    rc = cudaEventRecord(ev0_, stream_);
+    for (size_t i = 0; rc == cudaSuccess && st == rv9::ST_OK && i < seq.frames.size(); ++i) {
+      DevFrame* shown = nullptr;
+      st = run_frame(seq.frames[i], seq.d_data, false, &shown, err);
+    }
+    fixed_ = nullptr;
+    if (rc == cudaSuccess && st == rv9::ST_OK) rc = cudaEventRecord(ev1_, stream_);
+    if (rc != cudaSuccess) {
+      *err = cudaGetErrorString(rc);
+      st = rv9::ST_DEVICE;
+    }
+    if (st == rv9::ST_OK) st = sync(err);
+    if (st == rv9::ST_OK && (rc = cudaEventElapsedTime(ms, ev0_, ev1_)) != cudaSuccess) {
+      *err = cudaGetErrorString(rc);
+      st = rv9::ST_DEVICE;
+    }
+    if (st == rv9::ST_OK) device_ms += *ms;
+  }
+  if (prev != device_) cudaSetDevice(prev);
+  return st;
 }
 
 void Engine::sequence_free(Sequence* seq) {

@@ -24,6 +24,16 @@ cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm
                          void* hook_ctx);
 cudaError_t upload_filters(const int16_t* f);
 
+// The fixed wavefront scratch: a static device array of this many bytes.
+// Layout: [0, 256) counters (the intra ticket, the loop-filter ticket, the
+// error word), then the superblock done flags (4 bytes each, 256-byte
+// aligned extent), then the per-8x8 loop-filter records (4 bytes each).
+constexpr size_t kFixedScratchBytes = (size_t)1 << 20;
+size_t fixed_scratch_need(uint32_t mi_cols, uint32_t mi_rows, uint32_t sb64_cols, uint32_t sb64_rows);
+// Its device address on `device` (which must be current); the first call for
+// a device looks it up with cudaGetSymbolAddress.
+cudaError_t fixed_scratch_address(int device, void** ptr);
+
 // A decoded frame in device memory: three SB-aligned planes of 1 byte per
 // sample at 8 bits, 2 above, and the intra cell map.
 struct DevFrame {
@@ -37,6 +47,7 @@ struct DevFrame {
   uint8_t* cells[3] = {nullptr, nullptr, nullptr};
   int32_t cell_stride[3] = {0, 0, 0};
   int refs = 0;  // reference slots holding it
+  int sim_refs = 0;  // scratch count of Engine::pool_covers
   uint8_t color_space = 1, color_range = 0;
   uint32_t render_w = 0, render_h = 0;
   size_t bps() const { return bit_depth > 8 ? 2 : 1; }
@@ -90,6 +101,11 @@ class Engine {
   // Reconstructs every frame of `seq` from scratch (empty slots first);
   // returns the CUDA-event time of the whole run.
   rv9::Status sequence_run(const Sequence& seq, bool per_kernel, float* ms, std::string* err);
+  // Like sequence_run (per_kernel off), allocating nothing: the wavefront
+  // scratch is the fixed static array, and every frame comes from the pool.
+  // Fails before any launch when a frame of the sequence needs more scratch
+  // than the array holds, or the pool lacks a frame the run would take.
+  rv9::Status sequence_run_fixed(const Sequence& seq, float* ms, std::string* err);
   void sequence_free(Sequence* seq);
   DevFrame* slot(int i) const { return slots_[i]; }
 
@@ -105,6 +121,7 @@ class Engine {
   rv9::Status run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
                         std::string* err);
   void reset_slots();
+  bool pool_covers(const Sequence& seq);
   static void hook(void* ctx, int kernel, int phase);
   void collect_kernel_events();
 
@@ -128,6 +145,7 @@ class Engine {
   int32_t* d_counters_ = nullptr;  // [0] intra, [1] lf, [2] error
   int32_t* h_error_ = nullptr;     // pinned copy of the error word
   uint32_t epoch_ = 0;
+  uint8_t* fixed_ = nullptr;  // the fixed scratch, during sequence_run_fixed
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   // Per-kernel timing.
   std::vector<cudaEvent_t> kev_;

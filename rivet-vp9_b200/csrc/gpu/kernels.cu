@@ -26,6 +26,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "dsp_math.cuh"
 #include "engine.h"
 #include "engine_types.h"
@@ -792,6 +794,35 @@ cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm
                          void* hook_ctx) {
   if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx);
   return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Fixed wavefront scratch, for callers that must not allocate device memory.
+//
+// The loop-filter and intra wavefront kernels take their scratch (tickets,
+// error word, superblock done flags, per-8x8 loop-filter records) through
+// KFrame pointers; Engine::sequence_run_fixed points them into this array
+// instead of the engine's allocations. The array is zero at module load.
+// Every caller on a device shares it, so calls that overlap on one device
+// (two decoders, two host threads) race on it.
+static __device__ __align__(256) uint8_t g_fixed_scratch[kFixedScratchBytes];
+
+cudaError_t fixed_scratch_address(int device, void** ptr) {
+  // Resolved once per device, with that device current.
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static void* addr[kMaxDevices] = {nullptr};
+  *ptr = nullptr;
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&p, g_fixed_scratch);
+    if (rc != cudaSuccess) return rc;
+    addr[device] = p;
+  }
+  *ptr = addr[device];
+  return cudaSuccess;
 }
 
 }  // namespace rv9g

@@ -71,7 +71,8 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decoder_frames_decoded", "rv9_last_error", "rv9_last_global_error", "rv9_decode_all",
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
-           "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_decoder_download_slot", "rv9_kernel_stats")
+           "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_decoder_download_slot", "rv9_kernel_stats",
+           "rv9_sequence_run_noalloc")
 
 
 class CKernelStat(ctypes.Structure):
@@ -113,6 +114,7 @@ def load_library(path=None):
     lib.rv9_sequence_load.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t),
                                       ctypes.c_size_t, ctypes.POINTER(vp)]
     lib.rv9_sequence_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.rv9_sequence_run_noalloc.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double)]
     for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
         getattr(lib, name).restype = ctypes.c_uint64
         getattr(lib, name).argtypes = [vp]
@@ -143,6 +145,18 @@ class Sequence:
         milliseconds of the run."""
         ms = ctypes.c_double()
         st = self._dec._lib.rv9_sequence_run(self._dec._dec, self._h, 1 if per_kernel else 0, ctypes.byref(ms))
+        if st != RV9_OK:
+            _raise(self._dec._lib, self._dec._dec, st)
+        return ms.value
+
+    def run_noalloc(self):
+        """run() without allocating device memory (rv9_sequence_run_noalloc):
+        the wavefront scratch is a fixed 1 MiB static device array shared by
+        every such call on the device (overlapping calls race), and the frame
+        buffers come from the decoder's pool, which an earlier run() of this
+        sequence fills. Raises InvalidInputError when either does not suffice."""
+        ms = ctypes.c_double()
+        st = self._dec._lib.rv9_sequence_run_noalloc(self._dec._dec, self._h, ctypes.byref(ms))
         if st != RV9_OK:
             _raise(self._dec._lib, self._dec._dec, st)
         return ms.value
