@@ -157,6 +157,13 @@ rv9_status rv9_sequence_run(rv9_decoder* dec, rv9_sequence* seq, int per_kernel,
  * the same device (two decoders, or two host threads) race on it and must be
  * serialised by the caller. */
 rv9_status rv9_sequence_run_noalloc(rv9_decoder* dec, rv9_sequence* seq, double* device_ms);
+/* Reconstructs seqs[i] on decs[i] for all i at once: every decoder (all
+ * distinct, on one device) runs its sequence on its own CUDA stream, frames
+ * issued round-robin, so independent streams' kernels overlap on the GPU.
+ * *device_ms receives the CUDA-event time from the common start to the last
+ * stream's end. A multi-stream throughput form with no reference counterpart. */
+rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int per_kernel,
+                             double* device_ms);
 uint32_t rv9_sequence_frames(const rv9_sequence* seq);
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* seq);     /* visible luma of shown frames */
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* seq); /* per run */

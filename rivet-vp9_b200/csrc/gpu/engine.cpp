@@ -569,6 +569,59 @@ rv9::Status Engine::sequence_run(const Sequence& seq, bool per_kernel, float* ms
   return rv9::ST_OK;
 }
 
+rv9::Status Engine::run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n, bool per_kernel,
+                                   float* ms, std::string* err) {
+  if (n == 0) {
+    *ms = 0;
+    return rv9::ST_OK;
+  }
+  Engine* e0 = engines[0];
+  for (size_t j = 0; j < n; ++j) {
+    if (engines[j]->device_ != e0->device_) {
+      *err = "decoders on different devices";
+      return rv9::ST_INVALID_INPUT;
+    }
+    for (size_t i = 0; i < j; ++i)
+      if (engines[i] == engines[j]) {
+        *err = "a decoder appears twice";
+        return rv9::ST_INVALID_INPUT;
+      }
+  }
+  // Every stream starts after the start event on engines[0]'s stream.
+  CK(cudaEventRecord(e0->ev0_, e0->stream_));
+  for (size_t j = 0; j < n; ++j) {
+    engines[j]->reset_slots();
+    if (j) CK(cudaStreamWaitEvent(engines[j]->stream_, e0->ev0_, 0));
+  }
+  size_t most = 0;
+  for (size_t j = 0; j < n; ++j) most = std::max(most, seqs[j]->frames.size());
+  for (size_t i = 0; i < most; ++i)
+    for (size_t j = 0; j < n; ++j) {
+      if (i >= seqs[j]->frames.size()) continue;
+      DevFrame* shown = nullptr;
+      rv9::Status st = engines[j]->run_frame(seqs[j]->frames[i], seqs[j]->d_data, per_kernel, &shown, err);
+      if (st != rv9::ST_OK) return st;
+    }
+  // engines[0]'s stream waits for every other stream's end.
+  for (size_t j = 1; j < n; ++j) {
+    CK(cudaEventRecord(engines[j]->ev1_, engines[j]->stream_));
+    CK(cudaStreamWaitEvent(e0->stream_, engines[j]->ev1_, 0));
+  }
+  CK(cudaEventRecord(e0->ev1_, e0->stream_));
+  rv9::Status first = rv9::ST_OK;
+  for (size_t j = 0; j < n; ++j) {
+    rv9::Status st = engines[j]->sync(err);
+    if (first == rv9::ST_OK) first = st;
+  }
+  if (first != rv9::ST_OK) return first;
+  CK(cudaEventElapsedTime(ms, e0->ev0_, e0->ev1_));
+  for (size_t j = 0; j < n; ++j) {
+    engines[j]->device_ms += *ms / n;
+    if (per_kernel) engines[j]->collect_kernel_events();
+  }
+  return rv9::ST_OK;
+}
+
 size_t fixed_scratch_need(uint32_t mi_cols, uint32_t mi_rows, uint32_t sb64_cols, uint32_t sb64_rows) {
   return 256 + align256((size_t)sb64_cols * sb64_rows * 4) + (size_t)mi_cols * mi_rows * 4;
 }

@@ -101,6 +101,14 @@ class Engine {
   // Reconstructs every frame of `seq` from scratch (empty slots first);
   // returns the CUDA-event time of the whole run.
   rv9::Status sequence_run(const Sequence& seq, bool per_kernel, float* ms, std::string* err);
+  // Reconstructs several sequences at once, one per engine (all engines
+  // distinct, on one device), each on its engine's own CUDA stream with
+  // frames issued round-robin, so that the streams' kernels overlap on the
+  // device. *ms is the CUDA-event time from the first launch to the last
+  // completion, on engines[0]'s stream.
+  static rv9::Status run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
+                                    bool per_kernel, float* ms, std::string* err);
+  int device() const { return device_; }
   // Like sequence_run (per_kernel off), allocating nothing: the wavefront
   // scratch is the fixed static array, and every frame comes from the pool.
   // Fails before any launch when a frame of the sequence needs more scratch

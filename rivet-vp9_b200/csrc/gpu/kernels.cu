@@ -591,7 +591,27 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
   for (int q = 0; q < 72; ++q) col[q * kLfW] = (int16_t)v[q];
 }
 
-// One superblock (all three planes) per ticket, tickets in raster order.
+// The superblock of ticket t, tickets in wavefront order: anti-diagonals
+// d = c + 2r in turn, rows ascending within one. Every dependency of (r, c)
+// lies on diagonal d-1 or d-2, so a grid about one diagonal wide keeps every
+// CTA busy, and consecutive tickets are independent.
+__device__ __forceinline__ void lf_ticket_sb(int t, int cols, int rows, int* sr, int* sc) {
+  for (int d = 0;; ++d) {
+    int r_lo = d - cols + 1 > 0 ? (d - cols + 2) >> 1 : 0;
+    int r_hi = (d >> 1) < rows - 1 ? (d >> 1) : rows - 1;
+    int n = r_hi - r_lo + 1;
+    if (n > 0) {
+      if (t < n) {
+        *sr = r_lo + t;
+        *sc = d - 2 * (r_lo + t);
+        return;
+      }
+      t -= n;
+    }
+  }
+}
+
+// One superblock (all three planes) per ticket.
 // The 64x64 interior of a superblock is untouched by the filtering of earlier
 // superblocks, so it is loaded before waiting; only the strips 8 samples
 // left and above (filtered by (r, c-1) and the row above) are loaded after.
@@ -604,9 +624,13 @@ __global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
   const int n_sb = k.sb64_cols * k.sb64_rows;
   const int bd = k.bit_depth;
   for (;;) {
-    if (threadIdx.x == 0) ticket = atomicAdd(&k.counters[1], 1);
+    if (threadIdx.x == 0) {
+      int tk = atomicAdd(&k.counters[1], 1), r = 0, c = 0;
+      if (tk < n_sb) lf_ticket_sb(tk, k.sb64_cols, k.sb64_rows, &r, &c);
+      ticket = tk < n_sb ? r * k.sb64_cols + c : n_sb;
+    }
     __syncthreads();
-    const int t = ticket;
+    const int t = ticket;  // the superblock's raster index
     __syncthreads();
     if (t >= n_sb) return;
     const int sr = t / k.sb64_cols, sc = t - sr * k.sb64_cols;
@@ -779,8 +803,12 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
     ++L;
   }
   if (k.lf_on) {
+    // Two diagonals' worth of CTAs: one filtering, one loading ahead.
     int n_sb = k.sb64_cols * k.sb64_rows;
-    int grid = n_sb < n_sm * 4 ? n_sb : n_sm * 4;
+    int diag = (k.sb64_cols + 1) / 2 < k.sb64_rows ? (k.sb64_cols + 1) / 2 : k.sb64_rows;
+    int grid = 2 * diag + 2;
+    grid = grid < n_sb ? grid : n_sb;
+    grid = grid < n_sm * 3 ? grid : n_sm * 3;
     mark(K_LF, 0);
     k_lf<T><<<grid, kLfThreads, 0, s>>>(k);
     mark(K_LF, 1);

@@ -4,6 +4,7 @@
 #pragma once
 #include <stddef.h>
 #include <stdint.h>
+#include <string.h>
 
 namespace rv9 {
 
@@ -65,15 +66,11 @@ class BoolDecoder {
   inline bool read(int prob) {
     uint32_t split = 1 + (((range_ - 1) * (uint32_t)prob) >> 8);
     uint64_t big = (uint64_t)split << 56;
-    bool bit;
-    if (value_ < big) {
-      range_ = split;
-      bit = false;
-    } else {
-      range_ -= split;
-      value_ -= big;
-      bit = true;
-    }
+    // Branch-free: the decoded bit is data, not control flow.
+    const bool bit = value_ >= big;
+    const uint64_t m = 0 - (uint64_t)bit;
+    range_ = bit ? range_ - split : split;
+    value_ -= big & m;
     int shift = __builtin_clz(range_) - 24;
     range_ <<= shift;
     value_ <<= shift;
@@ -109,6 +106,19 @@ class BoolDecoder {
 
  private:
   inline void fill() {
+    if (end_ - p_ >= 8) {
+      // Whole bytes that fit below the valid bits, from one big-endian load.
+      // The part of the next byte that also lands is ORed in again, at the
+      // same position, by the next fill.
+      uint64_t w;
+      memcpy(&w, p_, 8);
+      w = __builtin_bswap64(w);
+      const int nbytes = (64 - bits_) >> 3;
+      value_ |= w >> bits_;
+      p_ += nbytes;
+      bits_ += nbytes * 8;
+      return;
+    }
     while (bits_ <= 56) {
       if (p_ < end_) {
         value_ |= (uint64_t)(*p_++) << (56 - bits_);

@@ -124,6 +124,20 @@ inline uint8_t pareto(int node, uint8_t prob) {
   return (uint8_t)(((uint32_t)vp9t_pareto_table[x][node - 2] + vp9t_pareto_table[x1][node - 2]) >> 1);
 }
 
+// pareto() for every probability value: row p holds the probabilities of
+// token-tree nodes 2..9 when node 1's probability is p.
+struct ParetoRows {
+  uint8_t row[256][8];
+  ParetoRows() {
+    for (int p = 0; p < 256; ++p)
+      for (int k = 2; k < 10; ++k) row[p][k - 2] = pareto(k, (uint8_t)p);
+  }
+};
+inline const uint8_t* pareto_row(uint8_t prob) {
+  static const ParetoRows rows;
+  return rows.row[prob];
+}
+
 // The scan order of get_scan (spec 6.4.25).
 inline const uint16_t* get_scan(int tx_sz, int tx_type) {
   switch (tx_sz) {
@@ -1379,8 +1393,27 @@ struct TileCoder {
         if (count) counts.more_coefs[tx_sz][ptype][ref_type][band][ctx][more ? 1 : 0] += 1;
         if (!more) break;
       }
-      int token = d.tree(TOKEN_TREE, [&](int node) { return pareto(node, probs[(1 + node) < 2 ? (1 + node) : 2]); },
-                         [&] { return token_of(wc[pos]); });
+      int token;
+      if constexpr (!C::kEncode) {
+        // The token tree unrolled past its first two nodes; the remaining
+        // nodes' probabilities come from one pareto row.
+        BoolDecoder& r = d.bd;
+        if (!r.read(probs[1])) {
+          token = ZERO_TOKEN;
+        } else if (!r.read(probs[2])) {
+          token = 1;  // ONE_TOKEN
+        } else {
+          const uint8_t* pp = pareto_row(probs[2]);
+          int n = 4;
+          do {
+            n = TOKEN_TREE[n + (int)r.read(pp[(n >> 1) - 2])];
+          } while (n > 0);
+          token = -n;
+        }
+      } else {
+        token = d.tree(TOKEN_TREE, [&](int node) { return pareto(node, probs[(1 + node) < 2 ? (1 + node) : 2]); },
+                       [&] { return token_of(wc[pos]); });
+      }
       if (count) counts.token[tx_sz][ptype][ref_type][band][ctx][token < 2 ? token : 2] += 1;
       token_cache[pos] = vp9t_energy_class[token];
       if (token == ZERO_TOKEN) {

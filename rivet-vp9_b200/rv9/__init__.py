@@ -72,7 +72,7 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_decoder_download_slot", "rv9_kernel_stats",
-           "rv9_sequence_run_noalloc")
+           "rv9_sequence_run_noalloc", "rv9_sequences_run")
 
 
 class CKernelStat(ctypes.Structure):
@@ -115,6 +115,8 @@ def load_library(path=None):
                                       ctypes.c_size_t, ctypes.POINTER(vp)]
     lib.rv9_sequence_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.rv9_sequence_run_noalloc.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double)]
+    lib.rv9_sequences_run.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_double)]
     for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
         getattr(lib, name).restype = ctypes.c_uint64
         getattr(lib, name).argtypes = [vp]
@@ -165,6 +167,23 @@ class Sequence:
         if self._h:
             self._dec._lib.rv9_sequence_free(self._dec._dec, self._h)
             self._h = None
+
+
+def run_concurrent(pairs, per_kernel=False):
+    """Reconstructs several (decoder, sequence) pairs at once, each decoder on
+    its own CUDA stream (rv9_sequences_run); returns the CUDA-event
+    milliseconds from the common start to the last stream's end."""
+    if not pairs:
+        return 0.0
+    lib = pairs[0][0]._lib
+    n = len(pairs)
+    decs = (ctypes.c_void_p * n)(*[d._dec for d, _ in pairs])
+    seqs = (ctypes.c_void_p * n)(*[s._h for _, s in pairs])
+    ms = ctypes.c_double()
+    st = lib.rv9_sequences_run(decs, seqs, n, 1 if per_kernel else 0, ctypes.byref(ms))
+    if st != RV9_OK:
+        _raise(lib, pairs[0][0]._dec, st)
+    return ms.value
 
 
 class Plane:
