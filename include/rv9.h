@@ -169,6 +169,10 @@ uint64_t rv9_sequence_luma_samples(const rv9_sequence* seq);     /* visible luma
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* seq); /* per run */
 uint64_t rv9_sequence_record_bytes(const rv9_sequence* seq);      /* device bytes held */
 void rv9_sequence_free(rv9_decoder* dec, rv9_sequence* seq);
+/* A device copy of `src` (its records and work lists) held by `dec`, without
+ * parsing again: many decoders replaying the same content each read their
+ * own records. */
+rv9_status rv9_sequence_clone(rv9_decoder* dec, const rv9_sequence* src, rv9_sequence** out);
 
 /* The frame in reference slot `slot` (0..7), packed like rv9_frame data. */
 rv9_status rv9_decoder_download_slot(rv9_decoder* dec, int slot, uint8_t* out, size_t cap, size_t* bytes);

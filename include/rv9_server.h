@@ -1,0 +1,96 @@
+/*
+ * rv9_server.h — serving many VP9 streams on one GPU.
+ *
+ * No counterpart in the reference, whose Decoder serves one stream per
+ * caller (src/decoder/mod.rs:150-216). This is the continuous-batching form:
+ * an engine holds many live streams, each with its eight reference slots and
+ * frame contexts resident on the device. A stream is admitted when the
+ * engine's HBM budget can hold its reservation, and waits (pending) until
+ * streams close otherwise. Decode requests (packets) are parsed on a pool of
+ * host threads, and each stream's reconstruction runs on its own CUDA stream,
+ * so requests of different streams overlap on the device as they arrive.
+ * Every result is bit-identical to decoding the stream alone with
+ * rv9_decode_all.
+ *
+ * Each completion reports the request's latency: from rv9_submit to the
+ * moment its frames are in host memory.
+ */
+#ifndef RV9_SERVER_H
+#define RV9_SERVER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "rv9.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rv9_engine rv9_engine;
+
+/* An engine on `device` (-1: current) admitting streams within
+ * `hbm_budget_bytes`, with `workers` host threads parsing (0: one per core).
+ * NULL when no usable device is present (rv9_last_global_error says why). */
+rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers);
+/* Closes every stream, waits for their submitted requests, then frees the
+ * engine, with any completions not yet released. */
+void rv9_engine_free(rv9_engine* eng);
+
+/* The largest frame a stream will carry, which sizes its reservation. */
+typedef struct rv9_stream_spec {
+  uint32_t max_width, max_height;
+  uint32_t bit_depth;   /* 8, 10 or 12 */
+  uint32_t ss_x, ss_y;  /* chroma subsampling: 1,1 for 4:2:0; 0,0 for 4:4:4 */
+} rv9_stream_spec;
+
+/* Device bytes the engine reserves for a stream of this spec: its pooled
+ * frames (eight slots and two in flight), record staging and scratch. Needs
+ * no device. */
+uint64_t rv9_stream_reservation(const rv9_stream_spec* spec);
+
+/* Opens a stream; *id receives its handle. The stream is admitted at once
+ * when the budget allows, else it is pending and its requests wait until
+ * other streams close. RV9_UNSUPPORTED when the spec alone exceeds the
+ * budget. */
+rv9_status rv9_stream_open(rv9_engine* eng, const rv9_stream_spec* spec, int64_t* id);
+/* Closes a stream once its submitted requests are done (a pending stream
+ * is admitted in turn first); its reservation then returns to the budget. */
+rv9_status rv9_stream_close(rv9_engine* eng, int64_t id);
+
+/* Queues one packet (a frame or a superframe) for the stream. The packet is
+ * copied; `tag` comes back in its completion. Requests of one stream complete
+ * in submission order. */
+rv9_status rv9_submit(rv9_engine* eng, int64_t id, const uint8_t* packet, size_t len, uint64_t tag);
+
+typedef struct rv9_completion {
+  int64_t stream;
+  uint64_t tag;
+  rv9_status status;    /* RV9_OK or the request's error */
+  uint32_t n_frames;    /* shown frames in frames[] (at most 2) */
+  double submit_ms;     /* submission time, ms since the engine was created */
+  double latency_ms;    /* submission to frames in host memory */
+  rv9_frame frames[2];  /* owned by the engine until rv9_completion_release */
+  void* handle;
+} rv9_completion;
+
+/* Up to `cap` finished requests, in completion order; waits up to
+ * `timeout_ms` for the first (0: no wait). Returns how many were written. */
+size_t rv9_poll(rv9_engine* eng, rv9_completion* out, size_t cap, int timeout_ms);
+/* Returns a completion's frame buffers to its stream. A stream holds four
+ * output buffers: requests wait while all four are out. */
+void rv9_completion_release(rv9_engine* eng, rv9_completion* c);
+
+typedef struct rv9_engine_stats {
+  uint64_t streams_open, streams_pending;
+  uint64_t requests_submitted, requests_completed;
+  uint64_t frames_decoded;
+  uint64_t reserved_bytes, budget_bytes;
+} rv9_engine_stats;
+void rv9_engine_get_stats(rv9_engine* eng, rv9_engine_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RV9_SERVER_H */

@@ -20,10 +20,12 @@ SOURCES = [
     "gpu/kernels.cu",
     "gpu/engine.cpp",
     "api/rv9_api.cpp",
+    "serve/server.cpp",
     "host/parser.cpp",
     "host/probs.cpp",
 ]
 HEADERS = [
+    "api/api_internal.h",
     "gpu/dsp_math.cuh",
     "gpu/engine_types.h",
     "gpu/engine.h",
@@ -49,7 +51,7 @@ def stale():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS]
-    deps += [os.path.join(HERE, "..", "include", h) for h in ("rv9.h", "rv9_records.h")]
+    deps += [os.path.join(HERE, "..", "include", h) for h in ("rv9.h", "rv9_records.h", "rv9_server.h")]
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps)
 

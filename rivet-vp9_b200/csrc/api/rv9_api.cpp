@@ -10,6 +10,7 @@
 
 #include "../../../include/rv9.h"
 #include "../gpu/engine.h"
+#include "api_internal.h"
 #include "../host/parser.h"
 
 struct rv9_decoder {
@@ -21,6 +22,10 @@ struct rv9_decoder {
 };
 
 static thread_local std::string g_global_err;
+
+namespace rv9api {
+void set_global_error(const std::string& msg) { g_global_err = msg; }
+}  // namespace rv9api
 
 static void fill_meta(const rv9g::DevFrame* f, rv9_frame* out) {
   out->width = f->width;
@@ -169,6 +174,20 @@ rv9_status rv9_sequence_load(rv9_decoder* d, const uint8_t* const* pkts, const s
   rv9_sequence* s = new rv9_sequence;
   rv9::Status st = d->engine.sequence_load(frames, &s->seq, &d->err);
   if (st != rv9::ST_OK) {
+    delete s;
+    return (rv9_status)st;
+  }
+  *out = s;
+  return RV9_OK;
+}
+
+rv9_status rv9_sequence_clone(rv9_decoder* d, const rv9_sequence* src, rv9_sequence** out) {
+  if (!d || !src || !out) return RV9_INVALID_INPUT;
+  *out = nullptr;
+  rv9_sequence* s = new rv9_sequence;
+  rv9::Status st = d->engine.sequence_clone(src->seq, &s->seq, &d->err);
+  if (st != rv9::ST_OK) {
+    d->engine.sequence_free(&s->seq);
     delete s;
     return (rv9_status)st;
   }

@@ -622,6 +622,81 @@ rv9::Status Engine::run_concurrent(Engine* const* engines, const Sequence* const
   return rv9::ST_OK;
 }
 
+static rv9_frame_desc geometry_desc(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t bd) {
+  rv9_frame_desc d;
+  memset(&d, 0, sizeof d);
+  d.width = width;
+  d.height = height;
+  d.mi_cols = (width + 7) >> 3;
+  d.mi_rows = (height + 7) >> 3;
+  d.sb64_cols = (d.mi_cols + 7) >> 3;
+  d.sb64_rows = (d.mi_rows + 7) >> 3;
+  d.ss_x = ss_x;
+  d.ss_y = ss_y;
+  d.bit_depth = bd;
+  return d;
+}
+
+size_t Engine::footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t bit_depth,
+                         int n_frames, size_t stage_bytes) {
+  rv9_frame_desc d = geometry_desc(width, height, ss_x, ss_y, bit_depth);
+  uint32_t aw = d.sb64_cols * 64, ah = d.sb64_rows * 64;
+  size_t bps = bit_depth > 8 ? 2 : 1, frame = 0;
+  for (int p = 0; p < 3; ++p) {
+    size_t w = p ? (aw >> ss_x) : aw, h = p ? (ah >> ss_y) : ah;
+    frame += align256(w * h * bps) + align256((w / 4) * (h / 4));
+  }
+  return (size_t)n_frames * frame + 2 * stage_bytes + (size_t)d.mi_cols * d.mi_rows * 4 +
+         (size_t)d.sb64_cols * d.sb64_rows * 4 + 64;
+}
+
+rv9::Status Engine::reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t bit_depth,
+                            int n_frames, size_t stage_bytes, std::string* err) {
+  rv9_frame_desc d = geometry_desc(width, height, ss_x, ss_y, bit_depth);
+  // Distinct frames: hold each one while taking the next.
+  std::vector<DevFrame*> held;
+  for (int i = 0; i < n_frames; ++i) {
+    DevFrame* f = alloc_frame(d);
+    if (!f) {
+      for (DevFrame* h : held) --h->refs;
+      *err = "out of device memory reserving frames";
+      return rv9::ST_DEVICE;
+    }
+    ++f->refs;
+    held.push_back(f);
+  }
+  for (DevFrame* h : held) --h->refs;
+  for (int s = 0; s < 2; ++s)
+    if (stage_bytes > stage_cap_[s]) {
+      CK(cudaStreamSynchronize(stream_));
+      cudaFree(d_stage_[s]);
+      cudaFreeHost(h_stage_[s]);
+      d_stage_[s] = nullptr;
+      h_stage_[s] = nullptr;
+      stage_cap_[s] = 0;
+      CK(cudaMalloc(&d_stage_[s], stage_bytes));
+      CK(cudaMallocHost(&h_stage_[s], stage_bytes));
+      stage_cap_[s] = stage_bytes;
+    }
+  size_t mi_len = (size_t)d.mi_cols * d.mi_rows;
+  if (mi_len > lf_mi_cap_) {
+    CK(cudaStreamSynchronize(stream_));
+    cudaFree(d_lf_mi_);
+    CK(cudaMalloc(&d_lf_mi_, mi_len * 4));
+    lf_mi_cap_ = mi_len;
+  }
+  size_t n_sb = (size_t)d.sb64_cols * d.sb64_rows;
+  if (n_sb > sb_cap_) {
+    CK(cudaStreamSynchronize(stream_));
+    cudaFree(d_sb_done_);
+    CK(cudaMalloc(&d_sb_done_, n_sb * 4));
+    CK(cudaMemsetAsync(d_sb_done_, 0, n_sb * 4, stream_));
+    sb_cap_ = n_sb;
+  }
+  CK(cudaStreamSynchronize(stream_));
+  return rv9::ST_OK;
+}
+
 size_t fixed_scratch_need(uint32_t mi_cols, uint32_t mi_rows, uint32_t sb64_cols, uint32_t sb64_rows) {
   return 256 + align256((size_t)sb64_cols * sb64_rows * 4) + (size_t)mi_cols * mi_rows * 4;
 }
@@ -704,6 +779,15 @@ rv9::Status Engine::sequence_run_fixed(const Sequence& seq, float* ms, std::stri
   }
   if (prev != device_) cudaSetDevice(prev);
   return st;
+}
+
+rv9::Status Engine::sequence_clone(const Sequence& src, Sequence* seq, std::string* err) {
+  seq->frames = src.frames;
+  seq->bytes = src.bytes;
+  seq->luma_samples = src.luma_samples;
+  CK(cudaMalloc(&seq->d_data, std::max<size_t>(src.bytes, 256)));
+  CK(cudaMemcpy(seq->d_data, src.d_data, src.bytes, cudaMemcpyDeviceToDevice));
+  return rv9::ST_OK;
 }
 
 void Engine::sequence_free(Sequence* seq) {

@@ -109,12 +109,26 @@ class Engine {
   static rv9::Status run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
                                     bool per_kernel, float* ms, std::string* err);
   int device() const { return device_; }
+  // The device error word as last copied back (nonzero after a wavefront
+  // wait gave up; sync() reports and clears it).
+  int32_t error_word() const { return h_error_ ? *(volatile int32_t*)(h_error_ + 1) : 0; }
+  // Device bytes one decoder of this geometry holds with `n_frames` pooled
+  // frames and record staging of `stage_bytes` (per buffer, two buffers).
+  static size_t footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t bit_depth,
+                          int n_frames, size_t stage_bytes);
+  // Allocates up front what decoding frames of this geometry takes: pooled
+  // frames, record staging, loop-filter and wavefront scratch. Decoding such
+  // frames then allocates nothing more.
+  rv9::Status reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t bit_depth,
+                      int n_frames, size_t stage_bytes, std::string* err);
   // Like sequence_run (per_kernel off), allocating nothing: the wavefront
   // scratch is the fixed static array, and every frame comes from the pool.
   // Fails before any launch when a frame of the sequence needs more scratch
   // than the array holds, or the pool lacks a frame the run would take.
   rv9::Status sequence_run_fixed(const Sequence& seq, float* ms, std::string* err);
   void sequence_free(Sequence* seq);
+  // A device copy of `src` on this engine's device.
+  rv9::Status sequence_clone(const Sequence& src, Sequence* seq, std::string* err);
   DevFrame* slot(int i) const { return slots_[i]; }
 
   // Stats.

@@ -1,0 +1,572 @@
+// Serving engine of rv9_server.h: many live streams on one GPU.
+//
+// Each stream owns a host parser and a reconstruction engine (reference
+// slots, pooled frames, its own CUDA stream). Host workers take one request
+// at a time from streams that are ready, parse it, launch its frames'
+// reconstruction on the stream's CUDA stream and queue the copies of the
+// shown frames into pinned buffers; a host function queued after them on the
+// same CUDA stream completes the request. One stream is only ever worked on
+// by one worker at a time, so its requests complete in order, while requests
+// of different streams overlap on the device.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../../include/rv9_server.h"
+#include "../api/api_internal.h"
+#include "../gpu/engine.h"
+#include "../host/parser.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int kReservedFrames = 10;  // eight slots, the frame being built, one spare
+constexpr int kOutBuffers = 4;       // pinned output buffers per stream
+constexpr int kMaxShown = 2;         // shown frames one request may carry
+
+struct OutBuf {
+  uint8_t* data = nullptr;
+  size_t cap = 0;
+};
+
+struct Request {
+  uint64_t tag = 0;
+  std::vector<uint8_t> packet;
+  double submit_ms = 0;
+};
+
+struct Stream;
+
+// A finished (or failed) request on its way to rv9_poll.
+struct Done {
+  std::shared_ptr<Stream> stream;
+  int64_t stream_id = 0;
+  uint64_t tag = 0;
+  rv9_status status = RV9_OK;
+  std::string err;
+  double submit_ms = 0, latency_ms = 0;
+  int out = -1;  // index of the stream's output buffer, or -1
+  uint32_t n_frames = 0;
+  rv9_frame frames[kMaxShown];
+};
+
+enum StreamState { PENDING, ADMITTING, ACTIVE, CLOSED };
+
+struct Stream {
+  int64_t id = 0;
+  rv9_stream_spec spec{};
+  uint64_t reservation = 0;
+  StreamState state = PENDING;
+  bool busy = false;         // a worker holds it
+  bool closing = false;      // close requested
+  bool needs_reset = false;  // a device error: reset the engine's scratch first
+  int inflight = 0;          // requests launched, not yet completed
+  std::deque<Request> queue;
+  rv9::Parser parser;
+  std::unique_ptr<rv9g::Engine> engine;
+  std::vector<OutBuf> outs;
+  std::vector<int> free_outs;
+  ~Stream() {
+    for (OutBuf& b : outs) cudaFreeHost(b.data);
+  }
+};
+
+size_t stage_bytes_of(const rv9_stream_spec& s) {
+  return std::max<size_t>((size_t)s.max_width * s.max_height * 3, 1 << 20);
+}
+
+uint64_t reservation_of(const rv9_stream_spec& s) {
+  return rv9g::Engine::footprint(s.max_width, s.max_height, s.ss_x, s.ss_y, s.bit_depth, kReservedFrames,
+                                 stage_bytes_of(s));
+}
+
+size_t packed_cap(const rv9_stream_spec& s) {
+  size_t bps = s.bit_depth > 8 ? 2 : 1;
+  size_t cw = (s.max_width + s.ss_x) >> s.ss_x, ch = (s.max_height + s.ss_y) >> s.ss_y;
+  return ((size_t)s.max_width * s.max_height + 2 * cw * ch) * bps;
+}
+
+}  // namespace
+
+struct rv9_engine {
+  int device = 0;
+  uint64_t budget = 0, reserved = 0;
+  Clock::time_point t0 = Clock::now();
+  std::mutex mu;
+  std::condition_variable work_cv, done_cv, idle_cv;
+  std::map<int64_t, std::shared_ptr<Stream>> streams;
+  std::deque<int64_t> pending;  // admission order
+  std::deque<Done*> done;
+  std::set<Done*> polled;  // handed out by rv9_poll, not yet released
+  int64_t next_id = 1;
+  bool stop = false;
+  std::vector<std::thread> workers;
+  size_t cursor = 0;
+  uint64_t n_submitted = 0, n_completed = 0, n_frames = 0;
+
+  double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+
+  // Admits pending streams in order while the budget allows (caller holds mu).
+  void admit_locked() {
+    while (!pending.empty()) {
+      auto it = streams.find(pending.front());
+      if (it == streams.end()) {
+        pending.pop_front();
+        continue;
+      }
+      Stream& s = *it->second;
+      if (reserved + s.reservation > budget) break;
+      reserved += s.reservation;
+      s.state = ADMITTING;
+      pending.pop_front();
+    }
+  }
+
+  // Fails every queued request of `sp` with `st` (caller holds mu).
+  void fail_queue_locked(const std::shared_ptr<Stream>& sp, rv9_status st, const std::string& err) {
+    Stream& s = *sp;
+    while (!s.queue.empty()) {
+      Done* d = new Done;
+      d->stream = sp;
+      d->stream_id = s.id;
+      d->tag = s.queue.front().tag;
+      d->submit_ms = s.queue.front().submit_ms;
+      d->status = st;
+      d->err = err;
+      d->latency_ms = now_ms() - d->submit_ms;
+      s.queue.pop_front();
+      ++n_completed;
+      done.push_back(d);
+    }
+    done_cv.notify_all();
+  }
+
+  enum Action { NONE, ADMIT, DECODE, CLOSE };
+
+  // The next stream a worker may take, and what to do with it (caller holds
+  // mu): admit it, decode its next request (it has one and a free output
+  // buffer), or close it (closing and drained). Round-robin over streams.
+  Action pick_locked(std::shared_ptr<Stream>* out) {
+    if (streams.empty()) return NONE;
+    std::vector<std::shared_ptr<Stream>> order;
+    order.reserve(streams.size());
+    for (auto& kv : streams) order.push_back(kv.second);
+    size_t n = order.size();
+    for (size_t k = 0; k < n; ++k) {
+      auto& s = order[(cursor + k) % n];
+      if (s->busy) continue;
+      Action a = NONE;
+      if (s->state == ADMITTING)
+        a = ADMIT;
+      else if (s->state == ACTIVE && !s->queue.empty() && !s->free_outs.empty())
+        a = DECODE;
+      else if (s->state == ACTIVE && s->closing && s->queue.empty() && s->inflight == 0)
+        a = CLOSE;
+      if (a != NONE) {
+        cursor = (cursor + k + 1) % n;
+        s->busy = true;
+        *out = s;
+        return a;
+      }
+    }
+    return NONE;
+  }
+
+  // Returns a completion's output buffer to its stream and frees it (caller
+  // holds mu). The stream reference comes back to be dropped after the lock
+  // is released: the last one frees pinned memory, which must not happen
+  // under the lock that completion callbacks take.
+  std::shared_ptr<Stream> release_locked(Done* d) {
+    if (d->out >= 0) d->stream->free_outs.push_back(d->out);
+    std::shared_ptr<Stream> keep = std::move(d->stream);
+    delete d;
+    work_cv.notify_all();
+    return keep;
+  }
+
+  void finish(Done* d) {
+    std::lock_guard<std::mutex> lock(mu);
+    d->latency_ms = now_ms() - d->submit_ms;
+    if (d->stream->engine && d->stream->engine->error_word() != 0) {
+      // The engine's scratch is reset before the stream's next request.
+      d->stream->needs_reset = true;
+      if (d->status == RV9_OK) {
+        d->status = RV9_DEVICE;
+        d->err = "a device-side wait timed out";
+      }
+    }
+    d->stream->inflight -= 1;
+    ++n_completed;
+    if (d->status == RV9_OK) n_frames += d->n_frames;
+    done.push_back(d);
+    done_cv.notify_all();
+    work_cv.notify_all();
+    idle_cv.notify_all();
+  }
+
+  struct Callback {
+    rv9_engine* eng;
+    Done* d;
+  };
+  static void CUDART_CB host_fn(void* p) {
+    Callback* c = static_cast<Callback*>(p);
+    c->eng->finish(c->d);
+    delete c;
+  }
+
+  // Queues the completion behind the stream's device work.
+  void complete_after_device(Stream& s, Done* d) {
+    Callback* cb = new Callback{this, d};
+    if (cudaLaunchHostFunc(s.engine->stream(), host_fn, cb) == cudaSuccess) return;
+    delete cb;
+    if (d->status == RV9_OK) {
+      d->status = RV9_DEVICE;
+      d->err = "could not queue the completion";
+    }
+    finish(d);
+  }
+
+  void admit(const std::shared_ptr<Stream>& sp) {
+    Stream& s = *sp;
+    std::string err;
+    std::unique_ptr<rv9g::Engine> engine(new rv9g::Engine);
+    bool ok = engine->init(device, &err);
+    if (ok)
+      ok = engine->reserve(s.spec.max_width, s.spec.max_height, s.spec.ss_x, s.spec.ss_y, s.spec.bit_depth,
+                           kReservedFrames, stage_bytes_of(s.spec), &err) == rv9::ST_OK;
+    std::vector<OutBuf> outs;
+    size_t cap = packed_cap(s.spec) * kMaxShown;
+    for (int i = 0; ok && i < kOutBuffers; ++i) {
+      OutBuf b;
+      if (cudaMallocHost(&b.data, cap) != cudaSuccess) {
+        ok = false;
+        err = "out of pinned host memory for output buffers";
+        break;
+      }
+      b.cap = cap;
+      outs.push_back(b);
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    s.outs = std::move(outs);
+    if (ok) {
+      s.engine = std::move(engine);
+      for (int i = 0; i < (int)s.outs.size(); ++i) s.free_outs.push_back(i);
+      s.state = ACTIVE;
+    } else {
+      // Fail the stream's requests and drop it; its reservation returns.
+      s.state = CLOSED;
+      s.closing = true;
+      reserved -= s.reservation;
+      fail_queue_locked(sp, RV9_DEVICE, err.empty() ? "admission failed" : err);
+      streams.erase(s.id);
+      admit_locked();
+      idle_cv.notify_all();
+    }
+    s.busy = false;
+    work_cv.notify_all();
+  }
+
+  void close_drained(const std::shared_ptr<Stream>& sp) {
+    Stream& s = *sp;
+    std::unique_ptr<rv9g::Engine> engine;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      reserved -= s.reservation;
+      s.state = CLOSED;
+      engine.swap(s.engine);
+      streams.erase(s.id);
+      admit_locked();
+      s.busy = false;
+      work_cv.notify_all();
+    }
+    engine.reset();  // outside the lock: frees device memory
+    std::lock_guard<std::mutex> lock(mu);
+    idle_cv.notify_all();
+  }
+
+  void decode_request(const std::shared_ptr<Stream>& sp) {
+    Stream& s = *sp;
+    if (s.needs_reset) {
+      std::string err;
+      s.engine->sync(&err);  // reports the error once more and resets the scratch
+      s.needs_reset = false;
+    }
+    Request req;
+    int out;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      req = std::move(s.queue.front());
+      s.queue.pop_front();
+      out = s.free_outs.back();
+      s.free_outs.pop_back();
+      s.inflight += 1;
+    }
+    Done* d = new Done;
+    d->stream = sp;
+    d->stream_id = s.id;
+    d->tag = req.tag;
+    d->submit_ms = req.submit_ms;
+    d->out = out;
+    std::string err;
+    std::vector<std::pair<size_t, size_t>> frames;
+    rv9::superframe_split(req.packet.data(), req.packet.size(), &frames);
+    if (req.packet.empty()) {
+      d->status = RV9_BITSTREAM;
+      d->err = "empty packet";
+    }
+    rv9::ParsedFrame pf;
+    size_t off = 0;
+    for (auto& fr : frames) {
+      rv9::Status st = s.parser.parse_frame(req.packet.data() + fr.first, fr.second, &pf, &err);
+      rv9g::DevFrame* shown = nullptr;
+      if (st == rv9::ST_OK) st = s.engine->recon(pf, &shown, &err);
+      if (st != rv9::ST_OK) {
+        d->status = (rv9_status)st;
+        d->err = err;
+        break;
+      }
+      if (!shown) continue;
+      size_t nb = rv9g::Engine::packed_bytes(shown);
+      if (d->n_frames >= (uint32_t)kMaxShown || off + nb > s.outs[out].cap) {
+        d->status = RV9_UNSUPPORTED;
+        d->err = "a request showed more frames, or larger ones, than its stream spec allows";
+        break;
+      }
+      rv9_frame& f = d->frames[d->n_frames++];
+      memset(&f, 0, sizeof f);
+      f.width = shown->width;
+      f.height = shown->height;
+      f.bit_depth = shown->bit_depth;
+      f.chroma = shown->ss_x ? (shown->ss_y ? RV9_YUV420 : RV9_YUV422) : (shown->ss_y ? RV9_YUV440 : RV9_YUV444);
+      f.color_space = shown->color_space;
+      f.full_range = shown->color_range;
+      f.render_width = shown->render_w;
+      f.render_height = shown->render_h;
+      f.data = s.outs[out].data + off;
+      f.size = nb;
+      size_t poff = 0, bps = shown->bps();
+      for (int p = 0; p < 3; ++p) {
+        uint32_t w = p ? (shown->width + shown->ss_x) >> shown->ss_x : shown->width;
+        uint32_t h = p ? (shown->height + shown->ss_y) >> shown->ss_y : shown->height;
+        f.planes[p].offset = poff;
+        f.planes[p].width = w;
+        f.planes[p].height = h;
+        poff += (size_t)w * h * bps;
+      }
+      rv9::Status s2 = s.engine->download_async(shown, f.data, &err);
+      if (s2 != rv9::ST_OK) {
+        d->status = (rv9_status)s2;
+        d->err = err;
+        break;
+      }
+      off += nb;
+    }
+    complete_after_device(s, d);
+    std::lock_guard<std::mutex> lock(mu);
+    s.busy = false;
+    work_cv.notify_all();
+  }
+
+  void worker_loop() {
+    cudaSetDevice(device);
+    for (;;) {
+      std::shared_ptr<Stream> s;
+      Action a = NONE;
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        work_cv.wait(lock, [&] { return stop || (a = pick_locked(&s)) != NONE; });
+        if (a == NONE) return;  // stop
+      }
+      if (a == ADMIT)
+        admit(s);
+      else if (a == CLOSE)
+        close_drained(s);
+      else
+        decode_request(s);
+    }
+  }
+};
+
+extern "C" {
+
+uint64_t rv9_stream_reservation(const rv9_stream_spec* spec) { return spec ? reservation_of(*spec) : 0; }
+
+rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers) {
+  {
+    // The same device check as rv9_decoder_new, with its message.
+    rv9g::Engine probe;
+    std::string err;
+    if (!probe.init(device, &err)) {
+      rv9api::set_global_error(err);
+      return nullptr;
+    }
+    device = probe.device();
+  }
+  rv9_engine* e = new rv9_engine;
+  e->device = device;
+  e->budget = hbm_budget_bytes;
+  int n = workers ? (int)workers : (int)std::max(1u, std::thread::hardware_concurrency());
+  for (int i = 0; i < n; ++i) e->workers.emplace_back([e] { e->worker_loop(); });
+  return e;
+}
+
+rv9_status rv9_stream_close(rv9_engine* e, int64_t id);
+
+void rv9_engine_free(rv9_engine* e) {
+  if (!e) return;
+  std::vector<int64_t> ids;
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    for (auto& kv : e->streams) ids.push_back(kv.first);
+  }
+  for (int64_t id : ids) rv9_stream_close(e, id);
+  {
+    // Every stream drains and closes, then the workers stop. Completions are
+    // released as they come, so that no stream waits for an output buffer.
+    std::vector<std::shared_ptr<Stream>> dropped;
+    std::unique_lock<std::mutex> lock(e->mu);
+    for (;;) {
+      for (Done* d : e->polled) dropped.push_back(e->release_locked(d));
+      e->polled.clear();
+      while (!e->done.empty()) {
+        dropped.push_back(e->release_locked(e->done.front()));
+        e->done.pop_front();
+      }
+      if (e->streams.empty()) break;
+      lock.unlock();
+      dropped.clear();
+      lock.lock();
+      e->idle_cv.wait_for(lock, std::chrono::milliseconds(20));
+    }
+    e->stop = true;
+    e->work_cv.notify_all();
+    lock.unlock();
+    dropped.clear();
+  }
+  for (auto& t : e->workers) t.join();
+  for (Done* d : e->done) delete d;
+  delete e;
+}
+
+rv9_status rv9_stream_open(rv9_engine* e, const rv9_stream_spec* spec, int64_t* id) {
+  if (!e || !spec || !id) return RV9_INVALID_INPUT;
+  *id = 0;
+  if (spec->max_width == 0 || spec->max_height == 0 || spec->max_width > 16384 || spec->max_height > 16384 ||
+      (spec->bit_depth != 8 && spec->bit_depth != 10 && spec->bit_depth != 12) || spec->ss_x > 1 || spec->ss_y > 1)
+    return RV9_INVALID_INPUT;
+  uint64_t r = reservation_of(*spec);
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (r > e->budget) return RV9_UNSUPPORTED;
+  auto s = std::make_shared<Stream>();
+  s->id = e->next_id++;
+  s->spec = *spec;
+  s->reservation = r;
+  s->parser.set_threads(1);
+  e->streams[s->id] = s;
+  e->pending.push_back(s->id);
+  e->admit_locked();
+  *id = s->id;
+  e->work_cv.notify_all();
+  return RV9_OK;
+}
+
+rv9_status rv9_stream_close(rv9_engine* e, int64_t id) {
+  if (!e) return RV9_INVALID_INPUT;
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->streams.find(id);
+  if (it == e->streams.end()) return RV9_INVALID_INPUT;
+  std::shared_ptr<Stream> sp = it->second;
+  sp->closing = true;
+  if (sp->state == PENDING && sp->queue.empty()) {
+    // Never admitted and nothing to do: dropped at once. A pending stream
+    // with requests is admitted in turn, decodes them, then closes.
+    sp->state = CLOSED;
+    e->streams.erase(it);
+    e->idle_cv.notify_all();
+  }
+  e->work_cv.notify_all();
+  return RV9_OK;
+}
+
+rv9_status rv9_submit(rv9_engine* e, int64_t id, const uint8_t* packet, size_t len, uint64_t tag) {
+  if (!e || (!packet && len)) return RV9_INVALID_INPUT;
+  Request r;
+  r.tag = tag;
+  r.packet.assign(packet, packet + len);
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->streams.find(id);
+  if (it == e->streams.end() || it->second->closing) return RV9_INVALID_INPUT;
+  r.submit_ms = e->now_ms();
+  it->second->queue.push_back(std::move(r));
+  ++e->n_submitted;
+  e->work_cv.notify_all();
+  return RV9_OK;
+}
+
+size_t rv9_poll(rv9_engine* e, rv9_completion* out, size_t cap, int timeout_ms) {
+  if (!e || !out || cap == 0) return 0;
+  std::unique_lock<std::mutex> lock(e->mu);
+  if (e->done.empty() && timeout_ms > 0)
+    e->done_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms), [&] { return !e->done.empty(); });
+  size_t n = 0;
+  while (n < cap && !e->done.empty()) {
+    Done* d = e->done.front();
+    e->done.pop_front();
+    rv9_completion& c = out[n++];
+    memset(&c, 0, sizeof c);
+    c.stream = d->stream_id;
+    c.tag = d->tag;
+    c.status = d->status;
+    c.n_frames = d->status == RV9_OK ? d->n_frames : 0;
+    c.submit_ms = d->submit_ms;
+    c.latency_ms = d->latency_ms;
+    for (uint32_t i = 0; i < c.n_frames; ++i) c.frames[i] = d->frames[i];
+    c.handle = d;
+    e->polled.insert(d);
+  }
+  return n;
+}
+
+void rv9_completion_release(rv9_engine* e, rv9_completion* c) {
+  if (!e || !c || !c->handle) return;
+  Done* d = static_cast<Done*>(c->handle);
+  std::shared_ptr<Stream> keep;
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    if (!e->polled.erase(d)) return;  // not a live handle of this engine
+    keep = e->release_locked(d);
+  }
+  c->handle = nullptr;
+  // `keep` may be the last reference to a closed stream: freed here.
+}
+
+void rv9_engine_get_stats(rv9_engine* e, rv9_engine_stats* out) {
+  if (!e || !out) return;
+  std::lock_guard<std::mutex> lock(e->mu);
+  memset(out, 0, sizeof *out);
+  for (auto& kv : e->streams) {
+    if (kv.second->state == PENDING)
+      ++out->streams_pending;
+    else if (kv.second->state != CLOSED)
+      ++out->streams_open;
+  }
+  out->requests_submitted = e->n_submitted;
+  out->requests_completed = e->n_completed;
+  out->frames_decoded = e->n_frames;
+  out->reserved_bytes = e->reserved;
+  out->budget_bytes = e->budget;
+}
+
+}  // extern "C"

@@ -71,7 +71,7 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decoder_frames_decoded", "rv9_last_error", "rv9_last_global_error", "rv9_decode_all",
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
-           "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_decoder_download_slot", "rv9_kernel_stats",
+           "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
            "rv9_sequence_run_noalloc", "rv9_sequences_run")
 
 
@@ -123,6 +123,7 @@ def load_library(path=None):
     lib.rv9_sequence_frames.restype = ctypes.c_uint32
     lib.rv9_sequence_frames.argtypes = [vp]
     lib.rv9_sequence_free.argtypes = [vp, vp]
+    lib.rv9_sequence_clone.argtypes = [vp, vp, ctypes.POINTER(vp)]
     lib.rv9_decoder_download_slot.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
     lib.rv9_kernel_stats.restype = ctypes.c_size_t
     lib.rv9_kernel_stats.argtypes = [vp, ctypes.POINTER(CKernelStat), ctypes.c_size_t, ctypes.c_int]
@@ -307,6 +308,14 @@ class Decoder:
         if st != RV9_OK:
             _raise(self._lib, self._dec, st)
         return Sequence(self, seq)
+
+    def clone_sequence(self, seq):
+        """A copy of `seq` (any decoder's, same device) held by this decoder."""
+        out = ctypes.c_void_p()
+        st = self._lib.rv9_sequence_clone(self._dec, seq._h, ctypes.byref(out))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        return Sequence(self, out)
 
     def download_slot(self, slot, cap):
         buf = ctypes.create_string_buffer(cap)

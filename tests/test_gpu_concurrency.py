@@ -90,3 +90,21 @@ def test_rejects_a_decoder_twice():
         s1.free()
         s2.free()
         d.close()
+
+
+def test_clone_replays_the_same():
+    import rv9
+    a, b = rv9.Decoder(0), rv9.Decoder(0)
+    seq = a.load_sequence(read_packets(os.path.join(VECTORS_DIR, NAMES[1])))
+    try:
+        seq.run()
+        want = _slots(a)
+        copy = b.clone_sequence(seq)
+        assert copy.frames == seq.frames and copy.luma_samples == seq.luma_samples
+        seq.free()  # the copy owns its records
+        copy.run()
+        assert _slots(b) == want
+        copy.free()
+    finally:
+        a.close()
+        b.close()
