@@ -48,14 +48,40 @@ METRIC = "decoded Mpixels/s (bit-exact, 1080p 8-bit 4:2:0, 4 tile columns, q40+q
 STREAM_DIR = os.path.join(PKG, "_build", "streams")
 
 
+# Contents of the batched and served workloads: one generated stream per
+# (size, bit depth) class, `frames` long, looped to the workload's length
+# (each loop starts at a keyframe, so the looped stream is a valid one).
+BATCH_CLASSES = [
+    dict(name="b240_8", width=320, height=240, bit_depth=8, q=35, seed=11),
+    dict(name="b240_10", width=320, height=240, bit_depth=10, q=80, seed=12),
+    dict(name="b360_8", width=640, height=360, bit_depth=8, q=60, seed=13),
+    dict(name="b360_10", width=640, height=360, bit_depth=10, q=45, seed=14),
+    dict(name="b720_8", width=1280, height=720, bit_depth=8, q=70, seed=15),
+    dict(name="b720_10", width=1280, height=720, bit_depth=10, q=40, seed=16),
+    dict(name="b1080_8", width=1920, height=1080, bit_depth=8, q=55, seed=17),
+    dict(name="b1080_10", width=1920, height=1080, bit_depth=10, q=85, seed=18),
+]
+SERVE_CLASSES = [
+    dict(name="s720_8", width=1280, height=720, bit_depth=8, q=60, seed=21),
+    dict(name="s720_10", width=1280, height=720, bit_depth=10, q=60, seed=22),
+    dict(name="s1080_8", width=1920, height=1080, bit_depth=8, q=60, seed=23),
+    dict(name="s1080_10", width=1920, height=1080, bit_depth=10, q=60, seed=24),
+    dict(name="s2160_8", width=3840, height=2160, bit_depth=8, q=60, seed=25),
+    dict(name="s2160_10", width=3840, height=2160, bit_depth=10, q=60, seed=26),
+]
+CLASS_FRAMES = 30
+
+
 def stream_packets(spec):
     """Packets of a workload stream (generated once, cached under _build)."""
     from rv9 import containers, streams
     path = os.path.join(STREAM_DIR, spec["name"] + ".ivf")
     if not os.path.exists(path):
-        cfg = streams.config(spec["width"], spec["height"], spec["frames"], spec["q"], bit_depth=8, chroma=(1, 1),
-                             tile_cols_log2=2, golden_interval=8, seed=spec["seed"], pan=(3, 2), rectangles=12,
-                             noise=6)
+        w, h = spec["width"], spec["height"]
+        noise = spec.get("noise", 24 if spec.get("bit_depth", 8) > 8 else 6)
+        cfg = streams.config(w, h, spec.get("frames", CLASS_FRAMES), spec["q"], bit_depth=spec.get("bit_depth", 8),
+                             chroma=(1, 1), tile_cols_log2=2 if w >= 1024 else 0, golden_interval=8,
+                             seed=spec["seed"], pan=(3, 2), rectangles=12, noise=noise)
         pk = streams.generate(cfg)
         os.makedirs(STREAM_DIR, exist_ok=True)
         with open(path[:-4] + ".last.md5", "w") as f:
@@ -88,6 +114,12 @@ def dist_max(x, world, device=None):
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_value(units_per_rank, world, ms_max):
+    """Whole-job throughput in millions of units per second: every rank
+    processes `units_per_rank` (weak scaling), timed by the slowest rank."""
+    return units_per_rank * world / (ms_max / 1e3) / 1e6
 
 
 def dist_barrier(world):
@@ -181,6 +213,141 @@ def cpu_baseline(packets_list, frames):
     return samples / secs / 1e6, secs
 
 
+def looped(packets, n):
+    """`packets` repeated to `n` packets (each repeat starts at a keyframe)."""
+    return [packets[i % len(packets)] for i in range(n)]
+
+
+def percentile(xs, p):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(p / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def run_batched(local, dev, n_streams=64, frames=60):
+    """64 independent streams of uneven sizes and depths, all resident,
+    reconstructed at once (one CUDA stream each) against the plain path (the
+    same sequences one at a time)."""
+    import random
+
+    import torch
+    import rv9
+    rng = random.Random(64)
+    contents = [looped(stream_packets(c), frames) for c in BATCH_CLASSES]
+    picks = [rng.randrange(len(BATCH_CLASSES)) for _ in range(n_streams)]
+    loader = rv9.Decoder(device=local)
+    base = [loader.load_sequence(pk) for pk in contents]
+    decs = [rv9.Decoder(device=local) for _ in range(n_streams)]
+    seqs = [d.clone_sequence(base[k]) for d, k in zip(decs, picks)]
+    pairs = list(zip(decs, seqs))
+    luma = sum(sq.luma_samples for sq in seqs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(2):
+        rv9.run_concurrent(pairs)
+    flush.zero_()
+    torch.cuda.synchronize(dev)
+    ms_batched = min(rv9.run_concurrent(pairs) for _ in range(2))
+    ms_plain = 0.0
+    for d, sq in pairs:
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        ms_plain += sq.run()
+    out = {
+        "workload": f"{n_streams} streams over 8 generated contents {{320x240, 640x360, 1280x720, 1920x1080}} x "
+                    f"{{8, 10}}-bit 4:2:0, q per content in [35, 85], {CLASS_FRAMES} frames looped to {frames}",
+        "frames": sum(sq.frames for sq in seqs),
+        "value": round(luma / (ms_batched / 1e3) / 1e6, 2), "unit": "Mpixels/s",
+        "plain_per_stream": round(luma / (ms_plain / 1e3) / 1e6, 2),
+        "speedup_vs_plain": round(ms_plain / ms_batched, 2),
+        "ms_batched": round(ms_batched, 3), "ms_plain": round(ms_plain, 3),
+        "how": "rv9_sequences_run over 64 decoders (own CUDA stream and slots each) vs rv9_sequence_run one by one",
+    }
+    for sq in seqs + base:
+        sq.free()
+    for d in decs + [loader]:
+        d.close()
+    return out
+
+
+def run_served(local, rates=(500, 1000, 2000, 4000), n_streams=32, frames=120, seed=5):
+    """The serving loop: 32 live streams (40% 720p, 40% 1080p, 20% 2160p;
+    8/10-bit), requests arriving as a Poisson process at each total rate;
+    throughput and per-request latency (submit -> frames in host memory)."""
+    import random
+    import threading as th
+
+    import rv9
+    from rv9 import server
+    contents = {c["name"]: looped(stream_packets(c), frames) for c in SERVE_CLASSES}
+    rng = random.Random(seed)
+    mix = []
+    for i in range(n_streams):
+        size = "720" if i < 13 else ("1080" if i < 26 else "2160")
+        mix.append(f"s{size}_{8 if rng.random() < 0.5 else 10}")
+    spec = {c["name"]: c for c in SERVE_CLASSES}
+    luma = {n: spec[n]["width"] * spec[n]["height"] for n in spec}
+    results = []
+    # The plain single-stream path: one 1080p stream through rv9_decode_packets.
+    d = rv9.Decoder(device=local)
+    pk = contents["s1080_8"]
+    cap = len(pk) * 1920 * 1080 * 3 // 2 + (1 << 20)
+    import torch
+    buf = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+    d.decode_packets_to(pk[:30], buf.data_ptr(), cap)  # warm
+    t = time.perf_counter()
+    d.decode_packets_to(pk, buf.data_ptr(), cap)
+    plain = len(pk) * luma["s1080_8"] / (time.perf_counter() - t) / 1e6
+    d.close()
+    del buf
+    for rate in rates:
+        eng = server.Engine(local, hbm_budget=120 << 30)
+        sids = [eng.open_stream(spec[n]["width"], spec[n]["height"], spec[n]["bit_depth"]) for n in mix]
+        # Arrival times: per stream a Poisson process of rate/n_streams.
+        events = []
+        for j, n in enumerate(mix):
+            tt = 0.0
+            for i in range(frames):
+                tt += rng.expovariate(rate / n_streams)
+                events.append((tt, j, i))
+        events.sort()
+        done = []
+        t0 = time.perf_counter()
+
+        def feed():
+            for tt, j, i in events:
+                delay = t0 + tt - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                eng.submit(sids[j], contents[mix[j]][i], tag=i)
+
+        feeder = th.Thread(target=feed)
+        feeder.start()
+        total = len(events)
+        deadline = t0 + 600
+        while len(done) < total and time.perf_counter() < deadline:
+            done += eng.poll(max_items=256, timeout_ms=50, keep_frames=False)
+        wall = time.perf_counter() - t0
+        feeder.join()
+        for sid in sids:
+            eng.close_stream(sid)
+        eng.close()
+        lat = [c.latency_ms for c in done if c.ok]
+        px = sum(luma[mix[sids.index(c.stream)]] * c.n_frames for c in done if c.ok)
+        results.append({"offered_fps": rate, "completed": len(lat), "failed": len(done) - len(lat),
+                        "fps": round(len(lat) / wall, 1), "mpixels_s": round(px / wall / 1e6, 1),
+                        "p50_ms": round(percentile(lat, 50), 2) if lat else None,
+                        "p99_ms": round(percentile(lat, 99), 2) if lat else None, "wall_s": round(wall, 2)})
+    best = max(r["mpixels_s"] for r in results)
+    return {"workload": f"{n_streams} streams: 13 x 720p, 13 x 1080p, 6 x 2160p, 8/10-bit 4:2:0, q60, "
+                        f"{CLASS_FRAMES} frames looped to {frames}; Poisson arrivals; HBM budget 120 GB",
+            "rates": results, "plain_single_stream_e2e_mpixels_s": round(plain, 1),
+            "best_vs_plain": round(best / plain, 2),
+            "latency": "rv9_submit -> frames in pinned host memory (host-function callback)",
+            "host_cores": os.cpu_count()}
+
+
 def run_gpu(args, world, rank, local):
     import torch
     import rv9
@@ -244,7 +411,7 @@ def run_gpu(args, world, rank, local):
     ms_single = dist_max(ms_single, world, dev)
     kernel_stats()
     ms_max = dist_max(ms_total, world, dev)
-    value = luma_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+    value = whole_job_value(luma_per_step * args.steps, world, ms_max)
     # Roofline of the kernel with the most device time.
     top = max(ks.items(), key=lambda kv: kv[1]["ms"])
     name, st = top
@@ -298,6 +465,12 @@ def run_gpu(args, world, rank, local):
     gen_md5 = open(gen_md5_path).read().strip() if os.path.exists(gen_md5_path) and not args.frames else None
     check = {"e2e_equals_replay": last_md5 == replay_md5,
              "equals_generator_reconstruction": (gen_md5 == last_md5) if gen_md5 else None}
+    extra = {}
+    sections = args.sections.split(",") if world == 1 else []
+    if "batched" in sections:
+        extra["batched"] = run_batched(local, dev)
+    if "served" in sections:
+        extra["served"] = run_served(local)
     cpu = None
     if rank == 0 and world == 1:
         cpu_val, cpu_secs = cpu_baseline(packets, 8)
@@ -326,6 +499,7 @@ def run_gpu(args, world, rank, local):
             "kernels": kernels, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "bit_exact_check": check, "wall_s_timed": round(wall, 3),
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
 
 
@@ -389,6 +563,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rv9", choices=["rv9", "reference"])
     ap.add_argument("--frames", type=int, default=0, help="frames per stream (0: all; fewer for profiling runs)")
+    ap.add_argument("--sections", default="main,batched,served",
+                    help="comma list: main (always), batched (64 resident streams), served (32-stream serving loop)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

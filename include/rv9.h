@@ -76,6 +76,11 @@ rv9_decoder* rv9_decoder_new(int device);
 void rv9_decoder_free(rv9_decoder* dec);
 /* Host parsing threads: 0 = one per core (default), 1 = the calling thread. */
 void rv9_decoder_set_threads(rv9_decoder* dec, uint32_t threads);
+/* Frames rv9_decode_packets and rv9_sequence_load parse at once (0: one per
+ * four host threads, at most 8). Frames that depend on an earlier frame's
+ * parse (adapted contexts, previous motion vectors) still wait for it; key
+ * and error-resilient frames do not. Results are identical either way. */
+void rv9_decoder_set_parse_depth(rv9_decoder* dec, uint32_t frames);
 /* Frames of more than `pixels` luma samples are refused (RV9_UNSUPPORTED). */
 void rv9_decoder_set_max_pixels(rv9_decoder* dec, uint64_t pixels);
 uint64_t rv9_decoder_frames_decoded(const rv9_decoder* dec);

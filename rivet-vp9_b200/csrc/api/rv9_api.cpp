@@ -4,8 +4,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/rv9.h"
@@ -19,7 +21,15 @@ struct rv9_decoder {
   std::string err;
   rv9::ParsedFrame pf;
   double parse_ms = 0;
+  uint32_t parse_depth = 0;  // frames parsed at once; 0: one per four host threads
 };
+
+// Frames parsed at once by the multi-packet calls.
+static int parse_depth(const rv9_decoder* d) {
+  if (d->parse_depth) return (int)d->parse_depth;
+  int hw = (int)std::thread::hardware_concurrency();
+  return std::max(1, std::min(8, hw / 4));
+}
 
 static thread_local std::string g_global_err;
 
@@ -63,6 +73,7 @@ rv9_decoder* rv9_decoder_new(int device) {
 
 void rv9_decoder_free(rv9_decoder* d) { delete d; }
 void rv9_decoder_set_threads(rv9_decoder* d, uint32_t t) { d->parser.set_threads((int)t); }
+void rv9_decoder_set_parse_depth(rv9_decoder* d, uint32_t frames) { d->parse_depth = frames; }
 void rv9_decoder_set_max_pixels(rv9_decoder* d, uint64_t p) { d->parser.set_max_pixels(p); }
 uint64_t rv9_decoder_frames_decoded(const rv9_decoder* d) { return d->parser.frames_decoded(); }
 const char* rv9_last_error(const rv9_decoder* d) { return d->err.c_str(); }
@@ -129,25 +140,49 @@ rv9_status rv9_decode_packets(rv9_decoder* d, const uint8_t* const* pkts, const 
                               uint8_t* out, size_t cap, size_t* n_frames, size_t* bytes) {
   *n_frames = 0;
   *bytes = 0;
+  if (!d || (n && (!pkts || !lens))) return RV9_INVALID_INPUT;
+  // Frames parse `depth` at a time where the stream allows (FramePipeline);
+  // each is reconstructed in order as its records come out.
+  const int depth = parse_depth(d);
+  rv9::FramePipeline pipe(&d->parser, depth);
   std::vector<std::pair<size_t, size_t>> frames;
+  rv9::ParsedFrame& pf = d->pf;
+  auto consume = [&]() -> rv9_status {
+    auto t0 = std::chrono::steady_clock::now();
+    rv9::Status st = pipe.pop(&pf, &d->err);
+    d->parse_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (st != rv9::ST_OK) return (rv9_status)st;
+    rv9g::DevFrame* shown = nullptr;
+    st = d->engine.recon(pf, &shown, &d->err);
+    if (st != rv9::ST_OK) return (rv9_status)st;
+    if (shown) {
+      size_t nb = rv9g::Engine::packed_bytes(shown);
+      if (*bytes + nb > cap) {
+        d->err = "output buffer too small";
+        return RV9_INVALID_INPUT;
+      }
+      rv9::Status s2 = d->engine.download_async(shown, out + *bytes, &d->err);
+      if (s2 != rv9::ST_OK) return (rv9_status)s2;
+      *bytes += nb;
+      ++*n_frames;
+    }
+    return RV9_OK;
+  };
   for (size_t i = 0; i < n; ++i) {
     rv9::superframe_split(pkts[i], lens[i], &frames);
     for (auto& fr : frames) {
-      rv9g::DevFrame* shown = nullptr;
-      rv9_status st = decode_one(d, pkts[i] + fr.first, fr.second, &shown);
-      if (st != RV9_OK) return st;
-      if (shown) {
-        size_t nb = rv9g::Engine::packed_bytes(shown);
-        if (*bytes + nb > cap) {
-          d->err = "output buffer too small";
-          return RV9_INVALID_INPUT;
-        }
-        rv9::Status s2 = d->engine.download_async(shown, out + *bytes, &d->err);
-        if (s2 != rv9::ST_OK) return (rv9_status)s2;
-        *bytes += nb;
-        ++*n_frames;
+      auto t0 = std::chrono::steady_clock::now();
+      pipe.push(pkts[i] + fr.first, fr.second);
+      d->parse_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      while (pipe.in_flight() >= (size_t)depth) {
+        rv9_status st = consume();
+        if (st != RV9_OK) return st;
       }
     }
+  }
+  while (pipe.in_flight() > 0) {
+    rv9_status st = consume();
+    if (st != RV9_OK) return st;
   }
   return (rv9_status)d->engine.sync(&d->err);
 }
@@ -163,13 +198,25 @@ rv9_status rv9_sequence_load(rv9_decoder* d, const uint8_t* const* pkts, const s
   parser.set_threads(0);
   std::vector<rv9::ParsedFrame> frames;
   std::vector<std::pair<size_t, size_t>> split;
+  const int depth = parse_depth(d);
+  rv9::FramePipeline pipe(&parser, depth);
+  auto take = [&]() -> rv9::Status {
+    frames.emplace_back();
+    return pipe.pop(&frames.back(), &d->err);
+  };
   for (size_t i = 0; i < n; ++i) {
     rv9::superframe_split(pkts[i], lens[i], &split);
     for (auto& fr : split) {
-      frames.emplace_back();
-      rv9::Status st = parser.parse_frame(pkts[i] + fr.first, fr.second, &frames.back(), &d->err);
-      if (st != rv9::ST_OK) return (rv9_status)st;
+      pipe.push(pkts[i] + fr.first, fr.second);
+      while (pipe.in_flight() >= (size_t)depth) {
+        rv9::Status st = take();
+        if (st != rv9::ST_OK) return (rv9_status)st;
+      }
     }
+  }
+  while (pipe.in_flight() > 0) {
+    rv9::Status st = take();
+    if (st != rv9::ST_OK) return (rv9_status)st;
   }
   rv9_sequence* s = new rv9_sequence;
   rv9::Status st = d->engine.sequence_load(frames, &s->seq, &d->err);

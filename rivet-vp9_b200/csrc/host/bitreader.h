@@ -63,20 +63,45 @@ class BoolDecoder {
     return !read(128);
   }
 
-  inline bool read(int prob) {
-    uint32_t split = 1 + (((range_ - 1) * (uint32_t)prob) >> 8);
+  // The decoder's state as plain values. Hot loops keep a copy in locals
+  // (registers), so that their stores to byte arrays, which may alias
+  // anything, do not force the state back to memory on every read.
+  struct State {
+    uint64_t value;
+    uint32_t range;
+    int bits;
+    const uint8_t* p;
+    const uint8_t* end;
+  };
+  State save() const { return State{value_, range_, bits_, p_, end_}; }
+  void load(const State& s) {
+    value_ = s.value;
+    range_ = s.range;
+    bits_ = s.bits;
+    p_ = s.p;
+  }
+
+  static inline bool read(State& s, int prob) {
+    uint32_t split = 1 + (((s.range - 1) * (uint32_t)prob) >> 8);
     uint64_t big = (uint64_t)split << 56;
     // Branch-free: the decoded bit is data, not control flow.
-    const bool bit = value_ >= big;
+    const bool bit = s.value >= big;
     const uint64_t m = 0 - (uint64_t)bit;
-    range_ = bit ? range_ - split : split;
-    value_ -= big & m;
-    int shift = __builtin_clz(range_) - 24;
-    range_ <<= shift;
-    value_ <<= shift;
-    bits_ -= shift;
-    if (bits_ < 16) fill();
+    s.range = bit ? s.range - split : split;
+    s.value -= big & m;
+    int shift = __builtin_clz(s.range) - 24;
+    s.range <<= shift;
+    s.value <<= shift;
+    s.bits -= shift;
+    if (s.bits < 16) fill(s);
     return bit;
+  }
+
+  inline bool read(int prob) {
+    State s = save();
+    bool b = read(s, prob);
+    load(s);
+    return b;
   }
 
   uint32_t literal(int n) {
@@ -105,29 +130,34 @@ class BoolDecoder {
   }
 
  private:
-  inline void fill() {
-    if (end_ - p_ >= 8) {
+  static inline void fill(State& s) {
+    if (s.end - s.p >= 8) {
       // Whole bytes that fit below the valid bits, from one big-endian load.
       // The part of the next byte that also lands is ORed in again, at the
       // same position, by the next fill.
       uint64_t w;
-      memcpy(&w, p_, 8);
+      memcpy(&w, s.p, 8);
       w = __builtin_bswap64(w);
-      const int nbytes = (64 - bits_) >> 3;
-      value_ |= w >> bits_;
-      p_ += nbytes;
-      bits_ += nbytes * 8;
+      const int nbytes = (64 - s.bits) >> 3;
+      s.value |= w >> s.bits;
+      s.p += nbytes;
+      s.bits += nbytes * 8;
       return;
     }
-    while (bits_ <= 56) {
-      if (p_ < end_) {
-        value_ |= (uint64_t)(*p_++) << (56 - bits_);
-        bits_ += 8;
+    while (s.bits <= 56) {
+      if (s.p < s.end) {
+        s.value |= (uint64_t)(*s.p++) << (56 - s.bits);
+        s.bits += 8;
       } else {
-        bits_ = 64;  // zeros from here on
+        s.bits = 64;  // zeros from here on
         break;
       }
     }
+  }
+  inline void fill() {
+    State s = save();
+    fill(s);
+    load(s);
   }
   const uint8_t* p_ = nullptr;
   const uint8_t* end_ = nullptr;

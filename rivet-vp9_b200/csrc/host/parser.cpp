@@ -11,6 +11,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdlib>
+#include <functional>
+#include <memory>
 #include <thread>
 
 #include "../common/vp9_consts.h"
@@ -388,41 +390,24 @@ struct TileSpan {
   size_t size;
 };
 
-}  // namespace
+struct TileResult {
+  Status st = ST_OK;
+  std::string err;
+  int failed_tile = -1;
+  bool padding_ok = true;
+};
 
-// ---------------------------------------------------------------------------
-
-struct Parser::Impl {
-  Persistent st;
-  Probs contexts[4];
-  SlotInfo slots[8];
-  std::vector<uint8_t> prev_segment_ids;
-  std::vector<PrevMv> prev_mvs;
-  bool have_last_size = false;
-  uint32_t last_w = 0, last_h = 0;
-  bool last_show_frame = false;
-  bool legacy_uv = false;
-  // Frame working memory.
+// Working memory of one frame's tile parse.
+struct TileWork {
   std::vector<MiInfo> mi;
   std::vector<uint8_t> above_nonzero[3];
   std::vector<uint8_t> above_partition, above_seg_pred;
   std::vector<TileCoder<DecCoder>> tile_decs;
 
-  Impl() {
-    for (auto& c : contexts) c.set_default();
-  }
-
-  struct TileResult {
-    Status st = ST_OK;
-    std::string err;
-    int failed_tile = -1;
-    bool padding_ok = true;
-  };
-
   // Decodes all tiles of a frame into `tile_decs` (one per tile column).
-  TileResult decode_tiles(const FrameHeader& h, const SegParams& seg, const Probs& probs,
-                          const PrevMv* prev, const bool ref_ok[3], const uint8_t* data, size_t len,
-                          int threads) {
+  TileResult decode_tiles(const FrameHeader& h, const SegParams& seg, const Probs& probs, const PrevMv* prev,
+                          const std::vector<uint8_t>* prev_seg, const bool ref_ok[3], const uint8_t* data,
+                          size_t len, int threads) {
     TileResult res;
     size_t mi_len = (size_t)h.mi_rows * h.mi_cols;
     if (mi.size() < mi_len) mi.resize(mi_len);
@@ -434,8 +419,8 @@ struct Parser::Impl {
     fc.h = &h;
     fc.seg = &seg;
     fc.probs = &probs;
-    fc.prev_seg_ids = prev_segment_ids.data();
-    fc.prev_seg_len = prev_segment_ids.size();
+    fc.prev_seg_ids = prev_seg ? prev_seg->data() : nullptr;
+    fc.prev_seg_len = prev_seg ? prev_seg->size() : 0;
     fc.prev_mvs = prev;
     fc.mi = mi.data();
     for (int p = 0; p < 3; ++p) fc.above_nonzero[p] = above_nonzero[p].data();
@@ -523,6 +508,70 @@ struct Parser::Impl {
   }
 };
 
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+// The decoder's frame-to-frame state. The previous frame's segment ids and
+// motion vectors are shared, never written in place, so that a frame still
+// parsing keeps reading the ones it started with.
+struct FrameState {
+  Persistent st;
+  Probs contexts[4];
+  SlotInfo slots[8];
+  std::shared_ptr<std::vector<uint8_t>> prev_segment_ids = std::make_shared<std::vector<uint8_t>>();
+  std::shared_ptr<std::vector<PrevMv>> prev_mvs = std::make_shared<std::vector<PrevMv>>();
+  bool have_last_size = false;
+  uint32_t last_w = 0, last_h = 0;
+  bool last_show_frame = false;
+  bool legacy_uv = false;
+  FrameState() {
+    for (auto& c : contexts) c.set_default();
+  }
+};
+
+// One frame between its header (begin) and its state update (finish).
+struct Parser::Job {
+  Status st = ST_OK;  // of the header, then of the tiles
+  std::string err;
+  bool show_existing = false;
+  FrameHeader h;
+  SegParams seg;
+  Probs probs;  // after the compressed header
+  Probs pre;    // the context before it (the base of adaptation)
+  bool ref_ok[3] = {true, true, true};
+  std::shared_ptr<std::vector<uint8_t>> prev_seg;
+  std::shared_ptr<std::vector<PrevMv>> prev_mvs;  // set when the frame uses them
+  const uint8_t* tiles = nullptr;
+  size_t tiles_len = 0;
+  bool non420 = false;
+  bool late_ctx = false;  // adapts and refreshes a context at finish
+  FrameState snap;        // the state to restore if the tiles fail
+  ParsedFrame out;
+  std::unique_ptr<TileWork> work;
+  TileResult tr;
+  std::thread th;
+  bool running = false;
+  double seconds = 0;
+  // A frame settled early by the pipeline keeps its result here.
+  bool settled = false;
+  Status settled_status = ST_OK;
+  std::string settled_err;
+  ParsedFrame settled_out;
+};
+
+struct Parser::Impl {
+  FrameState s;
+  std::vector<std::unique_ptr<TileWork>> spare;  // reusable working memory
+
+  std::unique_ptr<TileWork> take_work() {
+    if (spare.empty()) return std::unique_ptr<TileWork>(new TileWork);
+    std::unique_ptr<TileWork> w = std::move(spare.back());
+    spare.pop_back();
+    return w;
+  }
+};
+
 Parser::Parser() : impl_(new Impl) {}
 Parser::~Parser() { delete impl_; }
 
@@ -570,185 +619,376 @@ static void fill_desc(const FrameHeader& h, const Persistent& st, const SlotInfo
   d->render_height = h.render_height;
 }
 
-// The frame process (reference src/decoder/mod.rs:218-422), without samples.
-Status Parser::parse_frame(const uint8_t* data, size_t len, ParsedFrame* out, std::string* err) {
-  auto t0 = std::chrono::steady_clock::now();
+// The frame process (reference src/decoder/mod.rs:218-422), without samples,
+// in three steps: begin (headers and everything the frame's header decides,
+// including the reference slots it refreshes), run (the tiles), finish (what
+// the tiles decide for later frames: adapted contexts, previous motion
+// vectors and segment ids, the legacy 4:4:4 layout). On a tile error the
+// state goes back to what the header left, as if the frame had been parsed
+// on its own.
+
+Parser::Job* Parser::begin(const uint8_t* data, size_t len, const AfterHeader& after_header) {
   Impl& I = *impl_;
-  out->blocks.clear();
-  out->toks.clear();
-  out->coefs.clear();
-  out->show_existing = false;
-  if (len == 0) {
-    *err = "empty frame";
-    return ST_BITSTREAM;
-  }
+  FrameState& S = I.s;
+  Job* job = new Job;
+  job->out.blocks.clear();
   try {
-    uint8_t saved_last_type = I.st.last_frame_type;
+    if (len == 0) bitstream_error("empty frame");
+    uint8_t saved_last_type = S.st.last_frame_type;
     ResetKind reset;
     int reset_idx = 0;
     FrameHeader h;
     try {
-      h = parse_uncompressed(data, len, I.st, &reset, &reset_idx);
+      h = parse_uncompressed(data, len, S.st, &reset, &reset_idx);
     } catch (const HeaderError& e) {
       throw ParseError{ST_BITSTREAM, e.msg};
     }
+    // What this frame reads of earlier frames' tile results; the pipeline
+    // settles those frames first.
+    if (after_header) after_header(h);
     if (h.show_existing_frame) {
-      I.st.last_frame_type = saved_last_type;
-      if (!I.slots[h.frame_to_show_map_idx].valid) bitstream_error("show_existing_frame of an empty slot");
-      out->show_existing = true;
-      out->show_slot = h.frame_to_show_map_idx;
-      out->show_frame = true;
-      out->refresh_mask = 0;
-      ++frames_;
-      return ST_OK;
+      S.st.last_frame_type = saved_last_type;
+      if (!S.slots[h.frame_to_show_map_idx].valid) bitstream_error("show_existing_frame of an empty slot");
+      job->show_existing = true;
+      job->out.show_existing = true;
+      job->out.show_slot = h.frame_to_show_map_idx;
+      job->out.show_frame = true;
+      job->out.refresh_mask = 0;
+      return job;
     }
     if ((uint64_t)h.width * h.height > max_pixels_) throw ParseError{ST_UNSUPPORTED, "frame size is above the decoder's limit"};
     if (h.header_size_in_bytes == 0) bitstream_error("compressed header of size 0");
     if (h.profile >= 4) throw ParseError{ST_UNSUPPORTED, "profile above 3"};
-    bool ref_ok[3] = {true, true, true};
     if (!h.frame_is_intra) {
       for (int i = 0; i < 3; ++i) {
-        const SlotInfo& s = I.slots[h.ref_frame_idx[i]];
+        const SlotInfo& s = S.slots[h.ref_frame_idx[i]];
         if (!s.valid) bitstream_error("reference to an empty slot");
         if (s.ss_x != h.ss_x || s.ss_y != h.ss_y || s.bit_depth != h.bit_depth)
           bitstream_error("reference frame of another format");
         // inter_scale's bounds (reference src/decoder/mod.rs:503-511).
-        ref_ok[i] = !(2 * h.width < s.width || 2 * h.height < s.height || h.width > 16 * s.width ||
-                      h.height > 16 * s.height);
+        job->ref_ok[i] = !(2 * h.width < s.width || 2 * h.height < s.height || h.width > 16 * s.width ||
+                           h.height > 16 * s.height);
       }
     }
     // compute_image_size() semantics (7.2.6).
-    bool first = !I.have_last_size;
-    bool same_size = I.have_last_size && I.last_w == h.width && I.last_h == h.height;
+    bool first = !S.have_last_size;
+    bool same_size = S.have_last_size && S.last_w == h.width && S.last_h == h.height;
     size_t mi_len = (size_t)h.mi_rows * h.mi_cols;
-    bool use_prev = !first && same_size && I.last_show_frame && !h.error_resilient_mode && !h.frame_is_intra;
-    if (!same_size) I.prev_segment_ids.assign(mi_len, 0);
-    I.have_last_size = true;
-    I.last_w = h.width;
-    I.last_h = h.height;
-    I.last_show_frame = h.show_frame;
-    if (h.past_independence) std::fill(I.prev_segment_ids.begin(), I.prev_segment_ids.end(), 0);
+    bool use_prev = !first && same_size && S.last_show_frame && !h.error_resilient_mode && !h.frame_is_intra;
+    if (!same_size) S.prev_segment_ids = std::make_shared<std::vector<uint8_t>>(mi_len, 0);
+    S.have_last_size = true;
+    S.last_w = h.width;
+    S.last_h = h.height;
+    S.last_show_frame = h.show_frame;
+    if (h.past_independence) S.prev_segment_ids = std::make_shared<std::vector<uint8_t>>(S.prev_segment_ids->size(), 0);
     if (reset == RESET_ALL) {
-      for (auto& c : I.contexts) c.set_default();
+      for (auto& c : S.contexts) c.set_default();
     } else if (reset == RESET_ONE) {
-      I.contexts[reset_idx].set_default();
+      S.contexts[reset_idx].set_default();
     }
-    Probs probs = I.contexts[h.frame_context_idx];
+    job->pre = S.contexts[h.frame_context_idx];
+    job->probs = job->pre;
     size_t comp_start = h.uncompressed_size;
     size_t comp_end = comp_start + h.header_size_in_bytes;
     if (comp_end > len) bitstream_error("compressed header runs past the end of the frame");
-    parse_compressed(data + comp_start, h.header_size_in_bytes, h, probs);
-    SegParams seg = I.st.seg;
-    const PrevMv* prev = use_prev && I.prev_mvs.size() >= mi_len ? I.prev_mvs.data() : nullptr;
-    const uint8_t* tiles = data + comp_end;
-    size_t tiles_len = len - comp_end;
-    bool non420 = !(h.ss_x == 1 && h.ss_y == 1);
-    h.legacy_uv = non420 && !h.frame_is_intra && I.legacy_uv;
-    Impl::TileResult tr = I.decode_tiles(h, seg, probs, prev, ref_ok, tiles, tiles_len, threads_);
-    if (h.frame_is_intra) {
-      if (non420 && !(tr.st == ST_OK && tr.padding_ok)) {
-        FrameHeader legacy = h;
-        legacy.legacy_uv = true;
-        // Keep the first attempt's records in case the retry fails too.
-        std::vector<TileCoder<DecCoder>> saved;
-        saved.swap(I.tile_decs);
-        Impl::TileResult retry = I.decode_tiles(legacy, seg, probs, prev, ref_ok, tiles, tiles_len, threads_);
-        if (retry.st == ST_OK && retry.padding_ok) {
-          tr = retry;
-          h = legacy;
-        } else {
-          I.tile_decs.swap(saved);
-          // The mode info of the first attempt is lost; only its status matters now.
-          if (tr.st == ST_OK) {
-            // Re-run the first attempt so the records and mode info are its own.
-            tr = I.decode_tiles(h, seg, probs, prev, ref_ok, tiles, tiles_len, threads_);
-          }
-        }
+    parse_compressed(data + comp_start, h.header_size_in_bytes, h, job->probs);
+    job->seg = S.st.seg;
+    job->prev_seg = S.prev_segment_ids;
+    if (use_prev && S.prev_mvs->size() >= mi_len) job->prev_mvs = S.prev_mvs;
+    job->tiles = data + comp_end;
+    job->tiles_len = len - comp_end;
+    job->non420 = !(h.ss_x == 1 && h.ss_y == 1);
+    h.legacy_uv = job->non420 && !h.frame_is_intra && S.legacy_uv;
+    bool adapts = !h.error_resilient_mode && !h.frame_parallel_decoding_mode;
+    job->late_ctx = adapts && h.refresh_frame_context;
+    // The state a tile error returns to.
+    job->snap = S;
+    // Header-decided updates: a context refreshed without adaptation, the
+    // reference slots, the records' frame description.
+    if (h.refresh_frame_context && !adapts) S.contexts[h.frame_context_idx] = job->probs;
+    fill_desc(h, S.st, S.slots, &job->out.desc);
+    job->out.show_frame = h.show_frame;
+    job->out.refresh_mask = h.refresh_frame_flags;
+    for (int i = 0; i < 3; ++i) job->out.ref_slot[i] = h.ref_frame_idx[i];
+    for (int i = 0; i < 8; ++i)
+      if ((h.refresh_frame_flags >> i) & 1) {
+        SlotInfo& sl = S.slots[i];
+        sl.valid = true;
+        sl.width = h.width;
+        sl.height = h.height;
+        sl.ss_x = h.ss_x;
+        sl.ss_y = h.ss_y;
+        sl.bit_depth = h.bit_depth;
+        S.st.ref_w[i] = h.width;
+        S.st.ref_h[i] = h.height;
       }
-      I.legacy_uv = h.legacy_uv;
+    job->h = h;
+  } catch (const ParseError& e) {
+    job->st = e.st;
+    job->err = e.msg ? e.msg : "bitstream error";
+  }
+  return job;
+}
+
+void Parser::run(Job* job) {
+  if (job->st != ST_OK || job->show_existing) return;
+  auto t0 = std::chrono::steady_clock::now();
+  const FrameHeader& h = job->h;
+  TileWork& W = *job->work;
+  const PrevMv* prev = job->prev_mvs ? job->prev_mvs->data() : nullptr;
+  TileResult tr = W.decode_tiles(h, job->seg, job->probs, prev, job->prev_seg.get(), job->ref_ok, job->tiles,
+                                 job->tiles_len, threads_);
+  if (h.frame_is_intra && job->non420 && !(tr.st == ST_OK && tr.padding_ok)) {
+    // Legacy 4:4:4 layout probe (reference README quirk): decode again with
+    // the 4:2:0 chroma layout; keep it if it parses cleanly.
+    FrameHeader legacy = h;
+    legacy.legacy_uv = true;
+    std::vector<TileCoder<DecCoder>> saved;
+    saved.swap(W.tile_decs);
+    TileResult retry = W.decode_tiles(legacy, job->seg, job->probs, prev, job->prev_seg.get(), job->ref_ok,
+                                      job->tiles, job->tiles_len, threads_);
+    if (retry.st == ST_OK && retry.padding_ok) {
+      tr = retry;
+      job->h.legacy_uv = true;
+      job->out.desc.legacy_uv = 1;
+    } else {
+      W.tile_decs.swap(saved);
+      // The mode info of the first attempt is lost: decode it once more.
+      if (tr.st == ST_OK)
+        tr = W.decode_tiles(h, job->seg, job->probs, prev, job->prev_seg.get(), job->ref_ok, job->tiles,
+                            job->tiles_len, threads_);
     }
-    if (tr.st != ST_OK) throw ParseError{tr.st, nullptr};
-    // Gather records in bitstream order of tile columns (tile rows within a
-    // column stay in order; a column reads nothing of another).
+  }
+  job->tr = tr;
+  if (tr.st == ST_OK) {
+    // Records in bitstream order of tile columns (tile rows within a column
+    // stay in order; a column reads nothing of another).
     uint32_t tile_cols = 1u << h.tile_cols_log2;
-    Counts counts;
-    counts.clear();
     size_t nb = 0, nt = 0, nc = 0;
     for (uint32_t c = 0; c < tile_cols; ++c) {
-      nb += I.tile_decs[c].blocks.size();
-      nt += I.tile_decs[c].toks.size();
-      nc += I.tile_decs[c].coefs.size();
+      nb += W.tile_decs[c].blocks.size();
+      nt += W.tile_decs[c].toks.size();
+      nc += W.tile_decs[c].coefs.size();
     }
-    out->blocks.reserve(nb);
-    out->toks.reserve(nt);
-    out->coefs.reserve(nc);
+    ParsedFrame& out = job->out;
+    out.blocks.clear();
+    out.toks.clear();
+    out.coefs.clear();
+    out.blocks.reserve(nb);
+    out.toks.reserve(nt);
+    out.coefs.reserve(nc);
     for (uint32_t c = 0; c < tile_cols; ++c) {
-      TileCoder<DecCoder>& td = I.tile_decs[c];
-      uint32_t tok_base = (uint32_t)out->toks.size(), coef_base = (uint32_t)out->coefs.size();
+      TileCoder<DecCoder>& td = W.tile_decs[c];
+      uint32_t tok_base = (uint32_t)out.toks.size(), coef_base = (uint32_t)out.coefs.size();
       for (rv9_block b : td.blocks) {
         b.tok_start += tok_base;
-        out->blocks.push_back(b);
+        out.blocks.push_back(b);
       }
       for (rv9_tok t : td.toks) {
         t.coef_start += coef_base;
-        out->toks.push_back(t);
+        out.toks.push_back(t);
       }
-      out->coefs.insert(out->coefs.end(), td.coefs.begin(), td.coefs.end());
-      counts.add(td.counts);
+      out.coefs.insert(out.coefs.end(), td.coefs.begin(), td.coefs.end());
     }
-    // Backward adaptation (refresh_probs, 6.1.2).
-    if (!h.error_resilient_mode && !h.frame_parallel_decoding_mode) {
-      const Probs& pre = I.contexts[h.frame_context_idx];
-      Probs adapted = probs;
-      adapted.load_except_tx_skip(pre);
-      adapt_coef_probs(adapted, counts, h.frame_is_intra, h.last_frame_type == KEY_FRAME);
-      if (!h.frame_is_intra) {
-        adapted.load_tx_skip(pre);
-        adapt_noncoef_probs(adapted, counts, h.interpolation_filter == SWITCHABLE, h.tx_mode == TX_MODE_SELECT,
-                            h.allow_high_precision_mv);
-      }
-      probs = adapted;
-    }
-    if (h.refresh_frame_context) I.contexts[h.frame_context_idx] = probs;
-    // Segmentation map for the next frame (8.1 step 3).
-    if (seg.enabled && seg.update_map) {
-      I.prev_segment_ids.resize(mi_len);
-      for (size_t i = 0; i < mi_len; ++i) I.prev_segment_ids[i] = I.mi[i].segment_id;
-    }
-    // PrevMvs / PrevRefFrames (8.10 step 2).
-    I.prev_mvs.resize(mi_len);
-    for (size_t i = 0; i < mi_len; ++i) {
-      const MiInfo& m = I.mi[i];
-      PrevMv& p = I.prev_mvs[i];
-      p.ref_frame[0] = m.ref_frame[0];
-      p.ref_frame[1] = m.ref_frame[1];
-      p.mv[0] = m.mv[0][3];
-      p.mv[1] = m.mv[1][3];
-    }
-    fill_desc(h, I.st, I.slots, &out->desc);
-    out->show_frame = h.show_frame;
-    out->refresh_mask = h.refresh_frame_flags;
-    for (int i = 0; i < 3; ++i) out->ref_slot[i] = h.ref_frame_idx[i];
-    // Reference update (8.10 step 1).
-    for (int i = 0; i < 8; ++i)
-      if ((h.refresh_frame_flags >> i) & 1) {
-        SlotInfo& s = I.slots[i];
-        s.valid = true;
-        s.width = h.width;
-        s.height = h.height;
-        s.ss_x = h.ss_x;
-        s.ss_y = h.ss_y;
-        s.bit_depth = h.bit_depth;
-        I.st.ref_w[i] = h.width;
-        I.st.ref_h[i] = h.height;
-      }
-    ++frames_;
-  } catch (const ParseError& e) {
-    *err = e.msg ? e.msg : "bitstream error";
-    return e.st;
   }
-  out->parse_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  job->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+Status Parser::finish(Job* job, ParsedFrame* out, std::string* err) {
+  Impl& I = *impl_;
+  FrameState& S = I.s;
+  if (job->st != ST_OK) {
+    *err = job->err;
+    return job->st;
+  }
+  if (job->show_existing) {
+    out->blocks.clear();
+    out->toks.clear();
+    out->coefs.clear();
+    out->show_existing = true;
+    out->show_slot = job->out.show_slot;
+    out->show_frame = true;
+    out->refresh_mask = 0;
+    ++frames_;
+    return ST_OK;
+  }
+  const FrameHeader& h = job->h;
+  TileWork& W = *job->work;
+  if (h.frame_is_intra) {
+    // The layout the probe settled on carries to the inter frames that
+    // follow, whether or not the tiles parsed.
+    job->snap.legacy_uv = job->h.legacy_uv;
+  }
+  if (job->tr.st != ST_OK) {
+    // Back to what this frame's header left. Frames before it may have
+    // finished since (the pipeline): their previous motion vectors and
+    // legacy layout stay; nothing else of theirs can be pending then.
+    FrameState now = S;
+    S = job->snap;
+    S.prev_mvs = now.prev_mvs;
+    if (!h.frame_is_intra) S.legacy_uv = now.legacy_uv;
+    *err = job->tr.err.empty() ? "bitstream error" : job->tr.err;
+    return job->tr.st;
+  }
+  if (h.frame_is_intra) S.legacy_uv = job->h.legacy_uv;
+  size_t mi_len = (size_t)h.mi_rows * h.mi_cols;
+  // Backward adaptation (refresh_probs, 6.1.2).
+  if (job->late_ctx) {
+    Counts counts;
+    counts.clear();
+    uint32_t tile_cols = 1u << h.tile_cols_log2;
+    for (uint32_t c = 0; c < tile_cols; ++c) counts.add(W.tile_decs[c].counts);
+    Probs adapted = job->probs;
+    adapted.load_except_tx_skip(job->pre);
+    adapt_coef_probs(adapted, counts, h.frame_is_intra, h.last_frame_type == KEY_FRAME);
+    if (!h.frame_is_intra) {
+      adapted.load_tx_skip(job->pre);
+      adapt_noncoef_probs(adapted, counts, h.interpolation_filter == SWITCHABLE, h.tx_mode == TX_MODE_SELECT,
+                          h.allow_high_precision_mv);
+    }
+    S.contexts[h.frame_context_idx] = adapted;
+  }
+  // Segmentation map for the next frame (8.1 step 3).
+  if (job->seg.enabled && job->seg.update_map) {
+    auto ids = std::make_shared<std::vector<uint8_t>>(mi_len);
+    for (size_t i = 0; i < mi_len; ++i) (*ids)[i] = W.mi[i].segment_id;
+    S.prev_segment_ids = ids;
+  }
+  // PrevMvs / PrevRefFrames (8.10 step 2).
+  auto mvs = std::make_shared<std::vector<PrevMv>>(mi_len);
+  for (size_t i = 0; i < mi_len; ++i) {
+    const MiInfo& m = W.mi[i];
+    PrevMv& p = (*mvs)[i];
+    p.ref_frame[0] = m.ref_frame[0];
+    p.ref_frame[1] = m.ref_frame[1];
+    p.mv[0] = m.mv[0][3];
+    p.mv[1] = m.mv[1][3];
+  }
+  S.prev_mvs = mvs;
+  out->show_existing = false;
+  out->show_frame = job->out.show_frame;
+  out->refresh_mask = job->out.refresh_mask;
+  for (int i = 0; i < 3; ++i) out->ref_slot[i] = job->out.ref_slot[i];
+  out->desc = job->out.desc;
+  out->blocks.swap(job->out.blocks);
+  out->toks.swap(job->out.toks);
+  out->coefs.swap(job->out.coefs);
+  out->parse_seconds = job->seconds;
+  ++frames_;
   return ST_OK;
+}
+
+void Parser::attach_work(Job* job) { job->work = impl_->take_work(); }
+
+void Parser::release(Job* job) {
+  if (!job) return;
+  if (job->th.joinable()) job->th.join();
+  if (job->work) impl_->spare.push_back(std::move(job->work));
+  delete job;
+}
+
+Status Parser::parse_frame(const uint8_t* data, size_t len, ParsedFrame* out, std::string* err) {
+  Job* job = begin(data, len, nullptr);
+  if (job->st == ST_OK && !job->show_existing) {
+    attach_work(job);
+    run(job);
+  }
+  Status st = finish(job, out, err);
+  release(job);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// Frame-parallel parsing.
+
+FramePipeline::FramePipeline(Parser* p, int depth) : p_(p), depth_(depth < 1 ? 1 : depth) {}
+
+FramePipeline::~FramePipeline() {
+  for (Parser::Job* j : q_) p_->release(j);
+}
+
+void FramePipeline::settle() {
+  // Finishes every frame in flight, in order (their results wait in q_).
+  for (Parser::Job* j : q_) {
+    if (j->running) {
+      j->th.join();
+      j->running = false;
+    }
+    if (!j->settled) {
+      j->settled_status = p_->finish(j, &j->settled_out, &j->settled_err);
+      j->settled = true;
+      if (j->settled_status != ST_OK) {
+        failed_ = true;
+        return;
+      }
+    }
+  }
+}
+
+Status FramePipeline::push(const uint8_t* data, size_t len) {
+  if (failed_) return ST_INVALID_INPUT;
+  // The new frame's header runs against the state that the frames before it
+  // leave. Those still in flight settle first, unless the new frame cannot
+  // depend on what they decide at finish: it is a key frame or error
+  // resilient (contexts reset, no previous motion vectors or segment ids),
+  // and no frame in flight adapts a context, carries a segment map or probes
+  // the legacy 4:4:4 layout that this frame would read.
+  bool pending = false, pending_intra_non420 = false;
+  for (Parser::Job* j : q_)
+    if (!j->settled && j->st == ST_OK && !j->show_existing) {
+      pending |= j->late_ctx || (j->seg.enabled && j->seg.update_map);
+      pending_intra_non420 |= j->h.frame_is_intra && j->non420;
+    }
+  Parser::Job* job = p_->begin(data, len, [&](const FrameHeader& h) {
+    bool fresh = h.error_resilient_mode || h.frame_type == KEY_FRAME;
+    bool non420 = !(h.ss_x == 1 && h.ss_y == 1);
+    if (pending || !fresh || h.show_existing_frame || (non420 && pending_intra_non420)) {
+      settle();
+      if (failed_) throw ParseError{ST_INVALID_INPUT, "an earlier frame failed"};
+    }
+  });
+  q_.push_back(job);
+  if (failed_) return ST_OK;  // an earlier frame failed: pop() reports it first
+  if (job->st == ST_OK && !job->show_existing) {
+    p_->attach_work(job);
+    job->running = true;
+    Parser* p = p_;
+    job->th = std::thread([p, job]() { p->run(job); });
+  }
+  return ST_OK;
+}
+
+Status FramePipeline::pop(ParsedFrame* out, std::string* err) {
+  if (q_.empty()) {
+    *err = "no frame in flight";
+    return ST_INVALID_INPUT;
+  }
+  Parser::Job* j = q_.front();
+  q_.pop_front();
+  Status st;
+  if (j->settled) {
+    st = j->settled_status;
+    if (st == ST_OK) {
+      *out = std::move(j->settled_out);
+    } else {
+      *err = j->settled_err;
+    }
+  } else {
+    if (j->running) {
+      j->th.join();
+      j->running = false;
+    }
+    st = p_->finish(j, out, err);
+  }
+  p_->release(j);
+  if (st != ST_OK) {
+    // Frames after a failed one are dropped (the state is the failed
+    // frame's, as the sequential parse leaves it).
+    for (Parser::Job* k : q_) p_->release(k);
+    q_.clear();
+    failed_ = true;
+  }
+  return st;
 }
 
 void superframe_split(const uint8_t* pkt, size_t len, std::vector<std::pair<size_t, size_t>>* out) {

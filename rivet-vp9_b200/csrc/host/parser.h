@@ -11,6 +11,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <deque>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -66,6 +68,10 @@ struct SlotInfo {
   uint32_t ss_x = 1, ss_y = 1, bit_depth = 8;
 };
 
+namespace syn {
+struct FrameHeader;
+}
+
 class Parser {
  public:
   Parser();
@@ -78,6 +84,20 @@ class Parser {
   // fills `err`.
   Status parse_frame(const uint8_t* data, size_t len, ParsedFrame* out, std::string* err);
 
+  // parse_frame in three steps, for frame-parallel parsing (FramePipeline):
+  // begin parses the headers and applies what they decide; `after_header`
+  // (may be empty) runs once the uncompressed header is read, before any
+  // other state is touched. run parses the tiles (any thread; reads only the
+  // job). finish applies what the tiles decide, in frame order, and hands out
+  // the records. Every job ends with release.
+  struct Job;
+  using AfterHeader = std::function<void(const syn::FrameHeader&)>;
+  Job* begin(const uint8_t* data, size_t len, const AfterHeader& after_header);
+  void attach_work(Job* job);
+  void run(Job* job);
+  Status finish(Job* job, ParsedFrame* out, std::string* err);
+  void release(Job* job);
+
   struct Impl;
 
  private:
@@ -85,6 +105,32 @@ class Parser {
   int threads_ = 0;
   uint64_t max_pixels_ = 8192ull * 8192ull;
   uint64_t frames_ = 0;
+};
+
+// Parses the frames of one stream in order with several in flight at once.
+// A frame whose parse may read what an earlier frame's tiles decide (adapted
+// contexts, previous motion vectors or segment ids) waits for those frames;
+// key frames and error-resilient frames do not, so streams made of them parse
+// `depth` frames at a time. Results come out in order, identical to
+// parse_frame's; after an error, the frames behind it are dropped and the
+// parser's state is the failed frame's, as with parse_frame.
+class FramePipeline {
+ public:
+  FramePipeline(Parser* parser, int depth);
+  ~FramePipeline();
+  // Starts a frame (its bytes must stay valid until it is popped).
+  Status push(const uint8_t* data, size_t len);
+  // The oldest frame's records (waits for its tiles).
+  Status pop(ParsedFrame* out, std::string* err);
+  size_t in_flight() const { return q_.size(); }
+  int depth() const { return depth_; }
+
+ private:
+  void settle();
+  Parser* p_;
+  int depth_;
+  std::deque<Parser::Job*> q_;
+  bool failed_ = false;
 };
 
 // Annex B: splits a packet into its frames (reference src/superframe.rs:6-53).

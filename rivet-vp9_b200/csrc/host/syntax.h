@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <memory>
 #include <vector>
 
 #include "../../../include/rv9_records.h"
@@ -123,6 +124,39 @@ inline uint8_t pareto(int node, uint8_t prob) {
   int x1 = x + 1 < 127 ? x + 1 : 127;
   return (uint8_t)(((uint32_t)vp9t_pareto_table[x][node - 2] + vp9t_pareto_table[x1][node - 2]) >> 1);
 }
+
+// A growable array of plain values whose growth leaves the new elements
+// uninitialised: the token loop reserves a block's worth of coefficient
+// words, writes the nonzero ones and gives the rest back.
+template <class T>
+class PodVec {
+ public:
+  size_t size() const { return size_; }
+  T* data() { return buf_.get(); }
+  const T* data() const { return buf_.get(); }
+  const T* begin() const { return buf_.get(); }
+  const T* end() const { return buf_.get() + size_; }
+  void clear() { size_ = 0; }
+  void push_back(T v) { *grow(1) = v; }
+  // `n` more elements at the end, uninitialised; returns the first.
+  T* grow(size_t n) {
+    if (size_ + n > cap_) {
+      size_t cap = std::max(size_ + n, cap_ * 2 + 1024);
+      std::unique_ptr<T[]> b(new T[cap]);
+      if (size_) memcpy(b.get(), buf_.get(), size_ * sizeof(T));
+      buf_ = std::move(b);
+      cap_ = cap;
+    }
+    T* p = buf_.get() + size_;
+    size_ += n;
+    return p;
+  }
+  void shrink_to(size_t n) { size_ = n < size_ ? n : size_; }
+
+ private:
+  std::unique_ptr<T[]> buf_;
+  size_t size_ = 0, cap_ = 0;
+};
 
 // pareto() for every probability value: row p holds the probabilities of
 // token-tree nodes 2..9 when node 1's probability is p.
@@ -405,7 +439,7 @@ struct TileCoder {
   Counts counts;
   std::vector<rv9_block> blocks;
   std::vector<rv9_tok> toks;
-  std::vector<uint32_t> coefs;
+  PodVec<uint32_t> coefs;
   std::vector<uint8_t> left_nonzero[3];
   std::vector<uint8_t> left_partition;
   std::vector<uint8_t> left_seg_pred;
@@ -1346,6 +1380,67 @@ struct TileCoder {
     return coef;
   }
 
+  // The token loop of tokens() for decoding, with the bool decoder's state
+  // in locals and the coefficient words written through a raw pointer;
+  // returns the end of block.
+  int tokens_dec(BoolDecoder& bdec, int tx_sz, int ptype, int ref_type, int ctx, const uint16_t* scan,
+                 const uint16_t (*nb)[2], const uint8_t* bands, const uint8_t (*cp)[6][3], bool count, int seg_eob,
+                 uint32_t bit_depth) {
+    BoolDecoder::State r = bdec.save();
+    const size_t base = coefs.size();
+    uint32_t* out = coefs.grow(seg_eob);
+    uint32_t n_out = 0;
+    uint8_t* tc = token_cache;
+    bool check_eob = true;
+    int c = 0;
+    for (; c < seg_eob; ++c) {
+      const int pos = scan[c];
+      const int band = bands[c];
+      if (c > 0) ctx = (1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1;
+      const uint8_t* probs = cp[band][ctx];
+      if (check_eob) {
+        bool more = BoolDecoder::read(r, probs[0]);
+        if (count) counts.more_coefs[tx_sz][ptype][ref_type][band][ctx][more ? 1 : 0] += 1;
+        if (!more) break;
+      }
+      int token;
+      if (!BoolDecoder::read(r, probs[1])) {
+        token = ZERO_TOKEN;
+      } else if (!BoolDecoder::read(r, probs[2])) {
+        token = 1;  // ONE_TOKEN
+      } else {
+        // The rest of the token tree, its probabilities from one pareto row.
+        const uint8_t* pp = pareto_row(probs[2]);
+        int n = 4;
+        do {
+          n = TOKEN_TREE[n + (int)BoolDecoder::read(r, pp[(n >> 1) - 2])];
+        } while (n > 0);
+        token = -n;
+      }
+      if (count) counts.token[tx_sz][ptype][ref_type][band][ctx][token < 2 ? token : 2] += 1;
+      tc[pos] = vp9t_energy_class[token];
+      if (token == ZERO_TOKEN) {
+        check_eob = false;
+        continue;
+      }
+      int32_t coef = EXTRA_BITS[token][2];
+      const int num_extra = EXTRA_BITS[token][1];
+      if (num_extra) {
+        if (token == DCT_VAL_CAT6)
+          for (int e = 0; e < (int)bit_depth - 8; ++e)
+            coef += (int32_t)BoolDecoder::read(r, 255) << (5 + (int)bit_depth - e);
+        const uint8_t* cat = CAT_PROBS[EXTRA_BITS[token][0]];
+        for (int e = 0; e < num_extra; ++e) coef += (int32_t)BoolDecoder::read(r, cat[e]) << (num_extra - 1 - e);
+      }
+      const bool sign = BoolDecoder::read(r, 128);
+      out[n_out++] = RV9_COEF_PACK(pos, sign ? -coef : coef);
+      check_eob = true;
+    }
+    coefs.shrink_to(base + n_out);
+    bdec.load(r);
+    return c;
+  }
+
   // tokens() (spec 6.4.24): records the nonzero coefficients; returns eob.
   int tokens(C& d, int plane, uint32_t start_x, uint32_t start_y, int tx_sz, int block_idx) {
     int seg_eob = 16 << (tx_sz << 1);
@@ -1383,6 +1478,9 @@ struct TileCoder {
     const int32_t* wc = nullptr;
     int w_eob = 0;
     if (C::kEncode) wc = enc_->tx_coefs(eb_, plane, start_x, start_y, tx_sz, scan, &w_eob);
+    if constexpr (!C::kEncode) {
+      c = tokens_dec(d.bd, tx_sz, ptype, ref_type, ctx, scan, nb, bands, cp, count, seg_eob, bd);
+    } else {
     for (; c < seg_eob; ++c) {
       int pos = scan[c];
       int band = bands[c];
@@ -1393,27 +1491,8 @@ struct TileCoder {
         if (count) counts.more_coefs[tx_sz][ptype][ref_type][band][ctx][more ? 1 : 0] += 1;
         if (!more) break;
       }
-      int token;
-      if constexpr (!C::kEncode) {
-        // The token tree unrolled past its first two nodes; the remaining
-        // nodes' probabilities come from one pareto row.
-        BoolDecoder& r = d.bd;
-        if (!r.read(probs[1])) {
-          token = ZERO_TOKEN;
-        } else if (!r.read(probs[2])) {
-          token = 1;  // ONE_TOKEN
-        } else {
-          const uint8_t* pp = pareto_row(probs[2]);
-          int n = 4;
-          do {
-            n = TOKEN_TREE[n + (int)r.read(pp[(n >> 1) - 2])];
-          } while (n > 0);
-          token = -n;
-        }
-      } else {
-        token = d.tree(TOKEN_TREE, [&](int node) { return pareto(node, probs[(1 + node) < 2 ? (1 + node) : 2]); },
-                       [&] { return token_of(wc[pos]); });
-      }
+      int token = d.tree(TOKEN_TREE, [&](int node) { return pareto(node, probs[(1 + node) < 2 ? (1 + node) : 2]); },
+                         [&] { return token_of(wc[pos]); });
       if (count) counts.token[tx_sz][ptype][ref_type][band][ctx][token < 2 ? token : 2] += 1;
       token_cache[pos] = vp9t_energy_class[token];
       if (token == ZERO_TOKEN) {
@@ -1424,6 +1503,7 @@ struct TileCoder {
         coefs.push_back(RV9_COEF_PACK(pos, sign ? -coef : coef));
         check_eob = true;
       }
+    }
     }
     if (c > 0) ++eob_total;
     t.eob = (uint16_t)c;

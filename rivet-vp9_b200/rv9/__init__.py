@@ -67,7 +67,7 @@ class CStats(ctypes.Structure):
 
 
 # Every symbol include/rv9.h declares.
-EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv9_decoder_set_max_pixels",
+EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv9_decoder_set_parse_depth", "rv9_decoder_set_max_pixels",
            "rv9_decoder_frames_decoded", "rv9_last_error", "rv9_last_global_error", "rv9_decode_all",
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
@@ -96,6 +96,7 @@ def load_library(path=None):
     lib.rv9_decoder_new.argtypes = [ctypes.c_int]
     lib.rv9_decoder_free.argtypes = [vp]
     lib.rv9_decoder_set_threads.argtypes = [vp, ctypes.c_uint32]
+    lib.rv9_decoder_set_parse_depth.argtypes = [vp, ctypes.c_uint32]
     lib.rv9_decoder_set_max_pixels.argtypes = [vp, ctypes.c_uint64]
     lib.rv9_decoder_frames_decoded.restype = ctypes.c_uint64
     lib.rv9_decoder_frames_decoded.argtypes = [vp]
@@ -245,6 +246,10 @@ class Decoder:
 
     def set_threads(self, n):
         self._lib.rv9_decoder_set_threads(self._dec, n)
+
+    def set_parse_depth(self, frames):
+        """Frames parsed at once by decode_packets / load_sequence (0: auto)."""
+        self._lib.rv9_decoder_set_parse_depth(self._dec, frames)
 
     def set_max_pixels(self, n):
         self._lib.rv9_decoder_set_max_pixels(self._dec, n)
