@@ -264,6 +264,23 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
   fw->o_coefs = put(out, pf.coefs.data(), pf.coefs.size());
   fw->o_units = put(out, units_.data(), units_.size());
   fw->o_res = put(out, res_.data(), res_.size());
+  // The intra wavefront takes its items in list order, one per free warp:
+  // superblocks in anti-diagonal order (d = column + 2 row; every superblock
+  // an intra block reads from lies on an earlier diagonal), bitstream order
+  // within a superblock. Bitstream order alone would keep the warps in flight
+  // on about one superblock row at a time.
+  if (!intra_.empty()) {
+    std::vector<std::pair<uint64_t, uint32_t>> key(intra_.size());
+    for (size_t i = 0; i < intra_.size(); ++i) {
+      const rv9_block& b = pf.blocks[intra_[i].block];
+      uint64_t d = (uint64_t)(b.mi_col >> 3) + 2 * (uint64_t)(b.mi_row >> 3);
+      key[i] = {(d << 32) | i, (uint32_t)i};
+    }
+    std::sort(key.begin(), key.end());
+    sorted_intra_.resize(intra_.size());
+    for (size_t i = 0; i < key.size(); ++i) sorted_intra_[i] = intra_[key[i].second];
+    intra_.swap(sorted_intra_);
+  }
   fw->o_intra = put(out, intra_.data(), intra_.size());
   out->resize(align256(out->size()));
   fw->bytes = out->size() - base;

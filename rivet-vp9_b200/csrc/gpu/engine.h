@@ -177,7 +177,7 @@ class Engine {
   // Work lists of the frame being built.
   std::vector<InterUnit> units_;
   std::vector<ResItem> res_;
-  std::vector<IntraItem> intra_;
+  std::vector<IntraItem> intra_, sorted_intra_;
 };
 
 }  // namespace rv9g

@@ -300,30 +300,49 @@ __device__ void itx_add(typename V::store_t* s, uint32_t rows, int tx_type, bool
 }
 
 // A transform block's residual added to dst (the prediction), by one warp.
+// The residual every sample of a DC-only block gets (the reference's
+// dc_only_value, src/dsp/itx.rs:684-694; exact for the 64-bit lane too,
+// whose products here fit 32 bits).
+template <class V>
+__device__ int dc_only_residual(const KFrame& k, const rv9_tok& t, int seg) {
+  const int n = 2 + t.tx_size;
+  int pt = t.plane ? 1 : 0;
+  int32_t dc = 0;
+  if (t.n_coef > 0) {
+    uint32_t w = k.coefs[t.coef_start];
+    int64_t dq = (int64_t)RV9_COEF_VAL(w) * k.dc_q[seg][pt];
+    if (t.tx_size == 3) dq /= 2;
+    dq = dq < INT32_MIN ? INT32_MIN : (dq > INT32_MAX ? INT32_MAX : dq);
+    dc = (int32_t)dq;
+  }
+  int shift = (n + 2) < 6 ? (n + 2) : 6;
+  V v = V::load(dc).mul(11585).rshift(14);
+  V w2 = V::load((int32_t)v.v).mul(11585).rshift(14);
+  // The 64-bit lane multiplies the low 32 bits: v fits them.
+  if (sizeof(typename V::store_t) == 4) w2 = v.mul(11585).rshift(14);
+  return w2.rshift(shift).residual();
+}
+
+template <class V, class T>
+__device__ void itx_add_size(int tx_size, typename V::store_t* s, uint32_t rows, int tx_type, bool lossless, T* dst,
+                             int dstride, int maxv, int lane) {
+  switch (tx_size) {
+    case 0: itx_add<V, 2>(s, rows, tx_type, lossless, dst, dstride, maxv, lane); break;
+    case 1: itx_add<V, 3>(s, rows, tx_type, lossless, dst, dstride, maxv, lane); break;
+    case 2: itx_add<V, 4>(s, rows, tx_type, lossless, dst, dstride, maxv, lane); break;
+    default: itx_add<V, 5>(s, rows, tx_type, lossless, dst, dstride, maxv, lane); break;
+  }
+}
+
+// Dequantise, inverse transform and add the residual of `t` to `dst`.
 template <class V, class T>
 __device__ void residual_add(const KFrame& k, const rv9_tok& t, int seg, T* dst, int dstride,
                              typename V::store_t* s, int lane) {
   const int maxv = (1 << k.bit_depth) - 1;
   const int n = 2 + t.tx_size, n0 = 1 << n;
   if (t.eob == 1 && t.tx_type == 0 && !k.lossless) {
-    // Only the DC coefficient: every sample gets the same residual (the
-    // reference's dc_only_value, src/dsp/itx.rs:684-694; exact for the
-    // 64-bit lane too, whose products here fit 32 bits).
-    int pt = t.plane ? 1 : 0;
-    int32_t dc = 0;
-    if (t.n_coef > 0) {
-      uint32_t w = k.coefs[t.coef_start];
-      int64_t dq = (int64_t)RV9_COEF_VAL(w) * k.dc_q[seg][pt];
-      if (t.tx_size == 3) dq /= 2;
-      dq = dq < INT32_MIN ? INT32_MIN : (dq > INT32_MAX ? INT32_MAX : dq);
-      dc = (int32_t)dq;
-    }
-    int shift = (n + 2) < 6 ? (n + 2) : 6;
-    V v = V::load(dc).mul(11585).rshift(14);
-    V w2 = V::load((int32_t)v.v).mul(11585).rshift(14);
-    // The 64-bit lane multiplies the low 32 bits: v fits them.
-    if (sizeof(typename V::store_t) == 4) w2 = v.mul(11585).rshift(14);
-    int res = w2.rshift(shift).residual();
+    // Only the DC coefficient: every sample gets the same residual.
+    int res = dc_only_residual<V>(k, t, seg);
     for (int i = lane; i < n0 * n0; i += 32) {
       int r = i >> n, c = i & (n0 - 1);
       T* px = dst + (size_t)r * dstride + c;
@@ -333,12 +352,7 @@ __device__ void residual_add(const KFrame& k, const rv9_tok& t, int seg, T* dst,
     return;
   }
   uint32_t rows = load_coefs<V>(k, t, seg, s, lane);
-  switch (t.tx_size) {
-    case 0: itx_add<V, 2>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
-    case 1: itx_add<V, 3>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
-    case 2: itx_add<V, 4>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
-    default: itx_add<V, 5>(s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane); break;
-  }
+  itx_add_size<V, T>(t.tx_size, s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane);
 }
 
 constexpr int kResWarps = 4;
@@ -389,6 +403,25 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
     const bool have_left = it.flags & 1, have_above = it.flags & 2;
     const bool not_on_right = it.flags & 4;
     const int x = it.x, y = it.y;
+    // The residual does not depend on the neighbours: its coefficients are
+    // dequantised into shared memory (or its DC-only value taken) before
+    // the wait, off the wavefront's critical path.
+    bool dc_only = false;
+    int dc_res = 0;
+    uint32_t rows = 0;
+    int tx_type = 0, res_tx = 0;
+    if (it.tok != NO_TOK) {
+      const rv9_tok t = k.toks[it.tok];
+      const int seg = k.blocks[it.block].segment_id;
+      tx_type = t.tx_type;
+      res_tx = t.tx_size;
+      if (t.eob == 1 && t.tx_type == 0 && !k.lossless) {
+        dc_only = true;
+        dc_res = dc_only_residual<V>(k, t, seg);
+      } else {
+        rows = load_coefs<V>(k, t, seg, sm->s, lane);
+      }
+    }
     // Wait for the cells the edges read: row y-1 and column x-1.
     {
       const uint8_t* cells = k.cells[plane];
@@ -454,8 +487,12 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
     }
     __syncwarp();
     if (it.tok != NO_TOK) {
-      const rv9_tok& t = k.toks[it.tok];
-      residual_add<V, int32_t>(k, t, k.blocks[it.block].segment_id, sm->pred, size, sm->s, lane);
+      if (dc_only) {
+        for (int i = lane; i < size * size; i += 32) sm->pred[i] = clampi(sm->pred[i] + dc_res, 0, maxv);
+        __syncwarp();
+      } else {
+        itx_add_size<V, int32_t>(res_tx, sm->s, rows, tx_type, k.lossless, sm->pred, size, maxv, lane);
+      }
     }
     T* dst = plane_ptr<T>(k.cur[plane]) + (size_t)y * stride + x;
     for (int i = lane; i < size * size; i += 32) {
