@@ -492,9 +492,24 @@ RV9_HD void lf_at(int pass, int sub_x, int sub_y, int row, int col, int e, int r
   }
 }
 
+// Where the per-8x8 loop-filter records come from: the frame's array, or a
+// superblock's 8x8 of them staged in shared memory.
+struct LfMiFrame {
+  const uint32_t* p;
+  int stride;
+  RV9_HD uint32_t operator()(int r, int c) const { return p[(size_t)r * stride + c]; }
+};
+struct LfMiTile {
+  const uint32_t* t;  // 8 x 8, row-major
+  int row0, col0;
+  RV9_HD uint32_t operator()(int r, int c) const { return t[(r - row0) * 8 + (c - col0)]; }
+};
+
 // The filter of edge `ed`, run `rn` of pass `pass` (0 vertical, 1 horizontal)
 // of plane `plane` in the superblock at mode-info (row, col).
-RV9_HD LfEdge lf_edge_entry(const LfParams& k, int plane, int pass, int row, int col, int ed, int rn) {
+template <class MiAt>
+RV9_HD LfEdge lf_edge_entry_at(const LfParams& k, const MiAt& mi_at, int plane, int pass, int row, int col, int ed,
+                               int rn) {
   LfEdge e{-1, 0, 0, 0};
   const int sub_x = plane ? k.ss_x : 0, sub_y = plane ? k.ss_y : 0;
   const int sub = pass == 0 ? sub_x : sub_y;
@@ -504,7 +519,7 @@ RV9_HD LfEdge lf_edge_entry(const LfParams& k, int plane, int pass, int row, int
   if (x >= 8 * k.mi_cols || y >= 8 * k.mi_rows) return e;
   int loop_col = ((x >> 3) >> sub_x) << sub_x;
   int loop_row = ((y >> 3) >> sub_y) << sub_y;
-  uint32_t m = k.lf_mi[(size_t)loop_row * k.mi_cols + loop_col];
+  uint32_t m = mi_at(loop_row, loop_col);
   int l = m & 63;
   if (l == 0) return e;
   int tx_sz = plane ? ((m >> 8) & 3) : ((m >> 6) & 3);
@@ -541,6 +556,10 @@ RV9_HD LfEdge lf_edge_entry(const LfParams& k, int plane, int pass, int row, int
   e.blimit = k.blimit[l];
   e.thresh = k.thresh[l];
   return e;
+}
+
+RV9_HD LfEdge lf_edge_entry(const LfParams& k, int plane, int pass, int row, int col, int ed, int rn) {
+  return lf_edge_entry_at(k, LfMiFrame{k.lf_mi, k.mi_cols}, plane, pass, row, col, ed, rn);
 }
 
 // The loop-filter record of a block (the MiInfo fields the filter reads).

@@ -361,9 +361,11 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
     CK(cudaMemsetAsync(d_sb_done_, 0, n_sb * 4, stream_));
     sb_cap_ = n_sb;
   }
-  if (!fixed_ && ++epoch_ == 0) {
+  // The loop filter's progress words carry the epoch's low 16 bits: clear
+  // them when those wrap, so that no stale word can match.
+  if (!fixed_ && ((++epoch_) & 0xffff) == 0) {
     CK(cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_));
-    epoch_ = 1;
+    ++epoch_;
   }
   KFrame k;
   memset(&k, 0, sizeof k);

@@ -71,7 +71,7 @@ struct KFrame {
   uint8_t lvl[8][4][2];
   uint8_t lf_limit[64], lf_blimit[64], lf_thresh[64];
   int32_t lf_on;
-  uint32_t* sb_done;        // per superblock: epoch when its filtering is done
+  uint32_t* sb_done;        // loop filter: per superblock row, epoch << 16 | superblocks done
   uint32_t epoch;
   int32_t* counters;        // [0] intra tickets, [1] lf tickets
   int32_t* error;           // nonzero: a device wait timed out (code)

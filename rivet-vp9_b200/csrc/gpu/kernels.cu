@@ -16,9 +16,10 @@
 //   k_intra       intra prediction + residual as a dependency wavefront:
 //                 a persistent grid takes transform blocks in bitstream order
 //                 and each warp waits only for the 4x4 cells its edges read
-//   k_lf          loop filter as a superblock wavefront: superblock (r, c)
-//                 waits for (r, c-1) and (r-1, c+1), then filters its
-//                 vertical then horizontal edges in shared memory
+//   k_lf_rows     loop filter: one CTA per superblock row, left to right,
+//                 each superblock's vertical then horizontal edges in shared
+//                 memory; a row waits only for the row above to be one
+//                 superblock ahead
 //
 // Inter prediction reads only reference frames, so it runs fully parallel
 // before the intra wavefront. Every wait is bounded: on timeout a kernel
@@ -517,7 +518,6 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
 // ---------------------------------------------------------------------------
 // Loop filter wavefront.
 
-constexpr int kLfThreads = 192;
 constexpr int kLfW = 80;   // tile row pitch (int16): 8 left + 64 + 8 of slack
 constexpr int kLfH = 72;   // 8 above + 64
 
@@ -628,155 +628,236 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
   for (int q = 0; q < 72; ++q) col[q * kLfW] = (int16_t)v[q];
 }
 
-// The superblock of ticket t, tickets in wavefront order: anti-diagonals
-// d = c + 2r in turn, rows ascending within one. Every dependency of (r, c)
-// lies on diagonal d-1 or d-2, so a grid about one diagonal wide keeps every
-// CTA busy, and consecutive tickets are independent.
-__device__ __forceinline__ void lf_ticket_sb(int t, int cols, int rows, int* sr, int* sc) {
-  for (int d = 0;; ++d) {
-    int r_lo = d - cols + 1 > 0 ? (d - cols + 2) >> 1 : 0;
-    int r_hi = (d >> 1) < rows - 1 ? (d >> 1) : rows - 1;
-    int n = r_hi - r_lo + 1;
-    if (n > 0) {
-      if (t < n) {
-        *sr = r_lo + t;
-        *sc = d - 2 * (r_lo + t);
-        return;
-      }
-      t -= n;
+// ---------------------------------------------------------------------------
+// Loop filter, one CTA per superblock row.
+//
+// A CTA owns a superblock row and filters its superblocks left to right, as
+// the reference does (vertical then horizontal edges per superblock,
+// src/decoder/loopfilter.rs:466-620). The strip that superblock c's filters
+// share with c+1 stays in shared memory, so the only wait is on the row
+// above: superblock (r, c)'s horizontal pass reads the row above's bottom
+// strip, final once that row has finished superblock c+1 (whose vertical
+// pass reaches 7 samples back into c). Each row publishes its progress as
+// (epoch << 16 | superblocks done).
+//
+// Warps 0-3 filter: vertical pass, top strip, horizontal pass. Warps 4-5
+// do the rest off that chain: they stage the next superblock (its 8x8
+// loop-filter records, edge decisions and 64x64 interior) into the other of
+// two buffers, hand the right strip over, and write filtered samples back
+// and publish progress. The two groups meet at two named barriers per
+// superblock: HDONE (filters -> stagers) and READY (stagers -> filters).
+
+constexpr int kLfRowThreads = 192;
+constexpr int kLfFilterThreads = 128;
+constexpr int kLfStageThreads = kLfRowThreads - kLfFilterThreads;
+constexpr int kBarFilter = 1, kBarStage = 2, kBarHDone = 3, kBarReady = 4;
+
+struct LfRowSmem {
+  int16_t px[2][3][kLfH][kLfW];
+  LfEdge edges[2][2][2][16][16];  // [buffer][luma, chroma][pass][edge][run]
+  uint32_t mi[2][64];
+  uint8_t limit[64], blimit[64], thresh[64];
+  int row;
+  int abort_flag;
+};
+
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Stages superblock (sr, sc) into buffer `b`: records, edge decisions (the
+// two chroma planes share theirs), interior. Run by `n` threads numbered
+// `t`, synchronised by barrier `bar` (0: the whole CTA).
+template <class T>
+__device__ void lf_row_prepare(const KFrame& k, LfRowSmem& S, const LfParams& P, int sr, int sc, int b, int t, int n,
+                               int bar) {
+  for (int i = t; i < 64; i += n) {
+    int mr = sr * 8 + (i >> 3), mc = sc * 8 + (i & 7);
+    S.mi[b][i] = (mr < k.mi_rows && mc < k.mi_cols) ? k.lf_mi[(size_t)mr * k.mi_cols + mc] : 0u;
+  }
+  if (bar == 0)
+    __syncthreads();
+  else
+    named_sync(bar, n);
+  const LfMiTile at{S.mi[b], sr * 8, sc * 8};
+  // Luma: 2 passes x 16 edges x 16 runs; chroma: its edges and runs only.
+  const int ce0 = 16 >> k.ss_x, ce1 = 16 >> k.ss_y;  // chroma edges of pass 0 / 1 (runs: the other)
+  const int n_luma = 512, n_c0 = ce0 * ce1, n_total = n_luma + 2 * n_c0;
+  for (int i = t; i < n_total; i += n) {
+    int plane, pass, ed, rn;
+    if (i < n_luma) {
+      plane = 0;
+      pass = i >> 8;
+      ed = (i >> 4) & 15;
+      rn = i & 15;
+    } else {
+      int j = i - n_luma;
+      plane = 1;
+      pass = j >= n_c0;
+      j -= pass * n_c0;
+      const int ne = pass ? ce1 : ce0, nrun = pass ? ce0 : ce1;
+      ed = j / nrun;
+      rn = j - ed * nrun;
+      (void)ne;
+    }
+    S.edges[b][plane][pass][ed][rn] = lf_edge_entry_at(P, at, plane, pass, sr * 8, sc * 8, ed, rn);
+  }
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    const int sxp = p ? k.ss_x : 0, syp = p ? k.ss_y : 0;
+    const int nc = (64 >> sxp) / 8, nr = 64 >> syp;
+    const int x0 = (sc * 64) >> sxp, y0 = (sr * 64) >> syp;
+    const T* src = plane_ptr<const T>(k.cur[p]);
+    const int stride = k.cur[p].stride;
+    for (int i = t; i < nr * nc; i += n) {
+      int r = i / nc, c = i - r * nc;
+      Chunk<T>::load(src + (size_t)(y0 + r) * stride + x0 + 8 * c, &S.px[b][p][8 + r][8 + 8 * c]);
     }
   }
 }
 
-// One superblock (all three planes) per ticket.
-// The 64x64 interior of a superblock is untouched by the filtering of earlier
-// superblocks, so it is loaded before waiting; only the strips 8 samples
-// left and above (filtered by (r, c-1) and the row above) are loaded after.
 template <class T>
-__global__ void __launch_bounds__(kLfThreads) k_lf(KFrame k) {
-  __shared__ __align__(16) int16_t px[3][kLfH][kLfW];
-  __shared__ LfEdge edges[3][2][16][16];
-  __shared__ int ticket;
-  __shared__ int abort_flag;
-  const int n_sb = k.sb64_cols * k.sb64_rows;
+__global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
+  extern __shared__ __align__(16) unsigned char lf_raw[];
+  LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
+  const int tid = threadIdx.x;
   const int bd = k.bit_depth;
+  const int cols = k.sb64_cols, rows = k.sb64_rows;
+  const uint32_t ep = (uint32_t)(k.epoch & 0xffff) << 16;
+  for (int i = tid; i < 64; i += kLfRowThreads) {
+    S.limit[i] = k.lf_limit[i];
+    S.blimit[i] = k.lf_blimit[i];
+    S.thresh[i] = k.lf_thresh[i];
+  }
+  const LfParams P{k.mi_cols, k.mi_rows, k.ss_x, k.ss_y, nullptr, S.limit, S.blimit, S.thresh};
+  int W[3], Hh[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    W[p] = 64 >> (p ? k.ss_x : 0);
+    Hh[p] = 64 >> (p ? k.ss_y : 0);
+  }
   for (;;) {
-    if (threadIdx.x == 0) {
-      int tk = atomicAdd(&k.counters[1], 1), r = 0, c = 0;
-      if (tk < n_sb) lf_ticket_sb(tk, k.sb64_cols, k.sb64_rows, &r, &c);
-      ticket = tk < n_sb ? r * k.sb64_cols + c : n_sb;
+    if (tid == 0) {
+      S.row = atomicAdd(&k.counters[1], 1);
+      S.abort_flag = 0;
     }
     __syncthreads();
-    const int t = ticket;  // the superblock's raster index
+    const int sr = S.row;
+    if (sr >= rows) return;
+    lf_row_prepare<T>(k, S, P, sr, 0, 0, tid, kLfRowThreads, 0);
     __syncthreads();
-    if (t >= n_sb) return;
-    const int sr = t / k.sb64_cols, sc = t - sr * k.sb64_cols;
-    const int row = sr * 8, col = sc * 8;
-    const LfParams P{k.mi_cols, k.mi_rows, k.ss_x, k.ss_y, k.lf_mi, k.lf_limit, k.lf_blimit, k.lf_thresh};
-    int nch[3], nrw[3], x0s[3], y0s[3];
-#pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      const int sxp = p ? k.ss_x : 0, syp = p ? k.ss_y : 0;
-      nch[p] = (64 >> sxp) / 8 + 1;  // 8-sample chunks per tile row, the left strip included
-      nrw[p] = (64 >> syp) + 8;
-      x0s[p] = (col * 8) >> sxp;
-      y0s[p] = (row * 8) >> syp;
-    }
-    // Edge decisions, and the interior (tile rows >= 8, chunks >= 1).
-    for (int i = threadIdx.x; i < 3 * 2 * 256; i += kLfThreads) {
-      int plane = i / 512, pass = (i >> 8) & 1, ed = (i >> 4) & 15, rn = i & 15;
-      edges[plane][pass][ed][rn] = lf_edge_entry(P, plane, pass, row, col, ed, rn);
-    }
-#pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      const T* src = plane_ptr<const T>(k.cur[p]);
-      const int stride = k.cur[p].stride;
-      const int nc = nch[p] - 1, nr = nrw[p] - 8;
-      for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
-        int r = i / nc, c = i - r * nc;
-        Chunk<T>::load(src + (size_t)(y0s[p] + r) * stride + x0s[p] + 8 * c, &px[p][8 + r][8 + 8 * c]);
-      }
-    }
-    // Wait for (r, c-1) and (r-1, c+1) (or (r-1, c) at the last column).
-    if (threadIdx.x == 0) {
-      abort_flag = 0;
-      const volatile uint32_t* done = k.sb_done;
-      int polls = 0;
-      int deps[2] = {sc > 0 ? t - 1 : -1, sr > 0 ? (t - k.sb64_cols + (sc + 1 < k.sb64_cols ? 1 : 0)) : -1};
-      for (int d = 0; d < 2 && !abort_flag; ++d) {
-        if (deps[d] < 0) continue;
-        while (done[deps[d]] != k.epoch) {
-          if (*(volatile int32_t*)k.error || ++polls > kWaitLimit) {
-            atomicCAS(k.error, 0, 2);
-            abort_flag = 1;
-            break;
+    if (tid < kLfFilterThreads) {
+      // ---- filters ----
+      const int tf = tid;
+      for (int sc = 0, cur = 0; sc < cols; ++sc, cur ^= 1) {
+        if (sc > 0) named_sync(kBarReady, kLfRowThreads);
+        const bool live = !S.abort_flag;
+        if (live) {
+          // Vertical edges, one thread per sample row.
+          const int total = Hh[0] + Hh[1] + Hh[2];
+          for (int task = tf; task < total; task += kLfFilterThreads) {
+            int p = task < Hh[0] ? 0 : (task < Hh[0] + Hh[1] ? 1 : 2);
+            int r = task - (p == 0 ? 0 : (p == 1 ? Hh[0] : Hh[0] + Hh[1]));
+            lf_row_regs(&S.px[cur][p][8 + r][0], S.edges[cur][p ? 1 : 0][0], 16 >> (p ? k.ss_x : 0), r >> 2, bd);
           }
-          if (polls > 64) __nanosleep(32);
         }
-      }
-      __threadfence();
-    }
-    __syncthreads();
-    if (abort_flag) return;
-    // The strips: left (tile rows >= 8, chunk 0) and top (rows < 8, chunks >= 1).
-#pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      const T* src = plane_ptr<const T>(k.cur[p]);
-      const int stride = k.cur[p].stride;
-      const int nl = sc > 0 ? nrw[p] - 8 : 0;
-      const int nt = sr > 0 ? 8 * (nch[p] - 1) : 0;
-      for (int i = threadIdx.x; i < nl + nt; i += kLfThreads) {
-        int r, c;
-        if (i < nl) {
-          r = 8 + i;
-          c = 0;
-        } else {
-          int j = i - nl;
-          r = j / (nch[p] - 1);
-          c = 1 + j - r * (nch[p] - 1);
+        // Wait for the row above to finish superblock c+1.
+        if (live && sr > 0 && tf == 0) {
+          const volatile uint32_t* prog = k.sb_done + (sr - 1);
+          const uint32_t need = (uint32_t)(sc + 2);
+          int polls = 0;
+          for (;;) {
+            uint32_t v = *prog;
+            if ((v & 0xffff0000u) == ep && (v & 0xffffu) >= need) break;
+            if (*(volatile int32_t*)k.error || ++polls > kWaitLimit) {
+              atomicCAS(k.error, 0, 2);
+              S.abort_flag = 1;
+              break;
+            }
+            if (polls > 32) __nanosleep(32);
+          }
+          __threadfence();
         }
-        Chunk<T>::load(src + (size_t)(y0s[p] - 8 + r) * stride + x0s[p] - 8 + 8 * c, &px[p][r][8 * c]);
-      }
-    }
-    __syncthreads();
-    // Vertical edges, one thread per sample row.
-    {
-      const int r0 = nrw[0] - 8, r1 = nrw[1] - 8;
-      const int total = r0 + 2 * r1;
-      for (int task = threadIdx.x; task < total; task += kLfThreads) {
-        int p = task < r0 ? 0 : (task < r0 + r1 ? 1 : 2);
-        int r = task - (p == 0 ? 0 : (p == 1 ? r0 : r0 + r1));
-        lf_row_regs(&px[p][8 + r][0], edges[p][0], 16 >> (p ? k.ss_x : 0), r >> 2, bd);
-      }
-    }
-    __syncthreads();
-    // Horizontal edges, one thread per sample column.
-    {
-      const int c0 = 8 * (nch[0] - 1), c1 = 8 * (nch[1] - 1);
-      const int total = c0 + 2 * c1;
-      for (int task = threadIdx.x; task < total; task += kLfThreads) {
-        int p = task < c0 ? 0 : (task < c0 + c1 ? 1 : 2);
-        int c = task - (p == 0 ? 0 : (p == 1 ? c0 : c0 + c1));
-        lf_col_regs(&px[p][0][8 + c], edges[p][1], 16 >> (p ? k.ss_y : 0), c >> 2, bd);
-      }
-    }
-    __syncthreads();
-    // Write back everything but the corner, 8 samples at a time.
+        named_sync(kBarFilter, kLfFilterThreads);
+        if (!S.abort_flag) {
+          // The top strip: the row above's bottom 8 rows.
+          if (sr > 0) {
 #pragma unroll
-    for (int p = 0; p < 3; ++p) {
-      T* dst = plane_ptr<T>(k.cur[p]);
-      const int stride = k.cur[p].stride;
-      const int nc = nch[p], nr = nrw[p];
-      for (int i = threadIdx.x; i < nr * nc; i += kLfThreads) {
-        int r = i / nc, c = i - r * nc;
-        int gy = y0s[p] - 8 + r, gx = x0s[p] - 8 + 8 * c;
-        if ((r >= 8 || c >= 1) && gy >= 0 && gx >= 0)
-          Chunk<T>::store(dst + (size_t)gy * stride + gx, &px[p][r][8 * c]);
+            for (int p = 0; p < 3; ++p) {
+              const T* src = plane_ptr<const T>(k.cur[p]);
+              const int stride = k.cur[p].stride;
+              const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
+              const int nc = W[p] / 8;
+              for (int i = tf; i < 8 * nc; i += kLfFilterThreads) {
+                int r = i / nc, c = i - r * nc;
+                Chunk<T>::load(src + (size_t)(y0 - 8 + r) * stride + x0 + 8 * c, &S.px[cur][p][r][8 + 8 * c]);
+              }
+            }
+            named_sync(kBarFilter, kLfFilterThreads);
+          }
+          // Horizontal edges, one thread per sample column.
+          const int total = W[0] + W[1] + W[2];
+          for (int task = tf; task < total; task += kLfFilterThreads) {
+            int p = task < W[0] ? 0 : (task < W[0] + W[1] ? 1 : 2);
+            int c = task - (p == 0 ? 0 : (p == 1 ? W[0] : W[0] + W[1]));
+            lf_col_regs(&S.px[cur][p][0][8 + c], S.edges[cur][p ? 1 : 0][1], 16 >> (p ? k.ss_y : 0), c >> 2, bd);
+          }
+        }
+        named_arrive(kBarHDone, kLfRowThreads);
+      }
+    } else {
+      // ---- stagers ----
+      const int ts = tid - kLfFilterThreads;
+      if (cols > 1) lf_row_prepare<T>(k, S, P, sr, 1, 1, ts, kLfStageThreads, kBarStage);
+      for (int sc = 0, cur = 0; sc < cols; ++sc, cur ^= 1) {
+        const int nxt = cur ^ 1;
+        named_sync(kBarHDone, kLfRowThreads);
+        // This superblock's right strip becomes the next one's left strip.
+        if (sc + 1 < cols) {
+#pragma unroll
+          for (int p = 0; p < 3; ++p)
+            for (int r = ts; r < Hh[p]; r += kLfStageThreads)
+              *reinterpret_cast<int4*>(&S.px[nxt][p][8 + r][0]) =
+                  *reinterpret_cast<const int4*>(&S.px[cur][p][8 + r][W[p]]);
+          named_arrive(kBarReady, kLfRowThreads);
+        }
+        if (!S.abort_flag) {
+#pragma unroll
+          for (int p = 0; p < 3; ++p) {
+            T* dst = plane_ptr<T>(k.cur[p]);
+            const int stride = k.cur[p].stride;
+            const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
+            const int nc = W[p] / 8;
+            // The left strip: superblock c-1's last 8 columns, final since
+            // this superblock's vertical pass.
+            if (sc > 0)
+              for (int r = ts; r < Hh[p]; r += kLfStageThreads)
+                Chunk<T>::store(dst + (size_t)(y0 + r) * stride + x0 - 8, &S.px[cur][p][8 + r][0]);
+            // The top strip, and the superblock but its last 8 columns (the
+            // next superblock's vertical pass still reaches them), or with
+            // them at the row's end.
+            const int r0 = sr > 0 ? 0 : 8;
+            const int nrow = 8 + Hh[p] - r0;
+            const bool last = sc + 1 == cols;
+            for (int i = ts; i < nrow * nc; i += kLfStageThreads) {
+              int r = r0 + i / nc, c = i % nc;
+              if (r >= 8 && c == nc - 1 && !last) continue;
+              Chunk<T>::store(dst + (size_t)(y0 - 8 + r) * stride + x0 + 8 * c, &S.px[cur][p][r][8 + 8 * c]);
+            }
+          }
+          __threadfence();
+        }
+        named_sync(kBarStage, kLfStageThreads);
+        if (ts == 0) *(volatile uint32_t*)&k.sb_done[sr] = ep | (uint32_t)(sc + 1 < cols ? sc + 1 : cols + 1);
+        // Stage superblock c+2 into this superblock's buffer, now written back.
+        if (sc + 2 < cols) lf_row_prepare<T>(k, S, P, sr, sc + 2, cur, ts, kLfStageThreads, kBarStage);
       }
     }
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) *(volatile uint32_t*)&k.sb_done[t] = k.epoch;
+    if (S.abort_flag) return;
   }
 }
 
@@ -840,14 +921,15 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
     ++L;
   }
   if (k.lf_on) {
-    // Two diagonals' worth of CTAs: one filtering, one loading ahead.
-    int n_sb = k.sb64_cols * k.sb64_rows;
-    int diag = (k.sb64_cols + 1) / 2 < k.sb64_rows ? (k.sb64_cols + 1) / 2 : k.sb64_rows;
-    int grid = 2 * diag + 2;
-    grid = grid < n_sb ? grid : n_sb;
-    grid = grid < n_sm * 3 ? grid : n_sm * 3;
+    // One CTA per superblock row (rows are taken in order from a ticket).
+    static bool lf_attr_set = false;
+    if (!lf_attr_set) {
+      cudaFuncSetAttribute(k_lf_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LfRowSmem));
+      lf_attr_set = true;
+    }
+    int grid = k.sb64_rows < n_sm ? k.sb64_rows : n_sm;
     mark(K_LF, 0);
-    k_lf<T><<<grid, kLfThreads, 0, s>>>(k);
+    k_lf_rows<T><<<grid, kLfRowThreads, sizeof(LfRowSmem), s>>>(k);
     mark(K_LF, 1);
     ++L;
   }
