@@ -640,14 +640,14 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
 // pass reaches 7 samples back into c). Each row publishes its progress as
 // (epoch << 16 | superblocks done).
 //
-// Warps 0-3 filter: vertical pass, top strip, horizontal pass. Warps 4-5
+// Warps 0-3 filter: vertical pass, top strip, horizontal pass. Warps 4-7
 // do the rest off that chain: they stage the next superblock (its 8x8
 // loop-filter records, edge decisions and 64x64 interior) into the other of
 // two buffers, hand the right strip over, and write filtered samples back
 // and publish progress. The two groups meet at two named barriers per
 // superblock: HDONE (filters -> stagers) and READY (stagers -> filters).
 
-constexpr int kLfRowThreads = 192;
+constexpr int kLfRowThreads = 256;
 constexpr int kLfFilterThreads = 128;
 constexpr int kLfStageThreads = kLfRowThreads - kLfFilterThreads;
 constexpr int kBarFilter = 1, kBarStage = 2, kBarHDone = 3, kBarReady = 4;
@@ -712,6 +712,7 @@ __device__ void lf_row_prepare(const KFrame& k, LfRowSmem& S, const LfParams& P,
     const int x0 = (sc * 64) >> sxp, y0 = (sr * 64) >> syp;
     const T* src = plane_ptr<const T>(k.cur[p]);
     const int stride = k.cur[p].stride;
+#pragma unroll 4
     for (int i = t; i < nr * nc; i += n) {
       int r = i / nc, c = i - r * nc;
       Chunk<T>::load(src + (size_t)(y0 + r) * stride + x0 + 8 * c, &S.px[b][p][8 + r][8 + 8 * c]);
