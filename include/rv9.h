@@ -130,10 +130,13 @@ void rv9_decoder_stats(rv9_decoder* dec, rv9_stats* out, int reset);
 typedef struct rv9_sequence rv9_sequence;
 rv9_status rv9_sequence_load(rv9_decoder* dec, const uint8_t* const* packets, const size_t* lens, size_t n,
                              rv9_sequence** out);
+/* Flags of rv9_sequence_run / rv9_sequences_run. */
+#define RV9_RUN_PER_KERNEL 1 /* bracket each launch with events for rv9_kernel_stats */
+#define RV9_RUN_GRAPH 2      /* replay the run as a CUDA graph, captured on first use
+                                (after one ordinary run); per-kernel timing is off */
 /* Reconstructs the sequence; *device_ms receives the CUDA-event time of the
- * run on the decoder's stream. With per_kernel, each launch is bracketed by
- * events for rv9_kernel_stats. */
-rv9_status rv9_sequence_run(rv9_decoder* dec, rv9_sequence* seq, int per_kernel, double* device_ms);
+ * run on the decoder's stream. */
+rv9_status rv9_sequence_run(rv9_decoder* dec, rv9_sequence* seq, int flags, double* device_ms);
 /* rv9_sequence_run without allocating. No counterpart in the reference
  * (whose decoder has no device and no replay): this entry point exists for
  * callers that must not allocate device memory while they decode — a
@@ -167,7 +170,7 @@ rv9_status rv9_sequence_run_noalloc(rv9_decoder* dec, rv9_sequence* seq, double*
  * issued round-robin, so independent streams' kernels overlap on the GPU.
  * *device_ms receives the CUDA-event time from the common start to the last
  * stream's end. A multi-stream throughput form with no reference counterpart. */
-rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int per_kernel,
+rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int flags,
                              double* device_ms);
 uint32_t rv9_sequence_frames(const rv9_sequence* seq);
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* seq);     /* visible luma of shown frames */

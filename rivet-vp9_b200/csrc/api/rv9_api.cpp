@@ -242,9 +242,11 @@ rv9_status rv9_sequence_clone(rv9_decoder* d, const rv9_sequence* src, rv9_seque
   return RV9_OK;
 }
 
-rv9_status rv9_sequence_run(rv9_decoder* d, rv9_sequence* s, int per_kernel, double* device_ms) {
+rv9_status rv9_sequence_run(rv9_decoder* d, rv9_sequence* s, int flags, double* device_ms) {
   float ms = 0;
-  rv9::Status st = d->engine.sequence_run(s->seq, per_kernel != 0, &ms, &d->err);
+  rv9::Status st = (flags & RV9_RUN_GRAPH) ? d->engine.sequence_replay(s->seq, &ms, &d->err)
+                                           : d->engine.sequence_run(s->seq, (flags & RV9_RUN_PER_KERNEL) != 0, &ms,
+                                                                    &d->err);
   *device_ms = ms;
   return (rv9_status)st;
 }
@@ -257,7 +259,7 @@ rv9_status rv9_sequence_run_noalloc(rv9_decoder* d, rv9_sequence* s, double* dev
   return (rv9_status)st;
 }
 
-rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int per_kernel,
+rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int flags,
                              double* device_ms) {
   if (!device_ms || (n && (!decs || !seqs))) return RV9_INVALID_INPUT;
   *device_ms = 0;
@@ -270,7 +272,8 @@ rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs
   }
   float ms = 0;
   std::string err;
-  rv9::Status st = rv9g::Engine::run_concurrent(engines.data(), ss.data(), n, per_kernel != 0, &ms, &err);
+  rv9::Status st = rv9g::Engine::run_concurrent(engines.data(), ss.data(), n, (flags & RV9_RUN_PER_KERNEL) != 0, &ms,
+                                                &err, (flags & RV9_RUN_GRAPH) != 0);
   if (st != rv9::ST_OK && n) decs[0]->err = err;
   *device_ms = ms;
   return (rv9_status)st;

@@ -588,8 +588,69 @@ rv9::Status Engine::sequence_run(const Sequence& seq, bool per_kernel, float* ms
   return rv9::ST_OK;
 }
 
+rv9::Status Engine::sequence_graph(const Sequence& seq, std::string* err) {
+  if (seq.graph) return rv9::ST_OK;
+  float ms = 0;
+  rv9::Status st = sequence_run(seq, false, &ms, err);
+  if (st != rv9::ST_OK) return st;
+  device_ms -= ms;
+  uint64_t frames0 = frames, launches0 = launches, bytes0 = alg_bytes;
+  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_);
+  reset_slots();
+  for (size_t i = 0; e == cudaSuccess && st == rv9::ST_OK && i < seq.frames.size(); ++i) {
+    DevFrame* shown = nullptr;
+    st = run_frame(seq.frames[i], seq.d_data, false, &shown, err);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(stream_, &g);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess && st == rv9::ST_OK) e = cudaGraphInstantiate(&seq.graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  // The capture ran the host side once; the replays account for themselves.
+  seq.graph_launches = launches - launches0;
+  frames = frames0;
+  launches = launches0;
+  alg_bytes = bytes0;
+  for (int i = 0; i < 8; ++i) seq.graph_slots[i] = slots_[i];
+  if (st != rv9::ST_OK) return st;
+  if (e != cudaSuccess) {
+    seq.graph = nullptr;
+    *err = std::string("capturing the sequence: ") + cudaGetErrorString(e);
+    return rv9::ST_DEVICE;
+  }
+  return rv9::ST_OK;
+}
+
+// After a replay the reference slots are those the captured run left.
+static void adopt_slots(DevFrame** slots, DevFrame* const* from) {
+  for (int i = 0; i < 8; ++i) {
+    if (slots[i]) --slots[i]->refs;
+    slots[i] = from[i];
+    if (slots[i]) ++slots[i]->refs;
+  }
+}
+
+rv9::Status Engine::sequence_replay(const Sequence& seq, float* ms, std::string* err) {
+  rv9::Status st = sequence_graph(seq, err);
+  if (st != rv9::ST_OK) return st;
+  CK(cudaEventRecord(ev0_, stream_));
+  CK(cudaGraphLaunch(seq.graph, stream_));
+  CK(cudaEventRecord(ev1_, stream_));
+  st = sync(err);
+  if (st != rv9::ST_OK) return st;
+  CK(cudaEventElapsedTime(ms, ev0_, ev1_));
+  adopt_slots(slots_, seq.graph_slots);
+  device_ms += *ms;
+  frames += seq.frames.size();
+  launches += seq.graph_launches;
+  for (const FrameWork& fw : seq.frames) alg_bytes += fw.total_bytes;
+  return rv9::ST_OK;
+}
+
 rv9::Status Engine::run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n, bool per_kernel,
-                                   float* ms, std::string* err) {
+                                   float* ms, std::string* err, bool graphs) {
   if (n == 0) {
     *ms = 0;
     return rv9::ST_OK;
@@ -606,21 +667,37 @@ rv9::Status Engine::run_concurrent(Engine* const* engines, const Sequence* const
         return rv9::ST_INVALID_INPUT;
       }
   }
+  if (graphs)
+    for (size_t j = 0; j < n; ++j) {
+      rv9::Status st = engines[j]->sequence_graph(*seqs[j], err);
+      if (st != rv9::ST_OK) return st;
+    }
   // Every stream starts after the start event on engines[0]'s stream.
   CK(cudaEventRecord(e0->ev0_, e0->stream_));
   for (size_t j = 0; j < n; ++j) {
-    engines[j]->reset_slots();
+    if (!graphs) engines[j]->reset_slots();
     if (j) CK(cudaStreamWaitEvent(engines[j]->stream_, e0->ev0_, 0));
   }
-  size_t most = 0;
-  for (size_t j = 0; j < n; ++j) most = std::max(most, seqs[j]->frames.size());
-  for (size_t i = 0; i < most; ++i)
+  if (graphs) {
     for (size_t j = 0; j < n; ++j) {
-      if (i >= seqs[j]->frames.size()) continue;
-      DevFrame* shown = nullptr;
-      rv9::Status st = engines[j]->run_frame(seqs[j]->frames[i], seqs[j]->d_data, per_kernel, &shown, err);
-      if (st != rv9::ST_OK) return st;
+      CK(cudaGraphLaunch(seqs[j]->graph, engines[j]->stream_));
+      adopt_slots(engines[j]->slots_, seqs[j]->graph_slots);
+      engines[j]->frames += seqs[j]->frames.size();
+      engines[j]->launches += seqs[j]->graph_launches;
+      for (const FrameWork& fw : seqs[j]->frames) engines[j]->alg_bytes += fw.total_bytes;
     }
+    per_kernel = false;
+  } else {
+    size_t most = 0;
+    for (size_t j = 0; j < n; ++j) most = std::max(most, seqs[j]->frames.size());
+    for (size_t i = 0; i < most; ++i)
+      for (size_t j = 0; j < n; ++j) {
+        if (i >= seqs[j]->frames.size()) continue;
+        DevFrame* shown = nullptr;
+        rv9::Status st = engines[j]->run_frame(seqs[j]->frames[i], seqs[j]->d_data, per_kernel, &shown, err);
+        if (st != rv9::ST_OK) return st;
+      }
+  }
   // engines[0]'s stream waits for every other stream's end.
   for (size_t j = 1; j < n; ++j) {
     CK(cudaEventRecord(engines[j]->ev1_, engines[j]->stream_));
@@ -810,6 +887,11 @@ rv9::Status Engine::sequence_clone(const Sequence& src, Sequence* seq, std::stri
 }
 
 void Engine::sequence_free(Sequence* seq) {
+  if (seq->graph) {
+    cudaStreamSynchronize(stream_);
+    cudaGraphExecDestroy(seq->graph);
+    seq->graph = nullptr;
+  }
   if (seq->d_data) {
     cudaStreamSynchronize(stream_);
     cudaFree(seq->d_data);

@@ -68,11 +68,17 @@ struct FrameWork {
 };
 
 // Parsed frames resident in device memory, for repeated reconstruction.
+struct DevFrame;
 struct Sequence {
   std::vector<FrameWork> frames;
   uint8_t* d_data = nullptr;
   size_t bytes = 0;
   uint64_t luma_samples = 0;  // visible, shown frames
+  // The whole run captured as a CUDA graph (Engine::sequence_graph), with
+  // the launches it holds and the reference slots it leaves.
+  mutable cudaGraphExec_t graph = nullptr;
+  mutable uint64_t graph_launches = 0;
+  mutable DevFrame* graph_slots[8] = {nullptr};
 };
 
 struct KernelStat {
@@ -101,13 +107,20 @@ class Engine {
   // Reconstructs every frame of `seq` from scratch (empty slots first);
   // returns the CUDA-event time of the whole run.
   rv9::Status sequence_run(const Sequence& seq, bool per_kernel, float* ms, std::string* err);
+  // Captures `seq`'s run as a CUDA graph once (after one ordinary run, which
+  // fills the frame pool and the scratch so that the capture allocates
+  // nothing), then replays it: the steady state without per-launch host
+  // work. The graph clears the loop filter's progress words before and
+  // after the frames, so the epochs baked into it can repeat.
+  rv9::Status sequence_graph(const Sequence& seq, std::string* err);
+  rv9::Status sequence_replay(const Sequence& seq, float* ms, std::string* err);
   // Reconstructs several sequences at once, one per engine (all engines
   // distinct, on one device), each on its engine's own CUDA stream with
   // frames issued round-robin, so that the streams' kernels overlap on the
   // device. *ms is the CUDA-event time from the first launch to the last
   // completion, on engines[0]'s stream.
   static rv9::Status run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
-                                    bool per_kernel, float* ms, std::string* err);
+                                    bool per_kernel, float* ms, std::string* err, bool graphs = false);
   int device() const { return device_; }
   // The device error word as last copied back (nonzero after a wavefront
   // wait gave up; sync() reports and clears it).

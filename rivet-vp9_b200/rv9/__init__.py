@@ -144,11 +144,13 @@ class Sequence:
         self.algorithmic_bytes = L.rv9_sequence_algorithmic_bytes(handle)
         self.record_bytes = L.rv9_sequence_record_bytes(handle)
 
-    def run(self, per_kernel=False):
+    def run(self, per_kernel=False, graph=False):
         """Reconstructs every frame on the device; returns the CUDA-event
-        milliseconds of the run."""
+        milliseconds of the run. `graph`: replay a CUDA graph of the run
+        (captured on first use)."""
         ms = ctypes.c_double()
-        st = self._dec._lib.rv9_sequence_run(self._dec._dec, self._h, 1 if per_kernel else 0, ctypes.byref(ms))
+        flags = (RV9_RUN_PER_KERNEL if per_kernel else 0) | (RV9_RUN_GRAPH if graph else 0)
+        st = self._dec._lib.rv9_sequence_run(self._dec._dec, self._h, flags, ctypes.byref(ms))
         if st != RV9_OK:
             _raise(self._dec._lib, self._dec._dec, st)
         return ms.value
@@ -171,7 +173,11 @@ class Sequence:
             self._h = None
 
 
-def run_concurrent(pairs, per_kernel=False):
+RV9_RUN_PER_KERNEL = 1
+RV9_RUN_GRAPH = 2
+
+
+def run_concurrent(pairs, per_kernel=False, graph=False):
     """Reconstructs several (decoder, sequence) pairs at once, each decoder on
     its own CUDA stream (rv9_sequences_run); returns the CUDA-event
     milliseconds from the common start to the last stream's end."""
@@ -182,7 +188,8 @@ def run_concurrent(pairs, per_kernel=False):
     decs = (ctypes.c_void_p * n)(*[d._dec for d, _ in pairs])
     seqs = (ctypes.c_void_p * n)(*[s._h for _, s in pairs])
     ms = ctypes.c_double()
-    st = lib.rv9_sequences_run(decs, seqs, n, 1 if per_kernel else 0, ctypes.byref(ms))
+    flags = (RV9_RUN_PER_KERNEL if per_kernel else 0) | (RV9_RUN_GRAPH if graph else 0)
+    st = lib.rv9_sequences_run(decs, seqs, n, flags, ctypes.byref(ms))
     if st != RV9_OK:
         _raise(lib, pairs[0][0]._dec, st)
     return ms.value

@@ -108,3 +108,31 @@ def test_clone_replays_the_same():
     finally:
         a.close()
         b.close()
+
+
+def test_graph_replay_equals_run():
+    # RV9_RUN_GRAPH: the run captured as a CUDA graph and replayed gives the
+    # same reference slots, replay after replay, alone and concurrently.
+    import rv9
+    decs = [rv9.Decoder(0) for _ in NAMES[:4]]
+    seqs = [d.load_sequence(read_packets(os.path.join(VECTORS_DIR, n))) for d, n in zip(decs, NAMES[:4])]
+    try:
+        want = []
+        for d, s in zip(decs, seqs):
+            s.run()
+            want.append(_slots(d))
+        for rep in range(2):
+            for d, s, w in zip(decs, seqs, want):
+                assert s.run(graph=True) > 0
+                assert _slots(d) == w
+        for rep in range(2):
+            rv9.run_concurrent(list(zip(decs, seqs)), graph=True)
+            for d, w in zip(decs, want):
+                assert _slots(d) == w
+        # An ordinary run after replays still matches.
+        seqs[0].run()
+        assert _slots(decs[0]) == want[0]
+    finally:
+        for d, s in zip(decs, seqs):
+            s.free()
+            d.close()
