@@ -636,21 +636,25 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
 // src/decoder/loopfilter.rs:466-620). The strip that superblock c's filters
 // share with c+1 stays in shared memory, so the only wait is on the row
 // above: superblock (r, c)'s horizontal pass reads the row above's bottom
-// strip, final once that row has finished superblock c+1 (whose vertical
-// pass reaches 7 samples back into c). Each row publishes its progress as
-// (epoch << 16 | superblocks done).
+// strip, final once that row has written superblock c back and filtered the
+// vertical edges of c+1 (which reach 7 samples back into c). Each row
+// publishes its progress as (epoch << 16 | steps): per superblock one step
+// when it is written back and one when the next superblock's vertical pass
+// has finalised its last 8 columns' bottom strip, so superblock c of the row
+// above is ready at 2 (c + 1) steps.
 //
 // Warps 0-3 filter: vertical pass, top strip, horizontal pass. Warps 4-7
 // do the rest off that chain: they stage the next superblock (its 8x8
 // loop-filter records, edge decisions and 64x64 interior) into the other of
-// two buffers, hand the right strip over, and write filtered samples back
-// and publish progress. The two groups meet at two named barriers per
-// superblock: HDONE (filters -> stagers) and READY (stagers -> filters).
+// two buffers, and write filtered samples back. The groups meet at named
+// barriers: HDONE (filters -> stagers) and READY (stagers -> filters), each
+// alternating between two barriers by superblock parity, since either group
+// may run up to a superblock ahead of the other.
 
 constexpr int kLfRowThreads = 256;
 constexpr int kLfFilterThreads = 128;
 constexpr int kLfStageThreads = kLfRowThreads - kLfFilterThreads;
-constexpr int kBarFilter = 1, kBarStage = 2, kBarHDone = 3, kBarReady = 4;
+constexpr int kBarFilter = 1, kBarStage = 2, kBarReady0 = 4, kBarHDone0 = 6;  // READY, HDONE: id + parity
 
 struct LfRowSmem {
   int16_t px[2][3][kLfH][kLfW];
@@ -742,19 +746,23 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
   }
   for (;;) {
     if (tid == 0) {
-      S.row = atomicAdd(&k.counters[1], 1);
+      const int r = atomicAdd(&k.counters[1], 1);
+      S.row = r;
       S.abort_flag = 0;
+      // This row's progress: two steps per superblock (see below), from 0.
+      if (r < rows) *(volatile uint32_t*)&k.sb_done[r] = ep;
     }
     __syncthreads();
     const int sr = S.row;
     if (sr >= rows) return;
+    uint32_t* const prog = k.sb_done + sr;
     lf_row_prepare<T>(k, S, P, sr, 0, 0, tid, kLfRowThreads, 0);
     __syncthreads();
     if (tid < kLfFilterThreads) {
       // ---- filters ----
       const int tf = tid;
       for (int sc = 0, cur = 0; sc < cols; ++sc, cur ^= 1) {
-        if (sc > 0) named_sync(kBarReady, kLfRowThreads);
+        if (sc > 0) named_sync(kBarReady0 + (sc & 1), kLfRowThreads);
         const bool live = !S.abort_flag;
         if (live) {
           // Vertical edges, one thread per sample row.
@@ -764,14 +772,29 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
             int r = task - (p == 0 ? 0 : (p == 1 ? Hh[0] : Hh[0] + Hh[1]));
             lf_row_regs(&S.px[cur][p][8 + r][0], S.edges[cur][p ? 1 : 0][0], 16 >> (p ? k.ss_x : 0), r >> 2, bd);
           }
+          // Superblock c-1's last 8 columns are final for this row now: they
+          // go out at once (the row below waits for their bottom 8 rows).
+          if (sc > 0) {
+            const int total_l = Hh[0] + Hh[1] + Hh[2];
+            for (int task = tf; task < total_l; task += kLfFilterThreads) {
+              int p = task < Hh[0] ? 0 : (task < Hh[0] + Hh[1] ? 1 : 2);
+              int r = task - (p == 0 ? 0 : (p == 1 ? Hh[0] : Hh[0] + Hh[1]));
+              const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
+              Chunk<T>::store(plane_ptr<T>(k.cur[p]) + (size_t)(y0 + r) * k.cur[p].stride + x0 - 8,
+                              &S.px[cur][p][8 + r][0]);
+            }
+            __threadfence();
+          }
         }
-        // Wait for the row above to finish superblock c+1.
+        named_sync(kBarFilter, kLfFilterThreads);
+        if (live && sc > 0 && tf == 0) atomicAdd(prog, 1u);
+        // Wait for the row above: superblock c's bottom strip final there.
         if (live && sr > 0 && tf == 0) {
-          const volatile uint32_t* prog = k.sb_done + (sr - 1);
-          const uint32_t need = (uint32_t)(sc + 2);
+          const volatile uint32_t* above = k.sb_done + (sr - 1);
+          const uint32_t need = 2u * (uint32_t)(sc + 1);
           int polls = 0;
           for (;;) {
-            uint32_t v = *prog;
+            uint32_t v = *above;
             if ((v & 0xffff0000u) == ep && (v & 0xffffu) >= need) break;
             if (*(volatile int32_t*)k.error || ++polls > kWaitLimit) {
               atomicCAS(k.error, 0, 2);
@@ -806,25 +829,31 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
             int c = task - (p == 0 ? 0 : (p == 1 ? W[0] : W[0] + W[1]));
             lf_col_regs(&S.px[cur][p][0][8 + c], S.edges[cur][p ? 1 : 0][1], 16 >> (p ? k.ss_y : 0), c >> 2, bd);
           }
+          named_sync(kBarFilter, kLfFilterThreads);
+          // This superblock's right strip becomes the next one's left strip.
+          if (sc + 1 < cols) {
+            const int nxt = cur ^ 1;
+            const int total_r = Hh[0] + Hh[1] + Hh[2];
+            for (int task = tf; task < total_r; task += kLfFilterThreads) {
+              int p = task < Hh[0] ? 0 : (task < Hh[0] + Hh[1] ? 1 : 2);
+              int r = task - (p == 0 ? 0 : (p == 1 ? Hh[0] : Hh[0] + Hh[1]));
+              *reinterpret_cast<int4*>(&S.px[nxt][p][8 + r][0]) =
+                  *reinterpret_cast<const int4*>(&S.px[cur][p][8 + r][W[p]]);
+            }
+          }
         }
-        named_arrive(kBarHDone, kLfRowThreads);
+        named_arrive(kBarHDone0 + (sc & 1), kLfRowThreads);
       }
     } else {
       // ---- stagers ----
       const int ts = tid - kLfFilterThreads;
-      if (cols > 1) lf_row_prepare<T>(k, S, P, sr, 1, 1, ts, kLfStageThreads, kBarStage);
+      if (cols > 1) {
+        lf_row_prepare<T>(k, S, P, sr, 1, 1, ts, kLfStageThreads, kBarStage);
+        named_arrive(kBarReady0 + 1, kLfRowThreads);
+      }
       for (int sc = 0, cur = 0; sc < cols; ++sc, cur ^= 1) {
-        const int nxt = cur ^ 1;
-        named_sync(kBarHDone, kLfRowThreads);
-        // This superblock's right strip becomes the next one's left strip.
-        if (sc + 1 < cols) {
-#pragma unroll
-          for (int p = 0; p < 3; ++p)
-            for (int r = ts; r < Hh[p]; r += kLfStageThreads)
-              *reinterpret_cast<int4*>(&S.px[nxt][p][8 + r][0]) =
-                  *reinterpret_cast<const int4*>(&S.px[cur][p][8 + r][W[p]]);
-          named_arrive(kBarReady, kLfRowThreads);
-        }
+        named_sync(kBarHDone0 + (sc & 1), kLfRowThreads);
+        const bool last = sc + 1 == cols;
         if (!S.abort_flag) {
 #pragma unroll
           for (int p = 0; p < 3; ++p) {
@@ -832,17 +861,11 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
             const int stride = k.cur[p].stride;
             const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
             const int nc = W[p] / 8;
-            // The left strip: superblock c-1's last 8 columns, final since
-            // this superblock's vertical pass.
-            if (sc > 0)
-              for (int r = ts; r < Hh[p]; r += kLfStageThreads)
-                Chunk<T>::store(dst + (size_t)(y0 + r) * stride + x0 - 8, &S.px[cur][p][8 + r][0]);
             // The top strip, and the superblock but its last 8 columns (the
             // next superblock's vertical pass still reaches them), or with
             // them at the row's end.
             const int r0 = sr > 0 ? 0 : 8;
             const int nrow = 8 + Hh[p] - r0;
-            const bool last = sc + 1 == cols;
             for (int i = ts; i < nrow * nc; i += kLfStageThreads) {
               int r = r0 + i / nc, c = i % nc;
               if (r >= 8 && c == nc - 1 && !last) continue;
@@ -852,9 +875,18 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
           __threadfence();
         }
         named_sync(kBarStage, kLfStageThreads);
-        if (ts == 0) *(volatile uint32_t*)&k.sb_done[sr] = ep | (uint32_t)(sc + 1 < cols ? sc + 1 : cols + 1);
+        // One step of the row's progress per superblock written back (two
+        // at the row's end, whose last strip goes out here); the filters add
+        // the other step when they write the superblock's last 8 columns,
+        // final after the next superblock's vertical pass. (The filters own
+        // columns 0-7 of a buffer: they overwrite them with the next left
+        // strip while this group may still be writing the buffer back.)
+        if (ts == 0) atomicAdd(prog, last ? 2u : 1u);
         // Stage superblock c+2 into this superblock's buffer, now written back.
-        if (sc + 2 < cols) lf_row_prepare<T>(k, S, P, sr, sc + 2, cur, ts, kLfStageThreads, kBarStage);
+        if (sc + 2 < cols) {
+          lf_row_prepare<T>(k, S, P, sr, sc + 2, cur, ts, kLfStageThreads, kBarStage);
+          named_arrive(kBarReady0 + ((sc + 2) & 1), kLfRowThreads);
+        }
       }
     }
     __syncthreads();
