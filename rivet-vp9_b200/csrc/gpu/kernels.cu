@@ -526,6 +526,17 @@ template <class T>
 struct Chunk;
 template <>
 struct Chunk<uint8_t> {
+  // The raw 8 samples, loaded ahead of the tile store.
+  using Raw = uint2;
+  static __device__ __forceinline__ Raw ldg(const uint8_t* g) { return __ldcg(reinterpret_cast<const uint2*>(g)); }
+  static __device__ __forceinline__ void put(Raw v, int16_t* t) {
+    int4 o;
+    o.x = (int)(v.x & 0xff) | (int)((v.x >> 8) & 0xff) << 16;
+    o.y = (int)((v.x >> 16) & 0xff) | (int)(v.x >> 24) << 16;
+    o.z = (int)(v.y & 0xff) | (int)((v.y >> 8) & 0xff) << 16;
+    o.w = (int)((v.y >> 16) & 0xff) | (int)(v.y >> 24) << 16;
+    *reinterpret_cast<int4*>(t) = o;
+  }
   static __device__ __forceinline__ void load(const uint8_t* g, int16_t* t) {
     uint2 v = __ldcg(reinterpret_cast<const uint2*>(g));
     int4 o;
@@ -547,6 +558,9 @@ struct Chunk<uint8_t> {
 };
 template <>
 struct Chunk<uint16_t> {
+  using Raw = int4;
+  static __device__ __forceinline__ Raw ldg(const uint16_t* g) { return __ldcg(reinterpret_cast<const int4*>(g)); }
+  static __device__ __forceinline__ void put(Raw v, int16_t* t) { *reinterpret_cast<int4*>(t) = v; }
   static __device__ __forceinline__ void load(const uint16_t* g, int16_t* t) {
     *reinterpret_cast<int4*>(t) = __ldcg(reinterpret_cast<const int4*>(g));
   }
@@ -764,6 +778,36 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
       for (int sc = 0, cur = 0; sc < cols; ++sc, cur ^= 1) {
         if (sc > 0) named_sync(kBarReady0 + (sc & 1), kLfRowThreads);
         const bool live = !S.abort_flag;
+        // The top strip (the row above's bottom 8 rows), loaded into
+        // registers before the vertical pass when the row above is already
+        // far enough; after the wait below otherwise.
+        const int need = 2 * (sc + 1);
+        typename Chunk<T>::Raw top[2];
+        bool top_early = false;
+        const int top_total = 8 * (W[0] + W[1] + W[2]) / 8;
+        auto top_addr = [&](int i) -> const T* {
+          int p = i < W[0] ? 0 : (i < W[0] + W[1] ? 1 : 2);
+          int j = i - (p == 0 ? 0 : (p == 1 ? W[0] : W[0] + W[1]));  // chunk within the plane's 8 rows
+          const int nc = W[p] / 8, r = j / nc, c = j - r * nc;
+          const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
+          return plane_ptr<const T>(k.cur[p]) + (size_t)(y0 - 8 + r) * k.cur[p].stride + x0 + 8 * c;
+        };
+        auto top_tile = [&](int i) -> int16_t* {
+          int p = i < W[0] ? 0 : (i < W[0] + W[1] ? 1 : 2);
+          int j = i - (p == 0 ? 0 : (p == 1 ? W[0] : W[0] + W[1]));
+          const int nc = W[p] / 8, r = j / nc, c = j - r * nc;
+          return &S.px[cur][p][r][8 + 8 * c];
+        };
+        if (live && sr > 0) {
+          uint32_t v;
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(k.sb_done + (sr - 1)) : "memory");
+          if ((v & 0xffff0000u) == ep && (int)(v & 0xffffu) >= need) {
+            top_early = true;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+              if (tf + q * kLfFilterThreads < top_total) top[q] = Chunk<T>::ldg(top_addr(tf + q * kLfFilterThreads));
+          }
+        }
         if (live) {
           // Vertical edges, one thread per sample row.
           const int total = Hh[0] + Hh[1] + Hh[2];
@@ -783,19 +827,22 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
               Chunk<T>::store(plane_ptr<T>(k.cur[p]) + (size_t)(y0 + r) * k.cur[p].stride + x0 - 8,
                               &S.px[cur][p][8 + r][0]);
             }
-            __threadfence();
           }
         }
         named_sync(kBarFilter, kLfFilterThreads);
-        if (live && sc > 0 && tf == 0) atomicAdd(prog, 1u);
+        // The barrier orders every filter thread's stores before this one
+        // thread's fence, which publishes them with the progress step.
+        if (live && sc > 0 && tf == 0) {
+          __threadfence();
+          atomicAdd(prog, 1u);
+        }
         // Wait for the row above: superblock c's bottom strip final there.
         if (live && sr > 0 && tf == 0) {
           const volatile uint32_t* above = k.sb_done + (sr - 1);
-          const uint32_t need = 2u * (uint32_t)(sc + 1);
           int polls = 0;
           for (;;) {
             uint32_t v = *above;
-            if ((v & 0xffff0000u) == ep && (v & 0xffffu) >= need) break;
+            if ((v & 0xffff0000u) == ep && (int)(v & 0xffffu) >= need) break;
             if (*(volatile int32_t*)k.error || ++polls > kWaitLimit) {
               atomicCAS(k.error, 0, 2);
               S.abort_flag = 1;
@@ -807,18 +854,11 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
         }
         named_sync(kBarFilter, kLfFilterThreads);
         if (!S.abort_flag) {
-          // The top strip: the row above's bottom 8 rows.
           if (sr > 0) {
 #pragma unroll
-            for (int p = 0; p < 3; ++p) {
-              const T* src = plane_ptr<const T>(k.cur[p]);
-              const int stride = k.cur[p].stride;
-              const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
-              const int nc = W[p] / 8;
-              for (int i = tf; i < 8 * nc; i += kLfFilterThreads) {
-                int r = i / nc, c = i - r * nc;
-                Chunk<T>::load(src + (size_t)(y0 - 8 + r) * stride + x0 + 8 * c, &S.px[cur][p][r][8 + 8 * c]);
-              }
+            for (int q = 0; q < 2; ++q) {
+              const int i = tf + q * kLfFilterThreads;
+              if (i < top_total) Chunk<T>::put(top_early ? top[q] : Chunk<T>::ldg(top_addr(i)), top_tile(i));
             }
             named_sync(kBarFilter, kLfFilterThreads);
           }
@@ -872,9 +912,9 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
               Chunk<T>::store(dst + (size_t)(y0 - 8 + r) * stride + x0 + 8 * c, &S.px[cur][p][r][8 + 8 * c]);
             }
           }
-          __threadfence();
         }
         named_sync(kBarStage, kLfStageThreads);
+        if (ts == 0) __threadfence();
         // One step of the row's progress per superblock written back (two
         // at the row's end, whose last strip goes out here); the filters add
         // the other step when they write the superblock's last 8 columns,
