@@ -399,60 +399,69 @@ RV9_HD int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v
 // The wide filter (spec 8.8.5.3): a rounded sliding mean over 2^log2 taps of
 // the samples at -(n+1) .. n (n = 2^(log2-1) - 1), replacing -n .. n-1. All
 // indices are compile-time constants so the line stays in registers.
+// Index t of the wide filter's window, clamped to its ends p(n)..q(n)
+// (relative to the edge at 8).
+RV9_HD constexpr int lfw_at(int t, int n) { return (t < -(n + 1) ? -(n + 1) : (t > n ? n : t)) + 8; }
+
+// The 8- and 16-wide filters (spec 8.8.5.3): each output is the rounded mean
+// of the sample itself and the 2n+1 samples centred on it, the window's ends
+// repeated. The window sum is carried from one output to the next.
 template <int LOG2>
 RV9_HD void lf_wide(int* s) {
   constexpr int n = (1 << (LOG2 - 1)) - 1;
+  int w = 0;
+#pragma unroll
+  for (int j = -n; j <= n; ++j) w += s[lfw_at(-n + j, n)];
   int f[16];
 #pragma unroll
   for (int i = -n; i < n; ++i) {
-    int t = s[i + 8];
-#pragma unroll
-    for (int j = -n; j <= n; ++j) {
-      const int p = (i + j) < -(n + 1) ? -(n + 1) : ((i + j) > n ? n : (i + j));
-      t += s[p + 8];
-    }
-    f[i + 8] = (t + (1 << (LOG2 - 1))) >> LOG2;
+    f[i + 8] = (s[i + 8] + w + (1 << (LOG2 - 1))) >> LOG2;
+    w += s[lfw_at(i + n + 1, n)] - s[lfw_at(i - n, n)];
   }
 #pragma unroll
   for (int i = -n; i < n; ++i) s[i + 8] = f[i + 8];
 }
 
+RV9_HD int imax(int a, int b) { return a > b ? a : b; }
+
 RV9_HD void lf_line(int* s, int filter_size, int limit, int blimit, int thresh, int bd) {
-  int q0 = s[8], q1 = s[9], q2 = s[10], q3 = s[11];
-  int p0 = s[7], p1 = s[6], p2 = s[5], p3 = s[4];
-  int sh = bd - 8;
-  int limit_bd = limit << sh, blimit_bd = blimit << sh;
-  if (iabs(p3 - p2) > limit_bd || iabs(p2 - p1) > limit_bd || iabs(p1 - p0) > limit_bd ||
-      iabs(q1 - q0) > limit_bd || iabs(q2 - q1) > limit_bd || iabs(q3 - q2) > limit_bd ||
-      iabs(p0 - q0) * 2 + iabs(p1 - q1) / 2 > blimit_bd)
-    return;
-  int thresh_bd = thresh << sh;
-  bool hev = iabs(p1 - p0) > thresh_bd || iabs(q1 - q0) > thresh_bd;
-  int one = 1 << sh;
-  bool flat = filter_size >= 1 && iabs(p1 - p0) <= one && iabs(q1 - q0) <= one && iabs(p2 - p0) <= one &&
-              iabs(q2 - q0) <= one && iabs(p3 - p0) <= one && iabs(q3 - q0) <= one;
-  if (filter_size == 0 || !flat) {
+  const int q0 = s[8], q1 = s[9], q2 = s[10], q3 = s[11];
+  const int p0 = s[7], p1 = s[6], p2 = s[5], p3 = s[4];
+  const int sh = bd - 8;
+  const int ap1 = iabs(p1 - p0), aq1 = iabs(q1 - q0);
+  // filterMask: every step within limit, the edge within blimit.
+  const int m = imax(imax(imax(iabs(p3 - p2), iabs(p2 - p1)), imax(ap1, aq1)), imax(iabs(q2 - q1), iabs(q3 - q2)));
+  if (m > (limit << sh) || iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1) > (blimit << sh)) return;
+  const int thresh_bd = thresh << sh;
+  const bool hev = ap1 > thresh_bd || aq1 > thresh_bd;
+  const int one = 1 << sh;
+  const bool flat = filter_size >= 1 && imax(imax(ap1, aq1), imax(imax(iabs(p2 - p0), iabs(q2 - q0)),
+                                                                  imax(iabs(p3 - p0), iabs(q3 - q0)))) <= one;
+  if (!flat) {
     // Narrow filter (spec 8.8.5.2).
-    int lo = -(1 << (bd - 1)), hi = (1 << (bd - 1)) - 1;
-    int off = 0x80 << sh;
-    int ps1 = p1 - off, ps0 = p0 - off, qs0 = q0 - off, qs1 = q1 - off;
+    const int lo = -(1 << (bd - 1)), hi = (1 << (bd - 1)) - 1;
+    const int off = 0x80 << sh;
+    const int ps1 = p1 - off, ps0 = p0 - off, qs0 = q0 - off, qs1 = q1 - off;
     int f = hev ? iclamp(ps1 - qs1, lo, hi) : 0;
     f = iclamp(f + 3 * (qs0 - ps0), lo, hi);
-    int f1 = iclamp(f + 4, lo, hi) >> 3, f2 = iclamp(f + 3, lo, hi) >> 3;
+    const int f1 = iclamp(f + 4, lo, hi) >> 3, f2 = iclamp(f + 3, lo, hi) >> 3;
     s[8] = iclamp(qs0 - f1, lo, hi) + off;
     s[7] = iclamp(ps0 + f2, lo, hi) + off;
     if (!hev) {
-      int g = (f1 + 1) >> 1;
+      const int g = (f1 + 1) >> 1;
       s[9] = iclamp(qs1 - g, lo, hi) + off;
       s[6] = iclamp(ps1 + g, lo, hi) + off;
     }
     return;
   }
   bool flat2 = filter_size >= 2;
+  if (flat2) {
+    int m2 = 0;
 #pragma unroll
-  for (int k = 4; k < 8; ++k)
-    if (iabs(s[8 - k - 1] - p0) > one || iabs(s[8 + k] - q0) > one) flat2 = false;
-  if (filter_size == 1 || !flat2)
+    for (int k = 4; k < 8; ++k) m2 = imax(m2, imax(iabs(s[8 - k - 1] - p0), iabs(s[8 + k] - q0)));
+    flat2 = m2 <= one;
+  }
+  if (!flat2)
     lf_wide<3>(s);
   else
     lf_wide<4>(s);
