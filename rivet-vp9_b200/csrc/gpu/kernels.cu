@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
   extern __shared__ __align__(16) unsigned char lf_raw[];
   LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
   const int tid = threadIdx.x;
-  const int bd = k.bit_depth;
+  const int bd = sizeof(T) == 1 ? 8 : k.bit_depth;  // a constant for 8-bit content
   const int cols = k.sb64_cols, rows = k.sb64_rows;
   const uint32_t ep = (uint32_t)(k.epoch & 0xffff) << 16;
   for (int i = tid; i < 64; i += kLfRowThreads) {
