@@ -282,6 +282,17 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
     intra_.swap(sorted_intra_);
   }
   fw->o_intra = put(out, intra_.data(), intra_.size());
+  // Jobs: one row of transform blocks of one block and plane (contiguous in
+  // this order), done by one warp in turn. Each depends on its left
+  // neighbour anyway, so a row loses no parallelism by staying on one warp.
+  intra_jobs_.clear();
+  for (size_t i = 0; i < intra_.size(); ++i)
+    if (i == 0 || intra_[i].block != intra_[i - 1].block || intra_[i].plane != intra_[i - 1].plane ||
+        intra_[i].y != intra_[i - 1].y)
+      intra_jobs_.push_back((uint32_t)i);
+  fw->n_intra_jobs = (uint32_t)intra_jobs_.size();
+  intra_jobs_.push_back((uint32_t)intra_.size());
+  fw->o_intra_jobs = put(out, intra_jobs_.data(), intra_jobs_.size());
   out->resize(align256(out->size()));
   fw->bytes = out->size() - base;
   fw->n_blocks = (uint32_t)pf.blocks.size();
@@ -430,6 +441,8 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   k.n_res = (int32_t)fw.n_res;
   k.intra = (const IntraItem*)(d_base + fw.o_intra);
   k.n_intra = (int32_t)fw.n_intra;
+  k.intra_jobs = (const uint32_t*)(d_base + fw.o_intra_jobs);
+  k.n_intra_jobs = (int32_t)fw.n_intra_jobs;
   // Loop filter levels and limits (8.8.1).
   k.lf_on = d.lf_level != 0;
   if (k.lf_on) {

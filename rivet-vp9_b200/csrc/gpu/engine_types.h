@@ -66,6 +66,10 @@ struct KFrame {
   int32_t n_res;
   const IntraItem* intra;
   int32_t n_intra;
+  // Intra jobs: one row of a block's transform blocks of one plane, items
+  // [intra_jobs[j], intra_jobs[j + 1]); n_intra_jobs + 1 entries.
+  const uint32_t* intra_jobs;
+  int32_t n_intra_jobs;
   // Loop filter.
   uint32_t* lf_mi;          // per 8x8: packed level / tx sizes / block size / skip
   uint8_t lvl[8][4][2];

@@ -393,10 +393,15 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
   const int maxv = (1 << k.bit_depth) - 1;
   volatile int32_t* err = k.error;
   for (;;) {
-    int idx = 0;
-    if (lane == 0) idx = atomicAdd(&k.counters[0], 1);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    if (idx >= k.n_intra) return;
+    // One job per ticket: a row of a block's transform blocks of one plane,
+    // done in order by this warp, so that the links along the row cost no
+    // ticket and no wait on another warp.
+    int job = 0;
+    if (lane == 0) job = atomicAdd(&k.counters[0], 1);
+    job = __shfl_sync(0xffffffffu, job, 0);
+    if (job >= k.n_intra_jobs) return;
+    const int idx_end = (int)k.intra_jobs[job + 1];
+    for (int idx = (int)k.intra_jobs[job]; idx < idx_end; ++idx) {
     const IntraItem it = k.intra[idx];
     const int plane = it.plane, log2 = it.tx_size + 2, size = 1 << log2;
     const int sx = plane ? k.ss_x : 0, sy = plane ? k.ss_y : 0;
@@ -512,6 +517,7 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
       }
     }
     __syncwarp();
+    }
   }
 }
 
@@ -986,7 +992,7 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
       cudaFuncSetAttribute(k_intra<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       attr_set = true;
     }
-    int want = (k.n_intra + kIntraWarps - 1) / kIntraWarps;
+    int want = (k.n_intra_jobs + kIntraWarps - 1) / kIntraWarps;
     int grid = want < n_sm * 4 ? want : n_sm * 4;
     mark(K_INTRA, 0);
     k_intra<T, V><<<grid, 32 * kIntraWarps, smem, s>>>(k);
