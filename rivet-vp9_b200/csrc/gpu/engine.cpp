@@ -262,6 +262,11 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
   fw->o_blocks = put(out, pf.blocks.data(), pf.blocks.size());
   fw->o_toks = put(out, pf.toks.data(), pf.toks.size());
   fw->o_coefs = put(out, pf.coefs.data(), pf.coefs.size());
+  // Regions of at most 16x16 first (one warp each), then the larger ones
+  // (one CTA each).
+  std::stable_partition(units_.begin(), units_.end(), [](const InterUnit& u) { return u.w4 <= 4 && u.h4 <= 4; });
+  fw->n_units_small = 0;
+  for (const InterUnit& u : units_) fw->n_units_small += (u.w4 <= 4 && u.h4 <= 4) ? 1 : 0;
   fw->o_units = put(out, units_.data(), units_.size());
   fw->o_res = put(out, res_.data(), res_.size());
   // The intra wavefront takes its items in list order, one per free warp:
@@ -437,6 +442,7 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   k.coefs = (const uint32_t*)(d_base + fw.o_coefs);
   k.units = (const InterUnit*)(d_base + fw.o_units);
   k.n_units = (int32_t)fw.n_units;
+  k.n_units_small = (int32_t)fw.n_units_small;
   k.res = (const ResItem*)(d_base + fw.o_res);
   k.n_res = (int32_t)fw.n_res;
   k.intra = (const IntraItem*)(d_base + fw.o_intra);

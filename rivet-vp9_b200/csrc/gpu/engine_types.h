@@ -60,8 +60,9 @@ struct KFrame {
   const rv9_block* blocks;
   const rv9_tok* toks;
   const uint32_t* coefs;
-  const InterUnit* units;
+  const InterUnit* units;  // regions of at most 16x16 first, then the rest
   int32_t n_units;
+  int32_t n_units_small;
   const ResItem* res;       // inter blocks' transform blocks with coefficients
   int32_t n_res;
   const IntraItem* intra;

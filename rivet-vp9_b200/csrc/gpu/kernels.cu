@@ -142,10 +142,9 @@ __device__ RefPos ref_position(const KFrame& k, const rv9_block& b, int ref_list
       mv1 = q4(bm[0][1] + bm[1][1] + bm[2][1] + bm[3][1]);
     }
   }
-  const uint8_t N8W[13] = {1, 1, 1, 1, 1, 2, 2, 2, 4, 4, 4, 8, 8};
-  const uint8_t N8H[13] = {1, 1, 1, 1, 2, 1, 2, 4, 2, 4, 8, 4, 8};
   int sx = plane ? k.ss_x : 0, sy = plane ? k.ss_y : 0;
-  int bh = N8H[b.mi_size], bw = N8W[b.mi_size];
+  // num_8x8 wide / high by block size, as 2-bit log2 fields of a constant.
+  int bh = 1 << ((0x3b99100u >> (2 * b.mi_size)) & 3), bw = 1 << ((0x3ea5400u >> (2 * b.mi_size)) & 3);
   int mi_row = b.mi_row, mi_col = b.mi_col;
   int to_top = -((mi_row * 8) * 16) >> sy;
   int to_bottom = (((k.mi_rows - bh - mi_row) * 8) * 16) >> sy;
@@ -177,14 +176,19 @@ __device__ RefPos ref_position(const KFrame& k, const rv9_block& b, int ref_list
 constexpr int kInterThreads = 128;
 constexpr int kInterTmpRows = 64 * 2 + 8;  // (h-1)*step/16 + 8 rows at steps up to 32
 
-// One prediction region per CTA: the horizontal pass over the clamped
-// reference rows into shared memory, then the vertical pass; for compound
-// blocks both predictions, then their rounded average (spec 8.5.2.3-8.5.2.5).
-template <class T>
-__global__ void __launch_bounds__(kInterThreads) k_inter(KFrame k) {
-  __shared__ uint16_t tmp[kInterTmpRows * 64];
-  __shared__ uint16_t pred[64 * 64];
-  const InterUnit u = k.units[blockIdx.x];
+// One prediction region: the horizontal pass over the clamped reference
+// rows into shared memory, then the vertical pass; for compound blocks both
+// predictions, then their rounded average (spec 8.5.2.3-8.5.2.5). NT
+// threads cooperate (a warp, or the whole CTA), `tid` numbering them.
+template <class T, int NT>
+__device__ __forceinline__ void inter_unit(const KFrame& k, const InterUnit& u, int tid, uint16_t* tmp, int tpitch,
+                                           uint16_t* pred, int ppitch) {
+  auto sync = [] {
+    if (NT == 32)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
   const rv9_block& b = k.blocks[u.block];
   const int w = u.w4 * 4, h = u.h4 * 4, plane = u.plane;
   const int maxv = (1 << k.bit_depth) - 1;
@@ -199,7 +203,7 @@ __global__ void __launch_bounds__(kInterThreads) k_inter(KFrame k) {
     const int last_x = rp.width - 1, last_y = rp.height - 1, rstride = rp.stride;
     const int ih = (((h - 1) * p.step_y + 15) >> 4) + 8;
     const int y0 = (p.start_y >> 4) - 3;
-    for (int i = threadIdx.x; i < ih * w; i += kInterThreads) {
+    for (int i = tid; i < ih * w; i += NT) {
       int r = i / w, c = i - r * w;
       int ry = clampi(y0 + r, 0, last_y);
       const T* src = ref + (size_t)ry * rstride;
@@ -209,27 +213,51 @@ __global__ void __launch_bounds__(kInterThreads) k_inter(KFrame k) {
       int32_t sum = 0;
 #pragma unroll
       for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)src[clampi(base + t, 0, last_x)];
-      tmp[r * 64 + c] = (uint16_t)clampi((sum + 64) >> 7, 0, maxv);
+      tmp[r * tpitch + c] = (uint16_t)clampi((sum + 64) >> 7, 0, maxv);
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < h * w; i += kInterThreads) {
+    sync();
+    for (int i = tid; i < h * w; i += NT) {
       int r = i / w, c = i - r * w;
       int pos = (p.start_y & 15) + p.step_y * r;
       int base = pos >> 4;
       const int16_t* f = c_filters[filter][pos & 15];
       int32_t sum = 0;
 #pragma unroll
-      for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)tmp[(base + t) * 64 + c];
+      for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)tmp[(base + t) * tpitch + c];
       int v = clampi((sum + 64) >> 7, 0, maxv);
       if (!compound)
         dst[(size_t)r * dstride + c] = (T)v;
       else if (rl == 0)
-        pred[r * 64 + c] = (uint16_t)v;
+        pred[r * ppitch + c] = (uint16_t)v;
       else
-        dst[(size_t)r * dstride + c] = (T)((pred[r * 64 + c] + v + 1) >> 1);
+        dst[(size_t)r * dstride + c] = (T)((pred[r * ppitch + c] + v + 1) >> 1);
     }
-    __syncthreads();
+    sync();
   }
+}
+
+// Regions larger than 16x16 (after the small ones in the list): one CTA each.
+template <class T>
+__global__ void __launch_bounds__(kInterThreads) k_inter(KFrame k) {
+  __shared__ uint16_t tmp[kInterTmpRows * 64];
+  __shared__ uint16_t pred[64 * 64];
+  const InterUnit u = k.units[k.n_units_small + blockIdx.x];
+  inter_unit<T, kInterThreads>(k, u, threadIdx.x, tmp, 64, pred, 64);
+}
+
+// Regions of at most 16x16 (the first n_units_small of the list): one warp
+// each, four per CTA. Rows of the horizontal pass: (16-1)*32/16 + 8 at the
+// largest reference step (2:1).
+constexpr int kInterSmallRows = 38;
+template <class T>
+__global__ void __launch_bounds__(kInterThreads) k_inter_small(KFrame k) {
+  __shared__ uint16_t tmp[kInterThreads / 32][kInterSmallRows * 16];
+  __shared__ uint16_t pred[kInterThreads / 32][16 * 16];
+  const int warp = threadIdx.x >> 5;
+  const int i = blockIdx.x * (kInterThreads / 32) + warp;
+  if (i >= k.n_units_small) return;
+  const InterUnit u = k.units[i];
+  inter_unit<T, 32>(k, u, threadIdx.x & 31, tmp[warp], 16, pred[warp], 16);
 }
 
 // ---------------------------------------------------------------------------
@@ -975,9 +1003,15 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
   }
   if (k.n_units > 0) {
     mark(K_INTER, 0);
-    k_inter<T><<<k.n_units, kInterThreads, 0, s>>>(k);
+    if (k.n_units_small > 0) {
+      k_inter_small<T><<<(k.n_units_small + kInterThreads / 32 - 1) / (kInterThreads / 32), kInterThreads, 0, s>>>(k);
+      ++L;
+    }
+    if (k.n_units > k.n_units_small) {
+      k_inter<T><<<k.n_units - k.n_units_small, kInterThreads, 0, s>>>(k);
+      ++L;
+    }
     mark(K_INTER, 1);
-    ++L;
   }
   if (k.n_res > 0) {
     mark(K_INTER_RES, 0);
