@@ -268,6 +268,13 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
   fw->n_units_small = 0;
   for (const InterUnit& u : units_) fw->n_units_small += (u.w4 <= 4 && u.h4 <= 4) ? 1 : 0;
   fw->o_units = put(out, units_.data(), units_.size());
+  // Residuals by transform size (the residual kernel packs 8, 4, 2 or 1 of
+  // them per warp).
+  std::stable_sort(res_.begin(), res_.end(), [&](const ResItem& a, const ResItem& b) {
+    return pf.toks[a.tok].tx_size < pf.toks[b.tok].tx_size;
+  });
+  for (int z = 0; z < 4; ++z) fw->n_res_by_size[z] = 0;
+  for (const ResItem& r : res_) ++fw->n_res_by_size[pf.toks[r.tok].tx_size & 3];
   fw->o_res = put(out, res_.data(), res_.size());
   // The intra wavefront takes its items in list order, one per free warp:
   // superblocks in anti-diagonal order (d = column + 2 row; every superblock
@@ -445,6 +452,7 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   k.n_units_small = (int32_t)fw.n_units_small;
   k.res = (const ResItem*)(d_base + fw.o_res);
   k.n_res = (int32_t)fw.n_res;
+  for (int z = 0; z < 4; ++z) k.n_res_by_size[z] = (int32_t)fw.n_res_by_size[z];
   k.intra = (const IntraItem*)(d_base + fw.o_intra);
   k.n_intra = (int32_t)fw.n_intra;
   k.intra_jobs = (const uint32_t*)(d_base + fw.o_intra_jobs);

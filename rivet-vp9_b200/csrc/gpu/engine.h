@@ -64,6 +64,7 @@ struct FrameWork {
   uint32_t n_blocks = 0, n_toks = 0, n_coefs = 0, n_units = 0, n_units_small = 0, n_res = 0, n_intra = 0,
            n_intra_jobs = 0;
   size_t o_blocks = 0, o_toks = 0, o_coefs = 0, o_units = 0, o_res = 0, o_intra = 0, o_intra_jobs = 0, bytes = 0;
+  uint32_t n_res_by_size[4] = {0, 0, 0, 0};
   uint64_t kbytes[K_COUNT] = {0};  // algorithmic bytes per kernel
   uint64_t total_bytes = 0;        // algorithmic bytes of the frame
 };

@@ -63,7 +63,8 @@ struct KFrame {
   const InterUnit* units;  // regions of at most 16x16 first, then the rest
   int32_t n_units;
   int32_t n_units_small;
-  const ResItem* res;       // inter blocks' transform blocks with coefficients
+  const ResItem* res;       // inter blocks' transform blocks with coefficients, 4x4 first, then 8x8, 16x16, 32x32
+  int32_t n_res_by_size[4];
   int32_t n_res;
   const IntraItem* intra;
   int32_t n_intra;

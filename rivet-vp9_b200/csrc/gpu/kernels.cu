@@ -8,14 +8,18 @@
 //                 reconstructs into zeroed planes, src/decoder/pool.rs:1-6)
 //   k_lf_mi       per 8x8 loop-filter record from the block records
 //   k_intra_mark  mark the 4x4 cells of intra transform blocks pending
-//   k_inter       inter prediction: one CTA per prediction region, 8-tap
-//                 H then V passes through shared memory, scaled references,
-//                 compound averaging fused (src/dsp/inter.rs, pixel.rs)
-//   k_inter_res   inverse transform + add of inter blocks' residuals: one
-//                 warp per transform block (src/dsp/itx.rs)
+//   k_inter_small / k_inter
+//                 inter prediction: a warp per region of at most 16x16, a
+//                 CTA per larger one; 8-tap H then V passes through shared
+//                 memory, scaled references, compound averaging fused
+//                 (src/dsp/inter.rs, pixel.rs)
+//   k_inter_res_n inverse transform + add of inter blocks' residuals, one
+//                 launch per transform size: 8, 4, 2 or 1 blocks per warp
+//                 (src/dsp/itx.rs)
 //   k_intra       intra prediction + residual as a dependency wavefront:
-//                 a persistent grid takes transform blocks in bitstream order
-//                 and each warp waits only for the 4x4 cells its edges read
+//                 a persistent grid takes rows of transform blocks in
+//                 superblock anti-diagonal order and each warp waits only
+//                 for the 4x4 cells its edges read
 //   k_lf_rows     loop filter: one CTA per superblock row, left to right,
 //                 each superblock's vertical then horizontal edges in shared
 //                 memory; a row waits only for the row above to be one
@@ -263,10 +267,6 @@ __global__ void __launch_bounds__(kInterThreads) k_inter_small(KFrame k) {
 // ---------------------------------------------------------------------------
 // Inverse transform + add, one warp per transform block.
 
-template <class V>
-struct Scratch {
-  typename V::store_t s[32 * 33];
-};
 
 // Dequantise the recorded coefficients of `t` into the warp's scratch (zeroed
 // first) and return the mask of rows holding a nonzero value (reference
@@ -363,42 +363,82 @@ __device__ void itx_add_size(int tx_size, typename V::store_t* s, uint32_t rows,
   }
 }
 
-// Dequantise, inverse transform and add the residual of `t` to `dst`.
-template <class V, class T>
-__device__ void residual_add(const KFrame& k, const rv9_tok& t, int seg, T* dst, int dstride,
-                             typename V::store_t* s, int lane) {
-  const int maxv = (1 << k.bit_depth) - 1;
-  const int n = 2 + t.tx_size, n0 = 1 << n;
-  if (t.eob == 1 && t.tx_type == 0 && !k.lossless) {
-    // Only the DC coefficient: every sample gets the same residual.
-    int res = dc_only_residual<V>(k, t, seg);
-    for (int i = lane; i < n0 * n0; i += 32) {
-      int r = i >> n, c = i & (n0 - 1);
-      T* px = dst + (size_t)r * dstride + c;
-      *px = (T)clampi((int)*px + res, 0, maxv);
-    }
-    __syncwarp();
-    return;
-  }
-  uint32_t rows = load_coefs<V>(k, t, seg, s, lane);
-  itx_add_size<V, T>(t.tx_size, s, rows, t.tx_type, k.lossless, dst, dstride, maxv, lane);
-}
-
 constexpr int kResWarps = 4;
 
-template <class T, class V>
-__global__ void __launch_bounds__(32 * kResWarps) k_inter_res(KFrame k) {
-  __shared__ Scratch<V> sc[kResWarps];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kResWarps + warp;
-  if (i >= k.n_res) return;
-  const ResItem it = k.res[i];
+// A transform block's residual added to dst by a group of n0 lanes of a warp
+// (lane l of the group: row l, then column l), `mask` the group's lanes:
+// 4x4 blocks go eight to a warp, 8x8 four, 16x16 two, 32x32 one.
+template <class V, int n, class T>
+__device__ void residual_add_group(const KFrame& k, const rv9_tok& t, int seg, T* dst, int dstride,
+                                   typename V::store_t* s, int l, unsigned mask) {
+  constexpr int n0 = 1 << n, sp = n0 + 1;
+  const int maxv = (1 << k.bit_depth) - 1;
+  if (t.eob == 1 && t.tx_type == 0 && !k.lossless) {
+    const int res = dc_only_residual<V>(k, t, seg);
+    for (int r = 0; r < n0; ++r) {
+      T* px = dst + (size_t)r * dstride + l;
+      *px = (T)clampi((int)*px + res, 0, maxv);
+    }
+    return;
+  }
+  for (int i = l; i < n0 * sp; i += n0) s[i] = 0;
+  __syncwarp(mask);
+  const int pt = t.plane ? 1 : 0;
+  const int64_t dcq = k.dc_q[seg][pt], acq = k.ac_q[seg][pt];
+  uint32_t rows = 0;
+  for (int i = l; i < t.n_coef; i += n0) {
+    uint32_t w = k.coefs[t.coef_start + i];
+    int pos = RV9_COEF_POS(w);
+    int64_t dq = (int64_t)RV9_COEF_VAL(w) * (pos == 0 ? dcq : acq);
+    if (n == 5) dq /= 2;
+    dq = dq < INT32_MIN ? INT32_MIN : (dq > INT32_MAX ? INT32_MAX : dq);
+    const int r = pos >> n, c = pos & (n0 - 1);
+    s[r * sp + c] = (typename V::store_t)(int32_t)dq;
+    rows |= 1u << r;
+  }
+  rows = __reduce_or_sync(mask, rows);
+  __syncwarp(mask);
+  const int row_kind = k.lossless ? 2 : ((t.tx_type == 0 || t.tx_type == 1) ? 0 : 1);
+  const int col_kind = k.lossless ? 2 : ((t.tx_type == 0 || t.tx_type == 2) ? 0 : 1);
+  if ((rows >> l) & 1) {
+    V v[n0];
+#pragma unroll
+    for (int q = 0; q < n0; ++q) v[q] = V::load(s[l * sp + q]);
+    tx1d<n>(v, row_kind, 2);
+#pragma unroll
+    for (int q = 0; q < n0; ++q) s[l * sp + q] = v[q].v;
+  }
+  __syncwarp(mask);
+  V v[n0];
+#pragma unroll
+  for (int i = 0; i < n0; ++i) v[i] = V::load(s[i * sp + l]);
+  tx1d<n>(v, col_kind, 0);
+  constexpr int shift = (n + 2) < 6 ? (n + 2) : 6;
+#pragma unroll
+  for (int i = 0; i < n0; ++i) {
+    V r = k.lossless ? v[i] : v[i].rshift(shift);
+    T* px = dst + (size_t)i * dstride + l;
+    *px = (T)clampi((int)*px + r.residual(), 0, maxv);
+  }
+}
+
+// The inter residuals of one transform size: items [first, first + count).
+template <class T, class V, int n>
+__global__ void __launch_bounds__(32 * kResWarps) k_inter_res_n(KFrame k, int first, int count) {
+  constexpr int n0 = 1 << n, G = 32 / n0, sp = n0 + 1;
+  __shared__ typename V::store_t sc[kResWarps][G][n0 * sp];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, grp = lane / n0, l = lane & (n0 - 1);
+  const int i = (blockIdx.x * kResWarps + warp) * G + grp;
+  if (i >= count) return;  // the whole group
+  const unsigned mask = n0 == 32 ? 0xffffffffu : (((1u << n0) - 1u) << (grp * n0));
+  const ResItem it = k.res[first + i];
   const rv9_tok& t = k.toks[it.tok];
   const rv9_block& b = k.blocks[it.block];
   const PlanePtr& pp = k.cur[t.plane];
   T* dst = plane_ptr<T>(pp) + (size_t)t.y * pp.stride + t.x;
-  residual_add<V, T>(k, t, b.segment_id, dst, pp.stride, sc[warp].s, lane);
+  residual_add_group<V, n, T>(k, t, b.segment_id, dst, pp.stride, sc[warp][grp], l, mask);
 }
+
 
 // ---------------------------------------------------------------------------
 // Intra wavefront.
@@ -1015,9 +1055,23 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
   }
   if (k.n_res > 0) {
     mark(K_INTER_RES, 0);
-    k_inter_res<T, V><<<(k.n_res + kResWarps - 1) / kResWarps, 32 * kResWarps, 0, s>>>(k);
+    int first = 0;
+#define RV9_RES_LAUNCH(N)                                                                            \
+  {                                                                                                  \
+    const int cnt = k.n_res_by_size[N - 2];                                                          \
+    if (cnt > 0) {                                                                                   \
+      const int per_cta = kResWarps * (32 >> N);                                                     \
+      k_inter_res_n<T, V, N><<<(cnt + per_cta - 1) / per_cta, 32 * kResWarps, 0, s>>>(k, first, cnt); \
+      ++L;                                                                                           \
+    }                                                                                                \
+    first += cnt;                                                                                    \
+  }
+    RV9_RES_LAUNCH(2)
+    RV9_RES_LAUNCH(3)
+    RV9_RES_LAUNCH(4)
+    RV9_RES_LAUNCH(5)
+#undef RV9_RES_LAUNCH
     mark(K_INTER_RES, 1);
-    ++L;
   }
   if (k.n_intra > 0) {
     size_t smem = sizeof(IntraSmem<V>) * kIntraWarps;
