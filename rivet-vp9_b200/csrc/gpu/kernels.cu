@@ -1080,8 +1080,13 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
       cudaFuncSetAttribute(k_intra<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       attr_set = true;
     }
+    // One CTA per SM at most: a warp per job of the wavefront's width (a
+    // diagonal of superblocks, a few rows of transform blocks each) with
+    // room to spare; more warps would only poll further ahead, taking issue
+    // slots and L2 bandwidth from the warps on the chain and from other
+    // streams' kernels.
     int want = (k.n_intra_jobs + kIntraWarps - 1) / kIntraWarps;
-    int grid = want < n_sm * 4 ? want : n_sm * 4;
+    int grid = want < n_sm ? want : n_sm;
     mark(K_INTRA, 0);
     k_intra<T, V><<<grid, 32 * kIntraWarps, smem, s>>>(k);
     mark(K_INTRA, 1);
