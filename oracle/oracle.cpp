@@ -1071,6 +1071,7 @@ struct rv9o_decoder {
 rv9o_decoder* rv9o_decoder_new(void) { return new rv9o_decoder; }
 void rv9o_decoder_free(rv9o_decoder* d) { delete d; }
 void rv9o_decoder_set_threads(rv9o_decoder* d, uint32_t t) { d->dec.parser.set_threads((int)t); }
+void rv9o_decoder_set_max_pixels(rv9o_decoder* d, uint64_t p) { d->dec.parser.set_max_pixels(p); }
 uint64_t rv9o_decoder_frames_decoded(const rv9o_decoder* d) { return d->dec.parser.frames_decoded(); }
 const char* rv9o_last_error(const rv9o_decoder* d) { return d->dec.err.c_str(); }
 double rv9o_recon_seconds(const rv9o_decoder* d) { return d->dec.recon_seconds; }

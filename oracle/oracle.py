@@ -43,6 +43,7 @@ def lib():
         L.rv9o_decoder_new.restype = vp
         L.rv9o_decoder_free.argtypes = [vp]
         L.rv9o_decoder_set_threads.argtypes = [vp, ctypes.c_uint32]
+        L.rv9o_decoder_set_max_pixels.argtypes = [vp, ctypes.c_uint64]
         L.rv9o_decoder_frames_decoded.restype = ctypes.c_uint64
         L.rv9o_decoder_frames_decoded.argtypes = [vp]
         L.rv9o_last_error.restype = ctypes.c_char_p
@@ -89,6 +90,9 @@ class OracleDecoder:
             self._L.rv9o_decoder_free(self._d)
         except Exception:
             pass
+
+    def set_max_pixels(self, pixels):
+        self._L.rv9o_decoder_set_max_pixels(self._d, pixels)
 
     def decode_all(self, packet):
         cap = 16
