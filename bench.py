@@ -283,7 +283,8 @@ def run_batched(local, dev, n_streams=64, frames=60):
     return out
 
 
-def run_served(local, rates=(500, 1000, 2000, 4000), n_streams=32, frames=120, seed=5):
+def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4000, 120)), n_streams=32, frames=120,
+               seed=5):
     """The serving loop: 32 live streams (40% 720p, 40% 1080p, 20% 2160p;
     8/10-bit), requests arriving as a Poisson process at each total rate;
     throughput and per-request latency (submit -> frames in host memory)."""
@@ -313,14 +314,22 @@ def run_served(local, rates=(500, 1000, 2000, 4000), n_streams=32, frames=120, s
     plain = len(pk) * luma["s1080_8"] / (time.perf_counter() - t) / 1e6
     d.close()
     del buf
-    for rate in rates:
+    for rate, nfr in rates:
         eng = server.Engine(local, hbm_budget=120 << 30)
         sids = [eng.open_stream(spec[n]["width"], spec[n]["height"], spec[n]["bit_depth"]) for n in mix]
+        # Set-up, untimed: every stream admitted (its reservation allocated)
+        # and its first frame (a keyframe) decoded.
+        for j, n in enumerate(mix):
+            eng.submit(sids[j], contents[n][0], tag=0)
+        warm = []
+        t_warm = time.perf_counter() + 300
+        while len(warm) < len(mix) and time.perf_counter() < t_warm:
+            warm += eng.poll(max_items=256, timeout_ms=50, keep_frames=False)
         # Arrival times: per stream a Poisson process of rate/n_streams.
         events = []
         for j, n in enumerate(mix):
             tt = 0.0
-            for i in range(frames):
+            for i in range(1, nfr):
                 tt += rng.expovariate(rate / n_streams)
                 events.append((tt, j, i))
         events.sort()
@@ -347,7 +356,8 @@ def run_served(local, rates=(500, 1000, 2000, 4000), n_streams=32, frames=120, s
         eng.close()
         lat = [c.latency_ms for c in done if c.ok]
         px = sum(luma[mix[sids.index(c.stream)]] * c.n_frames for c in done if c.ok)
-        results.append({"offered_fps": rate, "completed": len(lat), "failed": len(done) - len(lat),
+        results.append({"offered_fps": rate, "frames_per_stream": nfr, "completed": len(lat),
+                        "failed": len(done) - len(lat),
                         "fps": round(len(lat) / wall, 1), "mpixels_s": round(px / wall / 1e6, 1),
                         "p50_ms": round(percentile(lat, 50), 2) if lat else None,
                         "p99_ms": round(percentile(lat, 99), 2) if lat else None, "wall_s": round(wall, 2)})
@@ -356,7 +366,8 @@ def run_served(local, rates=(500, 1000, 2000, 4000), n_streams=32, frames=120, s
                         f"{CLASS_FRAMES} frames looped to {frames}; Poisson arrivals; HBM budget 120 GB",
             "rates": results, "plain_single_stream_e2e_mpixels_s": round(plain, 1),
             "best_vs_plain": round(best / plain, 2),
-            "latency": "rv9_submit -> frames in pinned host memory (host-function callback)",
+            "latency": "rv9_submit -> frames in pinned host memory (host-function callback); streams admitted and "
+                       "their first frame decoded before the timed arrivals",
             "host_cores": os.cpu_count()}
 
 
