@@ -405,6 +405,8 @@ def run_gpu(args, world, rank, local):
     def launches_total():
         return sum(d.stats()["kernel_launches"] for d in decs)
 
+    # Launch shapes per decoder from the autotuner (untimed).
+    tuned = [d.autotune(sq) for d, sq in pairs]
     for _ in range(args.warmup):
         step(False)
     kernel_stats()
@@ -524,6 +526,8 @@ def run_gpu(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": traffic},
+            "autotune": [{"intra_ctas_per_sm_x4": t["intra_ctas_per_sm_x4"], "inter_threads": t["inter_threads"],
+                          "best_ms": round(t["best_ms"], 3), "default_ms": round(t["default_ms"], 3)} for t in tuned],
             "graph_replay": {"value": round(whole_job_value(luma_per_step, world, ms_graph), 2),
                              "unit": "Mpixels/s", "ms_per_step": round(ms_graph, 3),
                              "how": "the same steps replayed as CUDA graphs (captured once; first replay untimed)"},

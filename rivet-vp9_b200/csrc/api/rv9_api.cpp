@@ -294,6 +294,18 @@ void rv9_sequence_free(rv9_decoder* d, rv9_sequence* s) {
   delete s;
 }
 
+rv9_status rv9_decoder_autotune(rv9_decoder* d, rv9_sequence* s, rv9_tune_result* out) {
+  if (!d || !s || !out) return RV9_INVALID_INPUT;
+  rv9g::TuneParams best;
+  float best_ms = 0, default_ms = 0;
+  rv9::Status st = d->engine.autotune(s->seq, &best, &best_ms, &default_ms, &d->err);
+  out->intra_ctas_per_sm_x4 = best.intra_ctas_per_sm_x4;
+  out->inter_threads = best.inter_threads;
+  out->best_ms = best_ms;
+  out->default_ms = default_ms;
+  return (rv9_status)st;
+}
+
 rv9_status rv9_decoder_download_slot(rv9_decoder* d, int slot, uint8_t* out, size_t cap, size_t* bytes) {
   *bytes = 0;
   if (slot < 0 || slot > 7 || !d->engine.slot(slot)) return RV9_INVALID_INPUT;

@@ -505,7 +505,14 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   }
   int L = 0;
   cur_fw_ = &fw;
-  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this));
+  TuneParams tune;
+  if (tune_override_) {
+    tune = *tune_override_;
+  } else {
+    auto it = tuned_.find(geometry_key(d));
+    if (it != tuned_.end()) tune = it->second;
+  }
+  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this, tune));
   cur_fw_ = nullptr;
   // The device's error word, read at the next sync.
   CK(cudaMemcpyAsync(h_error_ + 1, k.error, 4, cudaMemcpyDeviceToHost, stream_));
@@ -612,6 +619,56 @@ rv9::Status Engine::sequence_run(const Sequence& seq, bool per_kernel, float* ms
   CK(cudaEventElapsedTime(ms, ev0_, ev1_));
   device_ms += *ms;
   if (per_kernel) collect_kernel_events();
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::autotune(const Sequence& seq, TuneParams* best, float* best_ms, float* default_ms,
+                             std::string* err) {
+  *best = TuneParams();
+  *best_ms = *default_ms = 0;
+  if (seq.frames.empty()) return rv9::ST_OK;
+  const FrameWork* first = nullptr;
+  for (const FrameWork& fw : seq.frames)
+    if (!fw.show_existing) {
+      first = &fw;
+      break;
+    }
+  if (!first) return rv9::ST_OK;
+  // The sequence's time with given shapes: the best of three runs after one
+  // untimed run.
+  auto time_with = [&](const TuneParams& tp, float* out) -> rv9::Status {
+    tune_override_ = &tp;
+    float ms = 0, bestr = 0;
+    rv9::Status st = rv9::ST_OK;
+    for (int r = 0; r < 4 && st == rv9::ST_OK; ++r) {
+      st = sequence_run(seq, false, &ms, err);
+      device_ms -= ms;
+      if (r == 1 || (r > 1 && ms < bestr)) bestr = ms;
+    }
+    tune_override_ = nullptr;
+    *out = bestr;
+    return st;
+  };
+  rv9::Status st = time_with(TuneParams(), default_ms);
+  if (st != rv9::ST_OK) return st;
+  *best_ms = *default_ms;
+  const int grains[] = {1, 2, 4, 8, 16};
+  const int threads[] = {64, 128, 256};
+  for (int g : grains)
+    for (int t : threads) {
+      TuneParams tp;
+      tp.intra_ctas_per_sm_x4 = g;
+      tp.inter_threads = t;
+      float ms = 0;
+      st = time_with(tp, &ms);
+      if (st != rv9::ST_OK) return st;
+      if (ms < *best_ms) {
+        *best_ms = ms;
+        *best = tp;
+      }
+    }
+  for (const FrameWork& fw : seq.frames)
+    if (!fw.show_existing) tuned_[geometry_key(fw.desc)] = *best;
   return rv9::ST_OK;
 }
 

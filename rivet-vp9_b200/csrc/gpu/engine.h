@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -20,8 +21,15 @@ extern const char* const kKernelNames[K_COUNT];
 // Called around each launch when timing per kernel: phase 0 before, 1 after.
 typedef void (*LaunchHook)(void* ctx, int kernel, int phase);
 
+// Launch shapes the autotuner chooses per frame geometry: the intra
+// wavefront's grain (its grid, in quarter CTAs per SM) and the CTA size of
+// the large-region inter kernel.
+struct TuneParams {
+  int intra_ctas_per_sm_x4 = 4;  // 1, 2, 4, 8, 16: a quarter to four CTAs per SM
+  int inter_threads = 128;       // 64, 128 or 256
+};
 cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
-                         void* hook_ctx);
+                         void* hook_ctx, const TuneParams& tune = TuneParams());
 cudaError_t upload_filters(const int16_t* f);
 
 // The fixed wavefront scratch: a static device array of this many bytes.
@@ -104,6 +112,10 @@ class Engine {
   rv9::Status sync(std::string* err);
   static size_t packed_bytes(const DevFrame* f);
 
+  // Tries the launch shapes of TuneParams on `seq` (a few runs each), keeps
+  // the fastest for the geometry of its frames and returns it with its time
+  // and that of the defaults.
+  rv9::Status autotune(const Sequence& seq, TuneParams* best, float* best_ms, float* default_ms, std::string* err);
   // Device-resident sequences.
   rv9::Status sequence_load(const std::vector<rv9::ParsedFrame>& frames, Sequence* seq, std::string* err);
   // Reconstructs every frame of `seq` from scratch (empty slots first);
@@ -159,6 +171,12 @@ class Engine {
                         std::string* err);
   void reset_slots();
   bool pool_covers(const Sequence& seq);
+  static uint64_t geometry_key(const rv9_frame_desc& d) {
+    return (uint64_t)d.sb64_cols | (uint64_t)d.sb64_rows << 16 | (uint64_t)d.bit_depth << 32 |
+           (uint64_t)d.ss_x << 40 | (uint64_t)d.ss_y << 41;
+  }
+  std::map<uint64_t, TuneParams> tuned_;  // by frame geometry
+  const TuneParams* tune_override_ = nullptr;
   static void hook(void* ctx, int kernel, int phase);
   void collect_kernel_events();
 

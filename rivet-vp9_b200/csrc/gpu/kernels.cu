@@ -240,13 +240,14 @@ __device__ __forceinline__ void inter_unit(const KFrame& k, const InterUnit& u, 
   }
 }
 
-// Regions larger than 16x16 (after the small ones in the list): one CTA each.
-template <class T>
-__global__ void __launch_bounds__(kInterThreads) k_inter(KFrame k) {
+// Regions larger than 16x16 (after the small ones in the list): one CTA of
+// NT threads each.
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_inter(KFrame k) {
   __shared__ uint16_t tmp[kInterTmpRows * 64];
   __shared__ uint16_t pred[64 * 64];
   const InterUnit u = k.units[k.n_units_small + blockIdx.x];
-  inter_unit<T, kInterThreads>(k, u, threadIdx.x, tmp, 64, pred, 64);
+  inter_unit<T, NT>(k, u, threadIdx.x, tmp, 64, pred, 64);
 }
 
 // Regions of at most 16x16 (the first n_units_small of the list): one warp
@@ -1015,7 +1016,7 @@ cudaError_t upload_filters(const int16_t* f) { return cudaMemcpyToSymbol(c_filte
 
 template <class T, class V>
 static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches,
-                                  LaunchHook hook, void* hctx) {
+                                  LaunchHook hook, void* hctx, const TuneParams& tune) {
   int L = 0;
   auto mark = [&](int id, int phase) {
     if (hook) hook(hctx, id, phase);
@@ -1048,7 +1049,13 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
       ++L;
     }
     if (k.n_units > k.n_units_small) {
-      k_inter<T><<<k.n_units - k.n_units_small, kInterThreads, 0, s>>>(k);
+      const int nl = k.n_units - k.n_units_small;
+      if (tune.inter_threads == 64)
+        k_inter<T, 64><<<nl, 64, 0, s>>>(k);
+      else if (tune.inter_threads == 256)
+        k_inter<T, 256><<<nl, 256, 0, s>>>(k);
+      else
+        k_inter<T, 128><<<nl, 128, 0, s>>>(k);
       ++L;
     }
     mark(K_INTER, 1);
@@ -1086,7 +1093,8 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
     // slots and L2 bandwidth from the warps on the chain and from other
     // streams' kernels.
     int want = (k.n_intra_jobs + kIntraWarps - 1) / kIntraWarps;
-    int grid = want < n_sm ? want : n_sm;
+    int cap = (n_sm * tune.intra_ctas_per_sm_x4 + 3) / 4;
+    int grid = want < cap ? want : cap;
     mark(K_INTRA, 0);
     k_intra<T, V><<<grid, 32 * kIntraWarps, smem, s>>>(k);
     mark(K_INTRA, 1);
@@ -1110,9 +1118,9 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
 }
 
 cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
-                         void* hook_ctx) {
-  if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx);
-  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx);
+                         void* hook_ctx, const TuneParams& tune) {
+  if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune);
+  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune);
 }
 
 // ---------------------------------------------------------------------------

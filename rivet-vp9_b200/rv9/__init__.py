@@ -72,7 +72,12 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
-           "rv9_sequence_run_noalloc", "rv9_sequences_run")
+           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_decoder_autotune")
+
+
+class CTuneResult(ctypes.Structure):
+    _fields_ = [("intra_ctas_per_sm_x4", ctypes.c_int32), ("inter_threads", ctypes.c_int32),
+                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double)]
 
 
 class CKernelStat(ctypes.Structure):
@@ -116,6 +121,7 @@ def load_library(path=None):
                                       ctypes.c_size_t, ctypes.POINTER(vp)]
     lib.rv9_sequence_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.rv9_sequence_run_noalloc.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double)]
+    lib.rv9_decoder_autotune.argtypes = [vp, vp, ctypes.POINTER(CTuneResult)]
     lib.rv9_sequences_run.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_double)]
     for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
@@ -328,6 +334,16 @@ class Decoder:
         if st != RV9_OK:
             _raise(self._lib, self._dec, st)
         return Sequence(self, out)
+
+    def autotune(self, seq):
+        """Picks this decoder's launch shapes for the geometry of `seq`'s
+        frames (rv9_decoder_autotune); returns the choice and the times."""
+        r = CTuneResult()
+        st = self._lib.rv9_decoder_autotune(self._dec, seq._h, ctypes.byref(r))
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+        return {"intra_ctas_per_sm_x4": r.intra_ctas_per_sm_x4, "inter_threads": r.inter_threads,
+                "best_ms": r.best_ms, "default_ms": r.default_ms}
 
     def download_slot(self, slot, cap):
         buf = ctypes.create_string_buffer(cap)

@@ -136,3 +136,23 @@ def test_graph_replay_equals_run():
         for d, s in zip(decs, seqs):
             s.free()
             d.close()
+
+
+def test_autotune_keeps_results_exact():
+    # The autotuner's launch shapes change no sample: every vector's slots
+    # are the same after tuning as before.
+    import rv9
+    for name in NAMES[:3] + NAMES[4:6]:
+        d = rv9.Decoder(0)
+        s = d.load_sequence(read_packets(os.path.join(VECTORS_DIR, name)))
+        try:
+            s.run()
+            want = _slots(d)
+            r = d.autotune(s)
+            assert r["intra_ctas_per_sm_x4"] in (1, 2, 4, 8, 16) and r["inter_threads"] in (64, 128, 256)
+            assert 0 < r["best_ms"] <= r["default_ms"]
+            s.run()
+            assert _slots(d) == want, name
+        finally:
+            s.free()
+            d.close()
