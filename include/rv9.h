@@ -77,7 +77,7 @@ void rv9_decoder_free(rv9_decoder* dec);
 /* Host parsing threads: 0 = one per core (default), 1 = the calling thread. */
 void rv9_decoder_set_threads(rv9_decoder* dec, uint32_t threads);
 /* Frames rv9_decode_packets and rv9_sequence_load parse at once (0: one per
- * four host threads, at most 8). Frames that depend on an earlier frame's
+ * two host threads, at most 8). Frames that depend on an earlier frame's
  * parse (adapted contexts, previous motion vectors) still wait for it; key
  * and error-resilient frames do not. Results are identical either way. */
 void rv9_decoder_set_parse_depth(rv9_decoder* dec, uint32_t frames);

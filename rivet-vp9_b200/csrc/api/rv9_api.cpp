@@ -21,14 +21,14 @@ struct rv9_decoder {
   std::string err;
   rv9::ParsedFrame pf;
   double parse_ms = 0;
-  uint32_t parse_depth = 0;  // frames parsed at once; 0: one per four host threads
+  uint32_t parse_depth = 0;  // frames parsed at once; 0: one per two host threads
 };
 
 // Frames parsed at once by the multi-packet calls.
 static int parse_depth(const rv9_decoder* d) {
   if (d->parse_depth) return (int)d->parse_depth;
   int hw = (int)std::thread::hardware_concurrency();
-  return std::max(1, std::min(8, hw / 4));
+  return std::max(1, std::min(8, hw / 2));
 }
 
 static thread_local std::string g_global_err;

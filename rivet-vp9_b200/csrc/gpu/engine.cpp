@@ -157,23 +157,21 @@ static int uv_tx_size(const rv9_frame_desc& d, const rv9_block& b) {
   return std::min<int>(b.tx_size, MAX_TXSIZE_LOOKUP[uv]);
 }
 
-template <class T>
-static size_t put(std::vector<uint8_t>* out, const T* data, size_t n) {
-  size_t off = align256(out->size());
-  out->resize(off + n * sizeof(T));
-  if (n) memcpy(out->data() + off, data, n * sizeof(T));
-  return off;
-}
-
 // The work lists (the prediction regions and residuals of inter blocks, and
 // the intra transform blocks in bitstream order, replay's loop structure) and
-// the frame's staged bytes, appended to `out`. Algorithmic bytes per kernel:
-// inter 1 sample per predicted sample and reference plus the output; a
-// residual its coefficient words plus reading and writing its samples; intra
-// its samples out plus (3 n + 1) edge samples plus its coefficients; the loop
-// filter reading and writing the mode-info area once; all at 1 byte per
-// sample at 8 bits, 2 above.
-void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<uint8_t>* out) {
+// the frame's staged bytes, written where `reserve` says. Algorithmic bytes
+// per kernel: inter 1 sample per predicted sample and reference plus the
+// output; a residual its coefficient words plus reading and writing its
+// samples; intra its samples out plus (3 n + 1) edge samples plus its
+// coefficients; the loop filter reading and writing the mode-info area once;
+// all at 1 byte per sample at 8 bits, 2 above.
+//
+// The lists come out already in launch order, each bucketed as it is built
+// (no sort): inter regions of at most 16x16 first (one warp each), then the
+// larger ones (one CTA each); residuals by transform size (the residual
+// kernel packs 8, 4, 2 or 1 of them per warp); intra items by superblock
+// anti-diagonal. Within a bucket, bitstream order.
+bool Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageReserve& reserve) {
   const rv9_frame_desc& d = pf.desc;
   fw->desc = d;
   fw->show_existing = pf.show_existing;
@@ -183,17 +181,23 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
   for (int i = 0; i < 3; ++i) fw->ref_slot[i] = pf.ref_slot[i];
   memset(fw->kbytes, 0, sizeof fw->kbytes);
   fw->total_bytes = 0;
-  if (pf.show_existing) return;
-  units_.clear();
-  res_.clear();
+  if (pf.show_existing) return true;
+  units_small_.clear();
+  units_large_.clear();
+  for (auto& r : res_by_size_) r.clear();
   intra_.clear();
+  intra_diag_.clear();
   const uint64_t bps = d.bit_depth > 8 ? 2 : 1;
+  uint64_t out_bytes = 0;  // inter outputs, to take out of the reference bytes
   for (uint32_t bi = 0; bi < pf.blocks.size(); ++bi) {
     const rv9_block& b = pf.blocks[bi];
     const bool is_inter = b.flags & RV9_BLK_INTER;
     const bool avail_l = b.flags & RV9_BLK_AVAIL_L, avail_u = b.flags & RV9_BLK_AVAIL_U;
     const int bsize = std::max<int>(b.mi_size, BLOCK_8X8);
     const int nrefs = b.ref_frame[1] > INTRA_FRAME ? 2 : 1;
+    // Superblock anti-diagonal (column + 2 row): every superblock an intra
+    // block reads from lies on an earlier one.
+    const uint16_t diag = (uint16_t)((b.mi_col >> 3) + 2 * (b.mi_row >> 3));
     uint32_t tok = b.tok_start;
     for (int plane = 0; plane < 3; ++plane) {
       int tx_sz = plane ? uv_tx_size(d, b) : b.tx_size;
@@ -206,13 +210,16 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
         if (b.mi_size < BLOCK_8X8) {
           for (int y = 0; y < n4h; ++y)
             for (int x = 0; x < n4w; ++x)
-              units_.push_back(InterUnit{bi, (uint16_t)(base_x + 4 * x), (uint16_t)(base_y + 4 * y), (uint8_t)plane, 1,
-                                         1, (uint8_t)(y * n4w + x)});
+              units_small_.push_back(InterUnit{bi, (uint16_t)(base_x + 4 * x), (uint16_t)(base_y + 4 * y),
+                                               (uint8_t)plane, 1, 1, (uint8_t)(y * n4w + x)});
         } else {
-          units_.push_back(
-              InterUnit{bi, (uint16_t)base_x, (uint16_t)base_y, (uint8_t)plane, (uint8_t)n4w, (uint8_t)n4h, 0});
+          (n4w <= 4 && n4h <= 4 ? units_small_ : units_large_)
+              .push_back(InterUnit{bi, (uint16_t)base_x, (uint16_t)base_y, (uint8_t)plane, (uint8_t)n4w,
+                                   (uint8_t)n4h, 0});
         }
-        fw->kbytes[K_INTER] += (uint64_t)n4w * n4h * 16 * bps * (nrefs + 1);
+        const uint64_t out = (uint64_t)n4w * n4h * 16 * bps;
+        fw->kbytes[K_INTER] += out * (nrefs + 1);
+        out_bytes += out;
       }
       int max_x = (int)((d.mi_cols * 8) >> sx), max_y = (int)((d.mi_rows * 8) >> sy);
       int block_idx = 0;
@@ -229,7 +236,7 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
             const uint64_t coef_bytes = t != NO_TOK ? sizeof(rv9_tok) + 4ull * pf.toks[t].n_coef : 0;
             if (is_inter) {
               if (t != NO_TOK) {
-                res_.push_back(ResItem{t, bi});
+                res_by_size_[pf.toks[t].tx_size & 3].push_back(ResItem{t, bi});
                 fw->kbytes[K_INTER_RES] += coef_bytes + 2 * n0 * n0 * bps;
               }
             } else {
@@ -237,6 +244,7 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
               uint8_t fl = (uint8_t)((avail_l || x > 0 ? 1 : 0) | (avail_u || y > 0 ? 2 : 0) | (x + step < n4w ? 4 : 0));
               intra_.push_back(IntraItem{bi, t, (uint16_t)start_x, (uint16_t)start_y, (uint8_t)plane, (uint8_t)tx_sz,
                                          (uint8_t)mode, fl});
+              intra_diag_.push_back(diag);
               fw->kbytes[K_INTRA] += (n0 * n0 + 3 * n0 + 1) * bps + coef_bytes;
             }
           }
@@ -253,47 +261,19 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
   fw->kbytes[K_INTRA_MARK] = intra_.size() * sizeof(IntraItem);
   // The frame's algorithmic bytes: records read once, reference samples
   // predicted from, and the reconstructed samples written once.
-  uint64_t ref_bytes = fw->kbytes[K_INTER];
-  for (const InterUnit& u : units_) ref_bytes -= (uint64_t)u.w4 * u.h4 * 16 * bps;  // minus the outputs
+  const uint64_t ref_bytes = fw->kbytes[K_INTER] - out_bytes;
   fw->total_bytes = pf.blocks.size() * sizeof(rv9_block) + pf.toks.size() * sizeof(rv9_tok) +
                     pf.coefs.size() * 4 + ref_bytes + area;
-  size_t base = align256(out->size());
-  out->resize(base);
-  fw->o_blocks = put(out, pf.blocks.data(), pf.blocks.size());
-  fw->o_toks = put(out, pf.toks.data(), pf.toks.size());
-  fw->o_coefs = put(out, pf.coefs.data(), pf.coefs.size());
-  // Regions of at most 16x16 first (one warp each), then the larger ones
-  // (one CTA each).
-  std::stable_partition(units_.begin(), units_.end(), [](const InterUnit& u) { return u.w4 <= 4 && u.h4 <= 4; });
-  fw->n_units_small = 0;
-  for (const InterUnit& u : units_) fw->n_units_small += (u.w4 <= 4 && u.h4 <= 4) ? 1 : 0;
-  fw->o_units = put(out, units_.data(), units_.size());
-  // Residuals by transform size (the residual kernel packs 8, 4, 2 or 1 of
-  // them per warp).
-  std::stable_sort(res_.begin(), res_.end(), [&](const ResItem& a, const ResItem& b) {
-    return pf.toks[a.tok].tx_size < pf.toks[b.tok].tx_size;
-  });
-  for (int z = 0; z < 4; ++z) fw->n_res_by_size[z] = 0;
-  for (const ResItem& r : res_) ++fw->n_res_by_size[pf.toks[r.tok].tx_size & 3];
-  fw->o_res = put(out, res_.data(), res_.size());
-  // The intra wavefront takes its items in list order, one per free warp:
-  // superblocks in anti-diagonal order (d = column + 2 row; every superblock
-  // an intra block reads from lies on an earlier diagonal), bitstream order
-  // within a superblock. Bitstream order alone would keep the warps in flight
-  // on about one superblock row at a time.
+  // Intra items by anti-diagonal: a counting sort, stable.
   if (!intra_.empty()) {
-    std::vector<std::pair<uint64_t, uint32_t>> key(intra_.size());
-    for (size_t i = 0; i < intra_.size(); ++i) {
-      const rv9_block& b = pf.blocks[intra_[i].block];
-      uint64_t d = (uint64_t)(b.mi_col >> 3) + 2 * (uint64_t)(b.mi_row >> 3);
-      key[i] = {(d << 32) | i, (uint32_t)i};
-    }
-    std::sort(key.begin(), key.end());
+    size_t n_diag = (size_t)(d.sb64_cols + 2 * d.sb64_rows) + 1;
+    diag_start_.assign(n_diag + 1, 0);
+    for (uint16_t g : intra_diag_) ++diag_start_[g + 1];
+    for (size_t g = 0; g < n_diag; ++g) diag_start_[g + 1] += diag_start_[g];
     sorted_intra_.resize(intra_.size());
-    for (size_t i = 0; i < key.size(); ++i) sorted_intra_[i] = intra_[key[i].second];
+    for (size_t i = 0; i < intra_.size(); ++i) sorted_intra_[diag_start_[intra_diag_[i]]++] = intra_[i];
     intra_.swap(sorted_intra_);
   }
-  fw->o_intra = put(out, intra_.data(), intra_.size());
   // Jobs: one row of transform blocks of one block and plane (contiguous in
   // this order), done by one warp in turn. Each depends on its left
   // neighbour anyway, so a row loses no parallelism by staying on one warp.
@@ -304,15 +284,74 @@ void Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<u
       intra_jobs_.push_back((uint32_t)i);
   fw->n_intra_jobs = (uint32_t)intra_jobs_.size();
   intra_jobs_.push_back((uint32_t)intra_.size());
-  fw->o_intra_jobs = put(out, intra_jobs_.data(), intra_jobs_.size());
-  out->resize(align256(out->size()));
-  fw->bytes = out->size() - base;
+  // The staged layout: each array at a 256-byte boundary.
+  size_t n_res = 0;
+  for (int z = 0; z < 4; ++z) {
+    fw->n_res_by_size[z] = (uint32_t)res_by_size_[z].size();
+    n_res += res_by_size_[z].size();
+  }
+  const size_t n_units = units_small_.size() + units_large_.size();
+  size_t rel = 0;
+  auto place = [&](size_t bytes) {
+    size_t o = rel;
+    rel = align256(rel + bytes);
+    return o;
+  };
+  const size_t r_blocks = place(pf.blocks.size() * sizeof(rv9_block));
+  const size_t r_toks = place(pf.toks.size() * sizeof(rv9_tok));
+  const size_t r_coefs = place(pf.coefs.size() * 4);
+  const size_t r_units = place(n_units * sizeof(InterUnit));
+  const size_t r_res = place(n_res * sizeof(ResItem));
+  const size_t r_intra = place(intra_.size() * sizeof(IntraItem));
+  const size_t r_jobs = place(intra_jobs_.size() * 4);
+  size_t base = 0;
+  uint8_t* dst = reserve(rel, &base);
+  if (!dst) return false;
+  auto copy = [&](size_t r, const void* src, size_t bytes) {
+    if (bytes) memcpy(dst + r, src, bytes);
+  };
+  // Zero padding after each array, so that the staged bytes depend on the
+  // frame alone.
+  const size_t ends[7][2] = {{r_blocks, pf.blocks.size() * sizeof(rv9_block)},
+                             {r_toks, pf.toks.size() * sizeof(rv9_tok)},
+                             {r_coefs, pf.coefs.size() * 4},
+                             {r_units, n_units * sizeof(InterUnit)},
+                             {r_res, n_res * sizeof(ResItem)},
+                             {r_intra, intra_.size() * sizeof(IntraItem)},
+                             {r_jobs, intra_jobs_.size() * 4}};
+  for (const auto& e : ends) {
+    const size_t end = e[0] + e[1];
+    memset(dst + end, 0, align256(end) - end);
+  }
+  copy(r_blocks, pf.blocks.data(), pf.blocks.size() * sizeof(rv9_block));
+  copy(r_toks, pf.toks.data(), pf.toks.size() * sizeof(rv9_tok));
+  copy(r_coefs, pf.coefs.data(), pf.coefs.size() * 4);
+  copy(r_units, units_small_.data(), units_small_.size() * sizeof(InterUnit));
+  copy(r_units + units_small_.size() * sizeof(InterUnit), units_large_.data(),
+       units_large_.size() * sizeof(InterUnit));
+  size_t r = r_res;
+  for (int z = 0; z < 4; ++z) {
+    copy(r, res_by_size_[z].data(), res_by_size_[z].size() * sizeof(ResItem));
+    r += res_by_size_[z].size() * sizeof(ResItem);
+  }
+  copy(r_intra, intra_.data(), intra_.size() * sizeof(IntraItem));
+  copy(r_jobs, intra_jobs_.data(), intra_jobs_.size() * 4);
+  fw->o_blocks = base + r_blocks;
+  fw->o_toks = base + r_toks;
+  fw->o_coefs = base + r_coefs;
+  fw->o_units = base + r_units;
+  fw->o_res = base + r_res;
+  fw->o_intra = base + r_intra;
+  fw->o_intra_jobs = base + r_jobs;
+  fw->bytes = rel;
   fw->n_blocks = (uint32_t)pf.blocks.size();
   fw->n_toks = (uint32_t)pf.toks.size();
   fw->n_coefs = (uint32_t)pf.coefs.size();
-  fw->n_units = (uint32_t)units_.size();
-  fw->n_res = (uint32_t)res_.size();
+  fw->n_units = (uint32_t)n_units;
+  fw->n_units_small = (uint32_t)units_small_.size();
+  fw->n_res = (uint32_t)n_res;
   fw->n_intra = (uint32_t)intra_.size();
+  return true;
 }
 
 void Engine::hook(void* ctx, int kernel, int phase) {
@@ -532,27 +571,41 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
 
 rv9::Status Engine::recon(const rv9::ParsedFrame& pf, DevFrame** shown, std::string* err) {
   FrameWork fw;
-  host_work_.clear();
-  build_work(pf, &fw, &host_work_);
-  if (pf.show_existing) return run_frame(fw, nullptr, false, shown, err);
-  // Stage the bytes in the pinned buffer of this turn (its previous copy
-  // done), one copy to the device.
+  if (pf.show_existing) {
+    build_work(pf, &fw, StageReserve());
+    return run_frame(fw, nullptr, false, shown, err);
+  }
+  // The frame's bytes go straight into the pinned buffer of this turn (its
+  // previous copy done), then one copy to the device.
   int s = stage_;
   stage_ ^= 1;
   CK(cudaEventSynchronize(stage_ev_[s]));
+  cudaError_t alloc_err = cudaSuccess;
+  auto reserve = [&](size_t n, size_t* base) -> uint8_t* {
+    *base = 0;
+    if (n > h_stage_cap_[s]) {
+      size_t cap = std::max(n, h_stage_cap_[s] * 3 / 2);
+      cudaFreeHost(h_stage_[s]);
+      h_stage_[s] = nullptr;
+      h_stage_cap_[s] = 0;
+      if ((alloc_err = cudaMallocHost(&h_stage_[s], cap)) != cudaSuccess) return nullptr;
+      h_stage_cap_[s] = cap;
+    }
+    return h_stage_[s];
+  };
+  if (!build_work(pf, &fw, reserve)) {
+    *err = std::string("pinned staging buffer: ") + cudaGetErrorString(alloc_err);
+    return rv9::ST_DEVICE;
+  }
   if (fw.bytes > stage_cap_[s]) {
     size_t cap = std::max(fw.bytes, stage_cap_[s] * 3 / 2);
     CK(cudaStreamSynchronize(stream_));
     cudaFree(d_stage_[s]);
-    cudaFreeHost(h_stage_[s]);
     d_stage_[s] = nullptr;
-    h_stage_[s] = nullptr;
     stage_cap_[s] = 0;
     CK(cudaMalloc(&d_stage_[s], cap));
-    CK(cudaMallocHost(&h_stage_[s], cap));
     stage_cap_[s] = cap;
   }
-  memcpy(h_stage_[s], host_work_.data(), fw.bytes);
   CK(cudaMemcpyAsync(d_stage_[s], h_stage_[s], fw.bytes, cudaMemcpyHostToDevice, stream_));
   CK(cudaEventRecord(stage_ev_[s], stream_));
   return run_frame(fw, d_stage_[s], false, shown, err);
@@ -590,8 +643,13 @@ rv9::Status Engine::sequence_load(const std::vector<rv9::ParsedFrame>& frames, S
   std::vector<uint8_t> host;
   seq->frames.resize(frames.size());
   seq->luma_samples = 0;
+  auto reserve = [&](size_t n, size_t* base) -> uint8_t* {
+    *base = host.size();
+    host.resize(*base + n);
+    return host.data() + *base;
+  };
   for (size_t i = 0; i < frames.size(); ++i) {
-    build_work(frames[i], &seq->frames[i], &host);
+    build_work(frames[i], &seq->frames[i], reserve);
     const rv9::ParsedFrame& pf = frames[i];
     if (pf.show_existing || pf.show_frame) {
       // Visible luma of the shown frame (show_existing shows a slot of the
@@ -846,18 +904,24 @@ rv9::Status Engine::reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint
     held.push_back(f);
   }
   for (DevFrame* h : held) --h->refs;
-  for (int s = 0; s < 2; ++s)
+  for (int s = 0; s < 2; ++s) {
     if (stage_bytes > stage_cap_[s]) {
       CK(cudaStreamSynchronize(stream_));
       cudaFree(d_stage_[s]);
-      cudaFreeHost(h_stage_[s]);
       d_stage_[s] = nullptr;
-      h_stage_[s] = nullptr;
       stage_cap_[s] = 0;
       CK(cudaMalloc(&d_stage_[s], stage_bytes));
-      CK(cudaMallocHost(&h_stage_[s], stage_bytes));
       stage_cap_[s] = stage_bytes;
     }
+    if (stage_bytes > h_stage_cap_[s]) {
+      CK(cudaStreamSynchronize(stream_));
+      cudaFreeHost(h_stage_[s]);
+      h_stage_[s] = nullptr;
+      h_stage_cap_[s] = 0;
+      CK(cudaMallocHost(&h_stage_[s], stage_bytes));
+      h_stage_cap_[s] = stage_bytes;
+    }
+  }
   size_t mi_len = (size_t)d.mi_cols * d.mi_rows;
   if (mi_len > lf_mi_cap_) {
     CK(cudaStreamSynchronize(stream_));

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -166,7 +167,10 @@ class Engine {
 
  private:
   DevFrame* alloc_frame(const rv9_frame_desc& d);
-  void build_work(const rv9::ParsedFrame& pf, FrameWork* fw, std::vector<uint8_t>* out);
+  // Room for a frame's `n` staged bytes; *base receives their offset in the
+  // buffer that the frame's offsets refer to. nullptr when it can't be had.
+  using StageReserve = std::function<uint8_t*(size_t n, size_t* base)>;
+  bool build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageReserve& reserve);
   rv9::Status run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
                         std::string* err);
   void reset_slots();
@@ -185,10 +189,10 @@ class Engine {
   cudaStream_t stream_ = nullptr;
   std::vector<DevFrame*> pool_;
   DevFrame* slots_[8] = {nullptr};
-  // Record staging for recon(): pinned host buffers (double-buffered) and
-  // device buffers.
-  std::vector<uint8_t> host_work_;
+  // Record staging for recon(): pinned host buffers (double-buffered),
+  // which build_work writes into directly, and device buffers.
   uint8_t* h_stage_[2] = {nullptr, nullptr};
+  size_t h_stage_cap_[2] = {0, 0};
   uint8_t* d_stage_[2] = {nullptr, nullptr};
   size_t stage_cap_[2] = {0, 0};
   cudaEvent_t stage_ev_[2] = {nullptr, nullptr};
@@ -208,9 +212,11 @@ class Engine {
   size_t kev_used_ = 0;
   const FrameWork* cur_fw_ = nullptr;
   // Work lists of the frame being built.
-  std::vector<InterUnit> units_;
-  std::vector<ResItem> res_;
+  std::vector<InterUnit> units_small_, units_large_;
+  std::vector<ResItem> res_by_size_[4];
   std::vector<IntraItem> intra_, sorted_intra_;
+  std::vector<uint16_t> intra_diag_;
+  std::vector<uint32_t> diag_start_;
   std::vector<uint32_t> intra_jobs_;
 };
 

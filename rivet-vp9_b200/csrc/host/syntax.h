@@ -1391,51 +1391,59 @@ struct TileCoder {
     uint32_t* out = coefs.grow(seg_eob);
     uint32_t n_out = 0;
     uint8_t* tc = token_cache;
-    bool check_eob = true;
     int c = 0;
-    for (; c < seg_eob; ++c) {
-      const int pos = scan[c];
-      const int band = bands[c];
-      if (c > 0) ctx = (1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1;
-      const uint8_t* probs = cp[band][ctx];
-      if (check_eob) {
-        bool more = BoolDecoder::read(r, probs[0]);
-        if (count) counts.more_coefs[tx_sz][ptype][ref_type][band][ctx][more ? 1 : 0] += 1;
+    const uint8_t* probs = cp[bands[0]][ctx];
+    while (true) {
+      // more_coefs: read at the start and after every nonzero token.
+      {
+        const bool more = BoolDecoder::read(r, probs[0]);
+        if (count) counts.more_coefs[tx_sz][ptype][ref_type][bands[c]][ctx][more ? 1 : 0] += 1;
         if (!more) break;
       }
-      int token;
-      if (!BoolDecoder::read(r, probs[1])) {
-        token = ZERO_TOKEN;
-      } else if (!BoolDecoder::read(r, probs[2])) {
-        token = 1;  // ONE_TOKEN
-      } else {
-        // The rest of the token tree, its probabilities from one pareto row.
-        const uint8_t* pp = pareto_row(probs[2]);
-        int n = 4;
-        do {
-          n = TOKEN_TREE[n + (int)BoolDecoder::read(r, pp[(n >> 1) - 2])];
-        } while (n > 0);
-        token = -n;
+      // A run of zero tokens; after a zero token no more_coefs is read.
+      while (!BoolDecoder::read(r, probs[1])) {
+        if (count) counts.token[tx_sz][ptype][ref_type][bands[c]][ctx][0] += 1;
+        tc[scan[c]] = 0;
+        if (++c == seg_eob) goto done;
+        ctx = (1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1;
+        probs = cp[bands[c]][ctx];
       }
-      if (count) counts.token[tx_sz][ptype][ref_type][band][ctx][token < 2 ? token : 2] += 1;
-      tc[pos] = vp9t_energy_class[token];
-      if (token == ZERO_TOKEN) {
-        check_eob = false;
-        continue;
+      {
+        const int pos = scan[c];
+        int token;
+        int32_t coef;
+        if (!BoolDecoder::read(r, probs[2])) {
+          token = 1;  // ONE_TOKEN
+          coef = 1;
+          tc[pos] = 1;
+        } else {
+          // The rest of the token tree, its probabilities from one pareto row.
+          const uint8_t* pp = pareto_row(probs[2]);
+          int n = 4;
+          do {
+            n = TOKEN_TREE[n + (int)BoolDecoder::read(r, pp[(n >> 1) - 2])];
+          } while (n > 0);
+          token = -n;
+          tc[pos] = vp9t_energy_class[token];
+          coef = EXTRA_BITS[token][2];
+          const int num_extra = EXTRA_BITS[token][1];
+          if (num_extra) {
+            if (token == DCT_VAL_CAT6)
+              for (int e = 0; e < (int)bit_depth - 8; ++e)
+                coef += (int32_t)BoolDecoder::read(r, 255) << (5 + (int)bit_depth - e);
+            const uint8_t* cat = CAT_PROBS[EXTRA_BITS[token][0]];
+            for (int e = 0; e < num_extra; ++e) coef += (int32_t)BoolDecoder::read(r, cat[e]) << (num_extra - 1 - e);
+          }
+        }
+        if (count) counts.token[tx_sz][ptype][ref_type][bands[c]][ctx][token < 2 ? token : 2] += 1;
+        const bool sign = BoolDecoder::read(r, 128);
+        out[n_out++] = RV9_COEF_PACK(pos, sign ? -coef : coef);
       }
-      int32_t coef = EXTRA_BITS[token][2];
-      const int num_extra = EXTRA_BITS[token][1];
-      if (num_extra) {
-        if (token == DCT_VAL_CAT6)
-          for (int e = 0; e < (int)bit_depth - 8; ++e)
-            coef += (int32_t)BoolDecoder::read(r, 255) << (5 + (int)bit_depth - e);
-        const uint8_t* cat = CAT_PROBS[EXTRA_BITS[token][0]];
-        for (int e = 0; e < num_extra; ++e) coef += (int32_t)BoolDecoder::read(r, cat[e]) << (num_extra - 1 - e);
-      }
-      const bool sign = BoolDecoder::read(r, 128);
-      out[n_out++] = RV9_COEF_PACK(pos, sign ? -coef : coef);
-      check_eob = true;
+      if (++c == seg_eob) break;
+      ctx = (1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1;
+      probs = cp[bands[c]][ctx];
     }
+  done:
     coefs.shrink_to(base + n_out);
     bdec.load(r);
     return c;
