@@ -18,6 +18,8 @@
  * averaging and the loop filter — runs as CUDA kernels for sm_100a on the
  * decoder's GPU. There is no CPU reconstruction path: without a usable CUDA
  * device rv9_decoder_new returns NULL and rv9_last_global_error says why.
+ * The host parser is built for x86-64-v3 (AVX2, BMI2, LZCNT); on a CPU
+ * without it rv9_decoder_new likewise returns NULL.
  *
  * Frames come back in the reference's Frame layout: the visible Y, U, V
  * planes one after another, tightly packed (stride == width), one byte per

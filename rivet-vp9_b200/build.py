@@ -37,6 +37,11 @@ HEADERS = [
     "common/vp9_consts.h",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# The host parser's token loop is a chain of dependent shifts and leading-zero
+# counts: built for x86-64-v3 (BMI2 shifts, LZCNT) it runs about 5 % faster.
+# The C ABI refuses to create a decoder or engine on a host CPU without it
+# (rv9_api.cpp, built for the baseline ISA, checks before any parser code).
+HOST_FLAGS = {"host/parser.cpp": ["-Xcompiler", "-march=x86-64-v3"]}
 
 
 def nvcc():
@@ -88,7 +93,7 @@ def build(force=False, verbose=False):
         src = os.path.join(CSRC, s)
         obj = os.path.join(OUT, os.path.basename(s) + ".o")
         cmd = [nvcc(), "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-               *ARCH, "-c", src, "-o", obj]
+               *ARCH, *HOST_FLAGS.get(s, []), "-c", src, "-o", obj]
         if s.endswith(".cpp"):
             cmd[1:1] = ["-x", "cu"] if s.startswith("gpu/") else []
         if "-Xptxas" in os.environ.get("RV9_NVCC_FLAGS", ""):

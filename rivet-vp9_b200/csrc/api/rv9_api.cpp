@@ -35,6 +35,12 @@ static thread_local std::string g_global_err;
 
 namespace rv9api {
 void set_global_error(const std::string& msg) { g_global_err = msg; }
+bool host_isa_ok() {
+  __builtin_cpu_init();
+  if (__builtin_cpu_supports("x86-64-v3")) return true;
+  g_global_err = "the host parser is built for x86-64-v3 (AVX2, BMI2, LZCNT), which this CPU lacks";
+  return false;
+}
 }  // namespace rv9api
 
 static void fill_meta(const rv9g::DevFrame* f, rv9_frame* out) {
@@ -61,6 +67,7 @@ static void fill_meta(const rv9g::DevFrame* f, rv9_frame* out) {
 extern "C" {
 
 rv9_decoder* rv9_decoder_new(int device) {
+  if (!rv9api::host_isa_ok()) return nullptr;
   rv9_decoder* d = new rv9_decoder;
   std::string err;
   if (!d->engine.init(device, &err)) {

@@ -452,6 +452,11 @@ struct TileCoder {
   uint32_t eob_total = 0;
   uint8_t token_cache[1024];
   bool padding_ok = true;
+  // The frame's coefficient probabilities repacked: word k of a band holds
+  // node k's probability for context c in byte c, so the token loop takes a
+  // probability by shifting a word it fetched ahead, not by a load that
+  // waits for the context.
+  uint64_t coef_pk[4][2][2][6][3];
 
   void init(const FrameCtx* fc) {
     f = fc;
@@ -469,6 +474,15 @@ struct TileCoder {
     ss_x = h->ss_x;
     ss_y = h->ss_y;
     padding_ok = true;
+    for (int t = 0; t < 4; ++t)
+      for (int pt = 0; pt < 2; ++pt)
+        for (int rt = 0; rt < 2; ++rt)
+          for (int band = 0; band < 6; ++band)
+            for (int k = 0; k < 3; ++k) {
+              uint64_t w = 0;
+              for (int cx = 0; cx < 6; ++cx) w |= (uint64_t)fc->probs->coef[t][pt][rt][band][cx][k] << (8 * cx);
+              coef_pk[t][pt][rt][band][k] = w;
+            }
   }
 
   MiInfo& mi_at(uint32_t r, uint32_t c) const { return f->mi[(size_t)r * mi_cols + c]; }
@@ -1384,7 +1398,7 @@ struct TileCoder {
   // in locals and the coefficient words written through a raw pointer;
   // returns the end of block.
   int tokens_dec(BoolDecoder& bdec, int tx_sz, int ptype, int ref_type, int ctx, const uint16_t* scan,
-                 const uint16_t (*nb)[2], const uint8_t* bands, const uint8_t (*cp)[6][3], bool count, int seg_eob,
+                 const uint16_t (*nb)[2], const uint8_t* bands, const uint64_t (*pk)[3], bool count, int seg_eob,
                  uint32_t bit_depth) {
     BoolDecoder::State r = bdec.save();
     const size_t base = coefs.size();
@@ -1392,33 +1406,36 @@ struct TileCoder {
     uint32_t n_out = 0;
     uint8_t* tc = token_cache;
     int c = 0;
-    const uint8_t* probs = cp[bands[0]][ctx];
+    // The context as a shift into the band's words `w`.
+    int sh = ctx * 8;
+    const uint64_t* w = pk[bands[0]];
     while (true) {
       // more_coefs: read at the start and after every nonzero token.
       {
-        const bool more = BoolDecoder::read(r, probs[0]);
-        if (count) counts.more_coefs[tx_sz][ptype][ref_type][bands[c]][ctx][more ? 1 : 0] += 1;
+        const bool more = BoolDecoder::read(r, (uint8_t)(w[0] >> sh));
+        if (count) counts.more_coefs[tx_sz][ptype][ref_type][bands[c]][sh >> 3][more ? 1 : 0] += 1;
         if (!more) break;
       }
       // A run of zero tokens; after a zero token no more_coefs is read.
-      while (!BoolDecoder::read(r, probs[1])) {
-        if (count) counts.token[tx_sz][ptype][ref_type][bands[c]][ctx][0] += 1;
+      while (!BoolDecoder::read(r, (uint8_t)(w[1] >> sh))) {
+        if (count) counts.token[tx_sz][ptype][ref_type][bands[c]][sh >> 3][0] += 1;
         tc[scan[c]] = 0;
         if (++c == seg_eob) goto done;
-        ctx = (1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1;
-        probs = cp[bands[c]][ctx];
+        w = pk[bands[c]];
+        sh = ((1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1) * 8;
       }
       {
         const int pos = scan[c];
         int token;
         int32_t coef;
-        if (!BoolDecoder::read(r, probs[2])) {
+        const uint8_t p2 = (uint8_t)(w[2] >> sh);
+        if (!BoolDecoder::read(r, p2)) {
           token = 1;  // ONE_TOKEN
           coef = 1;
           tc[pos] = 1;
         } else {
           // The rest of the token tree, its probabilities from one pareto row.
-          const uint8_t* pp = pareto_row(probs[2]);
+          const uint8_t* pp = pareto_row(p2);
           int n = 4;
           do {
             n = TOKEN_TREE[n + (int)BoolDecoder::read(r, pp[(n >> 1) - 2])];
@@ -1435,13 +1452,13 @@ struct TileCoder {
             for (int e = 0; e < num_extra; ++e) coef += (int32_t)BoolDecoder::read(r, cat[e]) << (num_extra - 1 - e);
           }
         }
-        if (count) counts.token[tx_sz][ptype][ref_type][bands[c]][ctx][token < 2 ? token : 2] += 1;
+        if (count) counts.token[tx_sz][ptype][ref_type][bands[c]][sh >> 3][token < 2 ? token : 2] += 1;
         const bool sign = BoolDecoder::read(r, 128);
         out[n_out++] = RV9_COEF_PACK(pos, sign ? -coef : coef);
       }
       if (++c == seg_eob) break;
-      ctx = (1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1;
-      probs = cp[bands[c]][ctx];
+      w = pk[bands[c]];
+      sh = ((1 + tc[nb[c][0]] + tc[nb[c][1]]) >> 1) * 8;
     }
   done:
     coefs.shrink_to(base + n_out);
@@ -1487,7 +1504,8 @@ struct TileCoder {
     int w_eob = 0;
     if (C::kEncode) wc = enc_->tx_coefs(eb_, plane, start_x, start_y, tx_sz, scan, &w_eob);
     if constexpr (!C::kEncode) {
-      c = tokens_dec(d.bd, tx_sz, ptype, ref_type, ctx, scan, nb, bands, cp, count, seg_eob, bd);
+      c = tokens_dec(d.bd, tx_sz, ptype, ref_type, ctx, scan, nb, bands, coef_pk[tx_sz][ptype][ref_type], count,
+                     seg_eob, bd);
     } else {
     for (; c < seg_eob; ++c) {
       int pos = scan[c];

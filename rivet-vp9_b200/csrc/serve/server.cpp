@@ -404,6 +404,7 @@ extern "C" {
 uint64_t rv9_stream_reservation(const rv9_stream_spec* spec) { return spec ? reservation_of(*spec) : 0; }
 
 rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers) {
+  if (!rv9api::host_isa_ok()) return nullptr;
   {
     // The same device check as rv9_decoder_new, with its message.
     rv9g::Engine probe;
