@@ -251,6 +251,14 @@ def run_batched(local, dev, n_streams=64, frames=60):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     for _ in range(2):
         rv9.run_concurrent(pairs)
+    # The plain path first, with the default launch shapes.
+    ms_plain = 0.0
+    for d, sq in pairs:
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        ms_plain += sq.run()
+    # One launch shape for the whole batch, timed together (untimed here).
+    tuned = rv9.autotune_concurrent(pairs)
     flush.zero_()
     torch.cuda.synchronize(dev)
     ms_batched = min(rv9.run_concurrent(pairs) for _ in range(2))
@@ -258,11 +266,6 @@ def run_batched(local, dev, n_streams=64, frames=60):
     flush.zero_()
     torch.cuda.synchronize(dev)
     ms_batched_graph = min(rv9.run_concurrent(pairs, graph=True) for _ in range(2))
-    ms_plain = 0.0
-    for d, sq in pairs:
-        flush.zero_()
-        torch.cuda.synchronize(dev)
-        ms_plain += sq.run()
     out = {
         "workload": f"{n_streams} streams over 8 generated contents {{320x240, 640x360, 1280x720, 1920x1080}} x "
                     f"{{8, 10}}-bit 4:2:0, q per content in [35, 85], {CLASS_FRAMES} frames looped to {frames}",
@@ -275,6 +278,7 @@ def run_batched(local, dev, n_streams=64, frames=60):
                          "speedup_vs_plain": round(ms_plain / ms_batched_graph, 2),
                          "ms": round(ms_batched_graph, 3)},
         "how": "rv9_sequences_run over 64 decoders (own CUDA stream and slots each) vs rv9_sequence_run one by one",
+        "autotune": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in tuned.items()},
     }
     for sq in seqs + base:
         sq.free()
@@ -405,8 +409,8 @@ def run_gpu(args, world, rank, local):
     def launches_total():
         return sum(d.stats()["kernel_launches"] for d in decs)
 
-    # Launch shapes per decoder from the autotuner (untimed).
-    tuned = [d.autotune(sq) for d, sq in pairs]
+    # One launch shape for the two streams, timed together (untimed).
+    tuned = rv9.autotune_concurrent(pairs)
     for _ in range(args.warmup):
         step(False)
     kernel_stats()
@@ -459,10 +463,11 @@ def run_gpu(args, world, rank, local):
     frame_bytes = 1920 * 1080 * 3 // 2
     cap = max(len(pk) for pk in packets) * frame_bytes + (1 << 20)
     host_outs = [torch.empty(cap, dtype=torch.uint8, pin_memory=True) for _ in packets]
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 5))
     h2d = sum(s.record_bytes for s in seqs)
     d2h = 0
     e2e_secs = 0.0
+    e2e_each = []
     last_md5 = None
     for i in range(e2e_steps + 1):
         torch.cuda.synchronize(dev)
@@ -486,6 +491,7 @@ def run_gpu(args, world, rank, local):
             raise RuntimeError("an end-to-end decode thread failed")
         if i > 0:  # the first pass warms the frame pools
             e2e_secs += dt
+            e2e_each.append(round(dt * 1e3, 1))
         d2h = sum(nb for _, nb in results)
         nb = results[-1][1]
         last_md5 = hashlib.md5(bytes(host_outs[-1][nb - frame_bytes: nb].numpy())).hexdigest()
@@ -522,12 +528,11 @@ def run_gpu(args, world, rank, local):
                        "l2": "flushed before each step (256 MiB write); records per step exceed L2",
                        "parallelism": f"replicas x{world}", "records_resident_bytes": h2d},
             "e2e": {"value": round(e2e_value, 2), "unit": "Mpixels/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps, "ms_each_step": e2e_each},
             "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "traffic": traffic},
-            "autotune": [{"intra_ctas_per_sm_x4": t["intra_ctas_per_sm_x4"], "inter_threads": t["inter_threads"],
-                          "best_ms": round(t["best_ms"], 3), "default_ms": round(t["default_ms"], 3)} for t in tuned],
+            "autotune": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in tuned.items()},
             "graph_replay": {"value": round(whole_job_value(luma_per_step, world, ms_graph), 2),
                              "unit": "Mpixels/s", "ms_per_step": round(ms_graph, 3),
                              "how": "the same steps replayed as CUDA graphs (captured once; first replay untimed)"},

@@ -197,6 +197,14 @@ typedef struct rv9_tune_result {
   double default_ms;            /* ... and with the defaults (4, 128) */
 } rv9_tune_result;
 rv9_status rv9_decoder_autotune(rv9_decoder* dec, rv9_sequence* seq, rv9_tune_result* out);
+/* The same for sequences reconstructed together (rv9_sequences_run): each
+ * candidate shape is applied to every decoder and the batch is timed as a
+ * whole; every decoder keeps the fastest for its sequence's geometries. The
+ * best shape for one stream alone (a wavefront grid sized to the whole GPU)
+ * can crowd the other streams out when many share the device. Times are the
+ * batch's; graphs captured before tuning keep their old shapes. */
+rv9_status rv9_sequences_autotune(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n,
+                                  rv9_tune_result* out);
 
 /* The frame in reference slot `slot` (0..7), packed like rv9_frame data. */
 rv9_status rv9_decoder_download_slot(rv9_decoder* dec, int slot, uint8_t* out, size_t cap, size_t* bytes);

@@ -313,6 +313,28 @@ rv9_status rv9_decoder_autotune(rv9_decoder* d, rv9_sequence* s, rv9_tune_result
   return (rv9_status)st;
 }
 
+rv9_status rv9_sequences_autotune(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n,
+                                  rv9_tune_result* out) {
+  if (!out || (n && (!decs || !seqs))) return RV9_INVALID_INPUT;
+  std::vector<rv9g::Engine*> engines(n);
+  std::vector<const rv9g::Sequence*> ss(n);
+  for (size_t i = 0; i < n; ++i) {
+    if (!decs[i] || !seqs[i]) return RV9_INVALID_INPUT;
+    engines[i] = &decs[i]->engine;
+    ss[i] = &seqs[i]->seq;
+  }
+  rv9g::TuneParams best;
+  float best_ms = 0, default_ms = 0;
+  std::string err;
+  rv9::Status st = rv9g::Engine::autotune_concurrent(engines.data(), ss.data(), n, &best, &best_ms, &default_ms, &err);
+  if (st != rv9::ST_OK && n) decs[0]->err = err;
+  out->intra_ctas_per_sm_x4 = best.intra_ctas_per_sm_x4;
+  out->inter_threads = best.inter_threads;
+  out->best_ms = best_ms;
+  out->default_ms = default_ms;
+  return (rv9_status)st;
+}
+
 rv9_status rv9_decoder_download_slot(rv9_decoder* d, int slot, uint8_t* out, size_t cap, size_t* bytes) {
   *bytes = 0;
   if (slot < 0 || slot > 7 || !d->engine.slot(slot)) return RV9_INVALID_INPUT;

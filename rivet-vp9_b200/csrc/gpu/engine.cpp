@@ -730,6 +730,49 @@ rv9::Status Engine::autotune(const Sequence& seq, TuneParams* best, float* best_
   return rv9::ST_OK;
 }
 
+rv9::Status Engine::autotune_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
+                                        TuneParams* best, float* best_ms, float* default_ms, std::string* err) {
+  *best = TuneParams();
+  *best_ms = *default_ms = 0;
+  if (n == 0) return rv9::ST_OK;
+  // The batch's time with given shapes: the better of two runs after one
+  // untimed run.
+  auto time_with = [&](const TuneParams& tp, float* out) -> rv9::Status {
+    for (size_t j = 0; j < n; ++j) engines[j]->tune_override_ = &tp;
+    float ms = 0, bestr = 0;
+    rv9::Status st = rv9::ST_OK;
+    for (int r = 0; r < 3 && st == rv9::ST_OK; ++r) {
+      st = run_concurrent(engines, seqs, n, false, &ms, err);
+      if (r == 1 || (r > 1 && ms < bestr)) bestr = ms;
+    }
+    for (size_t j = 0; j < n; ++j) engines[j]->tune_override_ = nullptr;
+    *out = bestr;
+    return st;
+  };
+  rv9::Status st = time_with(TuneParams(), default_ms);
+  if (st != rv9::ST_OK) return st;
+  *best_ms = *default_ms;
+  const int grains[] = {1, 2, 4, 8, 16};
+  const int threads[] = {64, 128, 256};
+  for (int g : grains)
+    for (int t : threads) {
+      TuneParams tp;
+      tp.intra_ctas_per_sm_x4 = g;
+      tp.inter_threads = t;
+      float ms = 0;
+      st = time_with(tp, &ms);
+      if (st != rv9::ST_OK) return st;
+      if (ms < *best_ms) {
+        *best_ms = ms;
+        *best = tp;
+      }
+    }
+  for (size_t j = 0; j < n; ++j)
+    for (const FrameWork& fw : seqs[j]->frames)
+      if (!fw.show_existing) engines[j]->tuned_[geometry_key(fw.desc)] = *best;
+  return rv9::ST_OK;
+}
+
 rv9::Status Engine::sequence_graph(const Sequence& seq, std::string* err) {
   if (seq.graph) return rv9::ST_OK;
   float ms = 0;

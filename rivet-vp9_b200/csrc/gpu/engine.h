@@ -136,6 +136,13 @@ class Engine {
   // completion, on engines[0]'s stream.
   static rv9::Status run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
                                     bool per_kernel, float* ms, std::string* err, bool graphs = false);
+  // The autotuner for sequences reconstructed together: times run_concurrent
+  // with each candidate shape applied to every engine, and gives each engine
+  // the fastest for its sequence's geometries. Shapes that suit one stream
+  // alone (the whole GPU for one wavefront) can crowd the others out when
+  // many streams share the device.
+  static rv9::Status autotune_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
+                                         TuneParams* best, float* best_ms, float* default_ms, std::string* err);
   int device() const { return device_; }
   // The device error word as last copied back (nonzero after a wavefront
   // wait gave up; sync() reports and clears it).

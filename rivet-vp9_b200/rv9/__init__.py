@@ -72,7 +72,8 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
-           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_decoder_autotune")
+           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_decoder_autotune",
+           "rv9_sequences_autotune")
 
 
 class CTuneResult(ctypes.Structure):
@@ -122,6 +123,8 @@ def load_library(path=None):
     lib.rv9_sequence_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.rv9_sequence_run_noalloc.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double)]
     lib.rv9_decoder_autotune.argtypes = [vp, vp, ctypes.POINTER(CTuneResult)]
+    lib.rv9_sequences_autotune.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t,
+                                           ctypes.POINTER(CTuneResult)]
     lib.rv9_sequences_run.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_double)]
     for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
@@ -181,6 +184,24 @@ class Sequence:
 
 RV9_RUN_PER_KERNEL = 1
 RV9_RUN_GRAPH = 2
+
+
+def autotune_concurrent(pairs):
+    """Picks one launch shape for (decoder, sequence) pairs reconstructed
+    together (rv9_sequences_autotune); returns the choice and the batch's
+    times."""
+    if not pairs:
+        return None
+    lib = pairs[0][0]._lib
+    n = len(pairs)
+    decs = (ctypes.c_void_p * n)(*[d._dec for d, _ in pairs])
+    seqs = (ctypes.c_void_p * n)(*[s._h for _, s in pairs])
+    r = CTuneResult()
+    st = lib.rv9_sequences_autotune(decs, seqs, n, ctypes.byref(r))
+    if st != RV9_OK:
+        _raise(lib, pairs[0][0]._dec, st)
+    return {"intra_ctas_per_sm_x4": r.intra_ctas_per_sm_x4, "inter_threads": r.inter_threads,
+            "best_ms": r.best_ms, "default_ms": r.default_ms}
 
 
 def run_concurrent(pairs, per_kernel=False, graph=False):

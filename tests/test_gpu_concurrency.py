@@ -156,3 +156,28 @@ def test_autotune_keeps_results_exact():
         finally:
             s.free()
             d.close()
+
+
+def test_concurrent_autotune_keeps_results_exact():
+    # One shape for decoders reconstructed together: every decoder's slots
+    # after tuning are the same as after a plain run of its sequence alone.
+    import rv9
+    names = NAMES[:3] + NAMES[4:6]
+    decs = [rv9.Decoder(0) for _ in names]
+    seqs = [d.load_sequence(read_packets(os.path.join(VECTORS_DIR, n))) for d, n in zip(decs, names)]
+    try:
+        want = []
+        for d, s in zip(decs, seqs):
+            s.run()
+            want.append(_slots(d))
+        pairs = list(zip(decs, seqs))
+        r = rv9.autotune_concurrent(pairs)
+        assert r["intra_ctas_per_sm_x4"] in (1, 2, 4, 8, 16) and r["inter_threads"] in (64, 128, 256)
+        assert 0 < r["best_ms"] <= r["default_ms"]
+        rv9.run_concurrent(pairs)
+        for d, w, n in zip(decs, want, names):
+            assert _slots(d) == w, n
+    finally:
+        for d, s in zip(decs, seqs):
+            s.free()
+            d.close()
