@@ -186,15 +186,17 @@ rv9_status rv9_sequence_clone(rv9_decoder* dec, const rv9_sequence* src, rv9_seq
 
 /* Autotuner (no counterpart in the reference): times the sequence with each
  * candidate launch shape, namely the intra wavefront's grain (its grid: a
- * quarter to four CTAs per SM) and the CTA size of the large-region inter
- * kernel (64, 128 or 256 threads). It keeps the fastest for the geometry of
+ * quarter to four CTAs per SM), the CTA size of the large-region inter
+ * kernel (64, 128 or 256 threads), and whether the small-region inter kernel
+ * runs on a side stream beside it. It keeps the fastest for the geometry of
  * the sequence's frames, and this decoder then uses it for every frame of
  * that geometry. Results are bit-identical under every shape. */
 typedef struct rv9_tune_result {
   int32_t intra_ctas_per_sm_x4; /* chosen grain: quarter CTAs per SM */
   int32_t inter_threads;        /* chosen CTA size */
   double best_ms;               /* the sequence's time with them */
-  double default_ms;            /* ... and with the defaults (4, 128) */
+  double default_ms;            /* ... and with the defaults (4, 128, fork on) */
+  int32_t inter_fork;           /* 1: small inter regions on a side stream beside the large ones */
 } rv9_tune_result;
 rv9_status rv9_decoder_autotune(rv9_decoder* dec, rv9_sequence* seq, rv9_tune_result* out);
 /* The same for sequences reconstructed together (rv9_sequences_run): each

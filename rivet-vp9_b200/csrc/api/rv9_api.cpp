@@ -310,6 +310,7 @@ rv9_status rv9_decoder_autotune(rv9_decoder* d, rv9_sequence* s, rv9_tune_result
   out->inter_threads = best.inter_threads;
   out->best_ms = best_ms;
   out->default_ms = default_ms;
+  out->inter_fork = best.inter_fork ? 1 : 0;
   return (rv9_status)st;
 }
 
@@ -332,6 +333,7 @@ rv9_status rv9_sequences_autotune(rv9_decoder* const* decs, rv9_sequence* const*
   out->inter_threads = best.inter_threads;
   out->best_ms = best_ms;
   out->default_ms = default_ms;
+  out->inter_fork = best.inter_fork ? 1 : 0;
   return (rv9_status)st;
 }
 

@@ -46,6 +46,10 @@ Engine::~Engine() {
   cudaFree(d_counters_);
   cudaFreeHost(h_error_);
   for (cudaEvent_t e : kev_) cudaEventDestroy(e);
+  if (aux_.side) cudaStreamSynchronize(aux_.side);
+  if (aux_.fork) cudaEventDestroy(aux_.fork);
+  if (aux_.join) cudaEventDestroy(aux_.join);
+  if (aux_.side) cudaStreamDestroy(aux_.side);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -76,6 +80,9 @@ bool Engine::init(int device, std::string* err) {
       (e = cudaEventCreate(&ev0_)) != cudaSuccess || (e = cudaEventCreate(&ev1_)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&stage_ev_[0], cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&stage_ev_[1], cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&aux_.side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&aux_.fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&aux_.join, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaMalloc(&d_counters_, 64)) != cudaSuccess || (e = cudaMallocHost(&h_error_, 64)) != cudaSuccess) {
     *err = cudaGetErrorString(e);
     return false;
@@ -551,7 +558,10 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
     auto it = tuned_.find(geometry_key(d));
     if (it != tuned_.end()) tune = it->second;
   }
-  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this, tune));
+  // Captured graphs keep every launch on the one stream: replays of graphs
+  // with the fork's branches measured slower than without them.
+  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this, tune,
+                  capturing_ ? nullptr : &aux_));
   cur_fw_ = nullptr;
   // The device's error word, read at the next sync.
   CK(cudaMemcpyAsync(h_error_ + 1, k.error, 4, cudaMemcpyDeviceToHost, stream_));
@@ -725,6 +735,18 @@ rv9::Status Engine::autotune(const Sequence& seq, TuneParams* best, float* best_
         *best = tp;
       }
     }
+  {
+    // The best shape with the inter fork switched.
+    TuneParams tp = *best;
+    tp.inter_fork = !tp.inter_fork;
+    float ms = 0;
+    st = time_with(tp, &ms);
+    if (st != rv9::ST_OK) return st;
+    if (ms < *best_ms) {
+      *best_ms = ms;
+      *best = tp;
+    }
+  }
   for (const FrameWork& fw : seq.frames)
     if (!fw.show_existing) tuned_[geometry_key(fw.desc)] = *best;
   return rv9::ST_OK;
@@ -767,6 +789,18 @@ rv9::Status Engine::autotune_concurrent(Engine* const* engines, const Sequence* 
         *best = tp;
       }
     }
+  {
+    // The best shape with the inter fork switched.
+    TuneParams tp = *best;
+    tp.inter_fork = !tp.inter_fork;
+    float ms = 0;
+    st = time_with(tp, &ms);
+    if (st != rv9::ST_OK) return st;
+    if (ms < *best_ms) {
+      *best_ms = ms;
+      *best = tp;
+    }
+  }
   for (size_t j = 0; j < n; ++j)
     for (const FrameWork& fw : seqs[j]->frames)
       if (!fw.show_existing) engines[j]->tuned_[geometry_key(fw.desc)] = *best;
@@ -783,10 +817,12 @@ rv9::Status Engine::sequence_graph(const Sequence& seq, std::string* err) {
   CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_);
   reset_slots();
+  capturing_ = true;
   for (size_t i = 0; e == cudaSuccess && st == rv9::ST_OK && i < seq.frames.size(); ++i) {
     DevFrame* shown = nullptr;
     st = run_frame(seq.frames[i], seq.d_data, false, &shown, err);
   }
+  capturing_ = false;
   if (e == cudaSuccess) e = cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_);
   cudaGraph_t g = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(stream_, &g);

@@ -28,9 +28,16 @@ typedef void (*LaunchHook)(void* ctx, int kernel, int phase);
 struct TuneParams {
   int intra_ctas_per_sm_x4 = 4;  // 1, 2, 4, 8, 16: a quarter to four CTAs per SM
   int inter_threads = 128;       // 64, 128 or 256
+  bool inter_fork = true;        // small inter regions on the side stream, beside the large ones
+};
+// A side stream of the engine's, and the events that fork work onto it and
+// join it back (both launches of a frame then run side by side).
+struct LaunchAux {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
-                         void* hook_ctx, const TuneParams& tune = TuneParams());
+                         void* hook_ctx, const TuneParams& tune = TuneParams(), const LaunchAux* aux = nullptr);
 cudaError_t upload_filters(const int16_t* f);
 
 // The fixed wavefront scratch: a static device array of this many bytes.
@@ -194,6 +201,8 @@ class Engine {
   int device_ = 0;
   int n_sm_ = 148;
   cudaStream_t stream_ = nullptr;
+  LaunchAux aux_;
+  bool capturing_ = false;  // inside sequence_graph's capture
   std::vector<DevFrame*> pool_;
   DevFrame* slots_[8] = {nullptr};
   // Record staging for recon(): pinned host buffers (double-buffered),

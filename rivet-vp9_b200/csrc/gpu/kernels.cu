@@ -13,9 +13,9 @@
 //                 CTA per larger one; 8-tap H then V passes through shared
 //                 memory, scaled references, compound averaging fused
 //                 (src/dsp/inter.rs, pixel.rs)
-//   k_inter_res_n inverse transform + add of inter blocks' residuals, one
-//                 launch per transform size: 8, 4, 2 or 1 blocks per warp
-//                 (src/dsp/itx.rs)
+//   k_inter_res   inverse transform + add of inter blocks' residuals, all
+//                 transform sizes in one launch: 8, 4, 2 or 1 blocks per
+//                 warp by size (src/dsp/itx.rs)
 //   k_intra       intra prediction + residual as a dependency wavefront:
 //                 a persistent grid takes rows of transform blocks in
 //                 superblock anti-diagonal order and each warp waits only
@@ -423,23 +423,48 @@ __device__ void residual_add_group(const KFrame& k, const rv9_tok& t, int seg, T
   }
 }
 
-// The inter residuals of one transform size: items [first, first + count).
+// The inter residuals of all four transform sizes in one launch. The items
+// are sorted by size; CTAs take them size by size (the first ctas[0] CTAs the
+// 4x4 items, the next ctas[1] the 8x8 ones, and so on), so that the sizes run
+// side by side instead of one launch after another.
+struct ResSplit {
+  int count[4];  // items per size
+  int ctas[4];   // CTAs per size
+};
+
+// One CTA's share of the items of size n: CTA b of that size, items from
+// `first` (the size's first item) on.
 template <class T, class V, int n>
-__global__ void __launch_bounds__(32 * kResWarps) k_inter_res_n(KFrame k, int first, int count) {
+__device__ __forceinline__ void res_cta(const KFrame& k, int b, int first, int count, typename V::store_t* smem) {
   constexpr int n0 = 1 << n, G = 32 / n0, sp = n0 + 1;
-  __shared__ typename V::store_t sc[kResWarps][G][n0 * sp];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, grp = lane / n0, l = lane & (n0 - 1);
-  const int i = (blockIdx.x * kResWarps + warp) * G + grp;
+  const int i = (b * kResWarps + warp) * G + grp;
   if (i >= count) return;  // the whole group
   const unsigned mask = n0 == 32 ? 0xffffffffu : (((1u << n0) - 1u) << (grp * n0));
   const ResItem it = k.res[first + i];
   const rv9_tok& t = k.toks[it.tok];
-  const rv9_block& b = k.blocks[it.block];
+  const rv9_block& bk = k.blocks[it.block];
   const PlanePtr& pp = k.cur[t.plane];
   T* dst = plane_ptr<T>(pp) + (size_t)t.y * pp.stride + t.x;
-  residual_add_group<V, n, T>(k, t, b.segment_id, dst, pp.stride, sc[warp][grp], l, mask);
+  residual_add_group<V, n, T>(k, t, bk.segment_id, dst, pp.stride, smem + (warp * G + grp) * (n0 * sp), l, mask);
 }
 
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kResWarps) k_inter_res(KFrame k, ResSplit sp) {
+  // Per warp 32 (n0 + 1) words at most (one 32x32 block, or G smaller ones).
+  __shared__ typename V::store_t sc[kResWarps * 32 * 33];
+  int b = blockIdx.x, first = 0;
+  if (b < sp.ctas[0]) return res_cta<T, V, 2>(k, b, first, sp.count[0], sc);
+  b -= sp.ctas[0];
+  first += sp.count[0];
+  if (b < sp.ctas[1]) return res_cta<T, V, 3>(k, b, first, sp.count[1], sc);
+  b -= sp.ctas[1];
+  first += sp.count[1];
+  if (b < sp.ctas[2]) return res_cta<T, V, 4>(k, b, first, sp.count[2], sc);
+  b -= sp.ctas[2];
+  first += sp.count[2];
+  res_cta<T, V, 5>(k, b, first, sp.count[3], sc);
+}
 
 // ---------------------------------------------------------------------------
 // Intra wavefront.
@@ -1016,7 +1041,7 @@ cudaError_t upload_filters(const int16_t* f) { return cudaMemcpyToSymbol(c_filte
 
 template <class T, class V>
 static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches,
-                                  LaunchHook hook, void* hctx, const TuneParams& tune) {
+                                  LaunchHook hook, void* hctx, const TuneParams& tune, const LaunchAux* aux) {
   int L = 0;
   auto mark = [&](int id, int phase) {
     if (hook) hook(hctx, id, phase);
@@ -1044,11 +1069,23 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
   }
   if (k.n_units > 0) {
     mark(K_INTER, 0);
-    if (k.n_units_small > 0) {
-      k_inter_small<T><<<(k.n_units_small + kInterThreads / 32 - 1) / (kInterThreads / 32), kInterThreads, 0, s>>>(k);
+    // The two inter kernels write disjoint regions: with a side stream, the
+    // small regions run there beside the large ones (fork and join events on
+    // the frame's stream keep the chain's order around them).
+    const bool small = k.n_units_small > 0, large = k.n_units > k.n_units_small;
+    const bool fork = small && large && aux && aux->side && tune.inter_fork;
+    cudaError_t e;
+    if (fork) {
+      if ((e = cudaEventRecord(aux->fork, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(aux->side, aux->fork, 0)) != cudaSuccess) return e;
+    }
+    if (small) {
+      cudaStream_t ss = fork ? aux->side : s;
+      k_inter_small<T><<<(k.n_units_small + kInterThreads / 32 - 1) / (kInterThreads / 32), kInterThreads, 0, ss>>>(k);
       ++L;
     }
-    if (k.n_units > k.n_units_small) {
+    if (fork && (e = cudaEventRecord(aux->join, aux->side)) != cudaSuccess) return e;
+    if (large) {
       const int nl = k.n_units - k.n_units_small;
       if (tune.inter_threads == 64)
         k_inter<T, 64><<<nl, 64, 0, s>>>(k);
@@ -1058,26 +1095,21 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
         k_inter<T, 128><<<nl, 128, 0, s>>>(k);
       ++L;
     }
+    if (fork && (e = cudaStreamWaitEvent(s, aux->join, 0)) != cudaSuccess) return e;
     mark(K_INTER, 1);
   }
   if (k.n_res > 0) {
     mark(K_INTER_RES, 0);
-    int first = 0;
-#define RV9_RES_LAUNCH(N)                                                                            \
-  {                                                                                                  \
-    const int cnt = k.n_res_by_size[N - 2];                                                          \
-    if (cnt > 0) {                                                                                   \
-      const int per_cta = kResWarps * (32 >> N);                                                     \
-      k_inter_res_n<T, V, N><<<(cnt + per_cta - 1) / per_cta, 32 * kResWarps, 0, s>>>(k, first, cnt); \
-      ++L;                                                                                           \
-    }                                                                                                \
-    first += cnt;                                                                                    \
-  }
-    RV9_RES_LAUNCH(2)
-    RV9_RES_LAUNCH(3)
-    RV9_RES_LAUNCH(4)
-    RV9_RES_LAUNCH(5)
-#undef RV9_RES_LAUNCH
+    ResSplit rs;
+    int grid = 0;
+    for (int z = 0; z < 4; ++z) {
+      const int per_cta = kResWarps * (32 >> (z + 2));
+      rs.count[z] = (int)k.n_res_by_size[z];
+      rs.ctas[z] = (rs.count[z] + per_cta - 1) / per_cta;
+      grid += rs.ctas[z];
+    }
+    k_inter_res<T, V><<<grid, 32 * kResWarps, 0, s>>>(k, rs);
+    ++L;
     mark(K_INTER_RES, 1);
   }
   if (k.n_intra > 0) {
@@ -1118,9 +1150,10 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
 }
 
 cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
-                         void* hook_ctx, const TuneParams& tune) {
-  if (k.bit_depth > 8) return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune);
-  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune);
+                         void* hook_ctx, const TuneParams& tune, const LaunchAux* aux) {
+  if (k.bit_depth > 8)
+    return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune, aux);
+  return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune, aux);
 }
 
 // ---------------------------------------------------------------------------

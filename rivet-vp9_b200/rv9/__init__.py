@@ -78,7 +78,7 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
 
 class CTuneResult(ctypes.Structure):
     _fields_ = [("intra_ctas_per_sm_x4", ctypes.c_int32), ("inter_threads", ctypes.c_int32),
-                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double)]
+                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("inter_fork", ctypes.c_int32)]
 
 
 class CKernelStat(ctypes.Structure):
@@ -201,7 +201,7 @@ def autotune_concurrent(pairs):
     if st != RV9_OK:
         _raise(lib, pairs[0][0]._dec, st)
     return {"intra_ctas_per_sm_x4": r.intra_ctas_per_sm_x4, "inter_threads": r.inter_threads,
-            "best_ms": r.best_ms, "default_ms": r.default_ms}
+            "inter_fork": bool(r.inter_fork), "best_ms": r.best_ms, "default_ms": r.default_ms}
 
 
 def run_concurrent(pairs, per_kernel=False, graph=False):
@@ -364,7 +364,7 @@ class Decoder:
         if st != RV9_OK:
             _raise(self._lib, self._dec, st)
         return {"intra_ctas_per_sm_x4": r.intra_ctas_per_sm_x4, "inter_threads": r.inter_threads,
-                "best_ms": r.best_ms, "default_ms": r.default_ms}
+                "inter_fork": bool(r.inter_fork), "best_ms": r.best_ms, "default_ms": r.default_ms}
 
     def download_slot(self, slot, cap):
         buf = ctypes.create_string_buffer(cap)
