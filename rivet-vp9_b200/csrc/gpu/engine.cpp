@@ -16,8 +16,7 @@
 namespace rv9g {
 using namespace vp9;
 
-const char* const kKernelNames[K_COUNT] = {"k_zero_pad", "k_lf_mi", "k_intra_mark", "k_inter",
-                                           "k_inter_res", "k_intra", "k_lf"};
+const char* const kKernelNames[K_COUNT] = {"k_prep", "k_inter", "k_inter_res", "k_intra", "k_lf"};
 
 #define CK(call)                                                 \
   do {                                                           \
@@ -263,9 +262,9 @@ bool Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageRe
   const uint64_t area = (mi_w * mi_h + 2 * (mi_w >> d.ss_x) * (mi_h >> d.ss_y)) * bps;
   if (d.lf_level) {
     fw->kbytes[K_LF] = 2 * area;
-    fw->kbytes[K_LF_MI] = pf.blocks.size() * sizeof(rv9_block) + (uint64_t)d.mi_cols * d.mi_rows * 4;
+    fw->kbytes[K_PREP] = pf.blocks.size() * sizeof(rv9_block) + (uint64_t)d.mi_cols * d.mi_rows * 4;
   }
-  fw->kbytes[K_INTRA_MARK] = intra_.size() * sizeof(IntraItem);
+  fw->kbytes[K_PREP] += intra_.size() * sizeof(IntraItem);
   // The frame's algorithmic bytes: records read once, reference samples
   // predicted from, and the reconstructed samples written once.
   const uint64_t ref_bytes = fw->kbytes[K_INTER] - out_bytes;

@@ -16,7 +16,7 @@
 namespace rv9g {
 
 // Kernels of a frame, for per-kernel timing and byte accounting.
-enum KernelId { K_ZERO_PAD = 0, K_LF_MI, K_INTRA_MARK, K_INTER, K_INTER_RES, K_INTRA, K_LF, K_COUNT };
+enum KernelId { K_PREP = 0, K_INTER, K_INTER_RES, K_INTRA, K_LF, K_COUNT };
 extern const char* const kKernelNames[K_COUNT];
 
 // Called around each launch when timing per kernel: phase 0 before, 1 after.

@@ -4,10 +4,11 @@
 // stream (reference process: FrameDec::replay, src/decoder/block.rs:1405-1498,
 // then loopfilter::filter_frame, src/decoder/loopfilter.rs:51-81):
 //
-//   k_zero_pad    zero the samples beyond the mode-info area (the reference
-//                 reconstructs into zeroed planes, src/decoder/pool.rs:1-6)
-//   k_lf_mi       per 8x8 loop-filter record from the block records
-//   k_intra_mark  mark the 4x4 cells of intra transform blocks pending
+//   k_prep        three independent parts in one launch: zero the samples
+//                 beyond the mode-info area (the reference reconstructs into
+//                 zeroed planes, src/decoder/pool.rs:1-6), the per-8x8
+//                 loop-filter records from the block records, and the
+//                 pending marks of intra transform blocks' 4x4 cells
 //   k_inter_small / k_inter
 //                 inter prediction: a warp per region of at most 16x16, a
 //                 CTA per larger one; 8-tap H then V passes through shared
@@ -53,9 +54,10 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // ---------------------------------------------------------------------------
 // Zero the samples of the SB-aligned planes outside the mode-info area.
 
+// Zeroing the samples beyond the mode-info area of one plane: part `bx` of
+// `gx` (the reference reconstructs into zeroed planes).
 template <class T>
-__global__ void k_zero_pad(KFrame k) {
-  int plane = blockIdx.y;
+__device__ __forceinline__ void zero_pad_part(const KFrame& k, int plane, int bx, int gx) {
   int sx = plane ? k.ss_x : 0, sy = plane ? k.ss_y : 0;
   int mw = (k.mi_cols * 8) >> sx, mh = (k.mi_rows * 8) >> sy;
   int aw = (k.sb64_cols * 64) >> sx, ah = (k.sb64_rows * 64) >> sy;
@@ -64,7 +66,7 @@ __global__ void k_zero_pad(KFrame k) {
   // Right strip then bottom strip.
   int right = (aw - mw) * mh;
   int total = right + (ah - mh) * aw;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+  for (int i = bx * blockDim.x + threadIdx.x; i < total; i += gx * blockDim.x) {
     int x, y;
     if (i < right) {
       y = i / (aw - mw);
@@ -78,14 +80,10 @@ __global__ void k_zero_pad(KFrame k) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// Loop-filter records per 8x8 (the MiInfo fields loopfilter.rs reads):
-// bits 0-5 level, 6-7 luma tx size, 8-9 chroma tx size, 10-13 block size,
-// 14 coded (intra, or not skipped).
-
-__global__ void k_lf_mi(KFrame k, int n_blocks) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_blocks) return;
+// Loop-filter record per 8x8 (the MiInfo fields loopfilter.rs reads) of
+// block i: bits 0-5 level, 6-7 luma tx size, 8-9 chroma tx size, 10-13
+// block size, 14 coded (intra, or not skipped).
+__device__ __forceinline__ void lf_mi_block(const KFrame& k, int i) {
   const rv9_block& b = k.blocks[i];
   uint32_t v = lf_block_record(b.mi_size, b.tx_size, (b.flags & RV9_BLK_SKIP) ? 1 : 0, b.segment_id, b.y_mode,
                                b.ref_frame[0], k.lvl, k.legacy_uv, k.ss_x, k.ss_y);
@@ -96,12 +94,8 @@ __global__ void k_lf_mi(KFrame k, int n_blocks) {
     for (int x = b.mi_col; x < xe; ++x) k.lf_mi[(size_t)y * k.mi_cols + x] = v;
 }
 
-// ---------------------------------------------------------------------------
-// Intra cells: mark each intra transform block's 4x4 cells pending.
-
-__global__ void k_intra_mark(KFrame k) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= k.n_intra) return;
+// Intra item i's 4x4 cells marked pending.
+__device__ __forceinline__ void intra_mark_item(const KFrame& k, int i) {
   const IntraItem it = k.intra[i];
   int n = 1 << it.tx_size;  // cells per side
   uint8_t* cells = k.cells[it.plane];
@@ -109,6 +103,33 @@ __global__ void k_intra_mark(KFrame k) {
   int cx = it.x >> 2, cy = it.y >> 2;
   for (int y = 0; y < n; ++y)
     for (int x = 0; x < n; ++x) cells[(size_t)(cy + y) * cs + cx + x] = 1;
+}
+
+// A frame's preparation, three independent parts in one launch by CTA range:
+// the zeroed padding (zp_per_plane CTAs per plane), the loop-filter records
+// (one thread per block) and the intra cells' marks (one thread per item).
+constexpr int kPrepThreads = 256;
+struct PrepSplit {
+  int zp_per_plane, zp, lf, mark;  // CTAs of each part (zp = 3 zp_per_plane or 0)
+  int n_blocks;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kPrepThreads) k_prep(KFrame k, PrepSplit ps) {
+  int b = blockIdx.x;
+  if (b < ps.zp) {
+    zero_pad_part<T>(k, b / ps.zp_per_plane, b % ps.zp_per_plane, ps.zp_per_plane);
+    return;
+  }
+  b -= ps.zp;
+  if (b < ps.lf) {
+    const int i = b * kPrepThreads + threadIdx.x;
+    if (i < ps.n_blocks) lf_mi_block(k, i);
+    return;
+  }
+  b -= ps.lf;
+  const int i = b * kPrepThreads + threadIdx.x;
+  if (i < k.n_intra) intra_mark_item(k, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -1047,25 +1068,20 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
     if (hook) hook(hctx, id, phase);
   };
   {
-    int aw = k.sb64_cols * 64, ah = k.sb64_rows * 64;
-    if (k.mi_cols * 8 < aw || k.mi_rows * 8 < ah) {
-      mark(K_ZERO_PAD, 0);
-      k_zero_pad<T><<<dim3(64, 3), 256, 0, s>>>(k);
-      mark(K_ZERO_PAD, 1);
+    const int aw = k.sb64_cols * 64, ah = k.sb64_rows * 64;
+    PrepSplit ps;
+    ps.zp_per_plane = 64;
+    ps.zp = (k.mi_cols * 8 < aw || k.mi_rows * 8 < ah) ? 3 * ps.zp_per_plane : 0;
+    ps.n_blocks = (k.lf_on && n_blocks > 0) ? n_blocks : 0;
+    ps.lf = (ps.n_blocks + kPrepThreads - 1) / kPrepThreads;
+    ps.mark = (k.n_intra + kPrepThreads - 1) / kPrepThreads;
+    const int grid = ps.zp + ps.lf + ps.mark;
+    if (grid > 0) {
+      mark(K_PREP, 0);
+      k_prep<T><<<grid, kPrepThreads, 0, s>>>(k, ps);
+      mark(K_PREP, 1);
       ++L;
     }
-  }
-  if (k.lf_on && n_blocks > 0) {
-    mark(K_LF_MI, 0);
-    k_lf_mi<<<(n_blocks + 127) / 128, 128, 0, s>>>(k, n_blocks);
-    mark(K_LF_MI, 1);
-    ++L;
-  }
-  if (k.n_intra > 0) {
-    mark(K_INTRA_MARK, 0);
-    k_intra_mark<<<(k.n_intra + 127) / 128, 128, 0, s>>>(k);
-    mark(K_INTRA_MARK, 1);
-    ++L;
   }
   if (k.n_units > 0) {
     mark(K_INTER, 0);
