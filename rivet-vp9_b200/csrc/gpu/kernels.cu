@@ -667,6 +667,15 @@ struct Chunk<uint8_t> {
     o.w = (int)((v.y >> 16) & 0xff) | (int)(v.y >> 24) << 16;
     *reinterpret_cast<int4*>(t) = o;
   }
+  // 8 samples held as ints (a line in registers) to global memory.
+  static __device__ __forceinline__ void store_vals(uint8_t* g, const int* v) {
+    uint2 o;
+    o.x = (uint32_t)(v[0] & 0xff) | (uint32_t)(v[1] & 0xff) << 8 | (uint32_t)(v[2] & 0xff) << 16 |
+          (uint32_t)(v[3] & 0xff) << 24;
+    o.y = (uint32_t)(v[4] & 0xff) | (uint32_t)(v[5] & 0xff) << 8 | (uint32_t)(v[6] & 0xff) << 16 |
+          (uint32_t)(v[7] & 0xff) << 24;
+    __stcg(reinterpret_cast<uint2*>(g), o);
+  }
   static __device__ __forceinline__ void store(uint8_t* g, const int16_t* t) {
     int4 o = *reinterpret_cast<const int4*>(t);
     uint2 v;
@@ -685,14 +694,28 @@ struct Chunk<uint16_t> {
   static __device__ __forceinline__ void load(const uint16_t* g, int16_t* t) {
     *reinterpret_cast<int4*>(t) = __ldcg(reinterpret_cast<const int4*>(g));
   }
+  static __device__ __forceinline__ void store_vals(uint16_t* g, const int* v) {
+    int4 o;
+    o.x = (v[0] & 0xffff) | (v[1] << 16);
+    o.y = (v[2] & 0xffff) | (v[3] << 16);
+    o.z = (v[4] & 0xffff) | (v[5] << 16);
+    o.w = (v[6] & 0xffff) | (v[7] << 16);
+    __stcg(reinterpret_cast<int4*>(g), o);
+  }
   static __device__ __forceinline__ void store(uint16_t* g, const int16_t* t) {
     __stcg(reinterpret_cast<int4*>(g), *reinterpret_cast<const int4*>(t));
   }
 };
 
 // Vertical edges of one sample row held in registers (the row from 8 samples
-// left of the superblock), left to right.
-__device__ __forceinline__ void lf_row_regs(int16_t* line, const LfEdge (*e)[16], int n_edges, int run, int bd) {
+// left of the superblock), left to right. The first edge is the last to
+// touch the 8 samples left of the superblock (the next edge is a 4-wide one
+// at offset 4, or none): right after it they go to `strip` (the previous
+// superblock's last 8 columns, final for this row), when given, and with
+// `publish` the warp then adds one step to its row's progress.
+template <class T>
+__device__ __forceinline__ void lf_row_regs(int16_t* line, const LfEdge (*e)[16], int n_edges, int run, int bd,
+                                            T* strip, uint32_t* publish) {
   int v[72];
 #pragma unroll
   for (int q = 0; q < 72; q += 8) {
@@ -720,6 +743,15 @@ __device__ __forceinline__ void lf_row_regs(int16_t* line, const LfEdge (*e)[16]
           for (int q = 0; q < 16; ++q)
             if (4 * ed + q < 72) v[4 * ed + q] = s[q];
         }
+      }
+    }
+    if (ed == 0 && strip) {
+      Chunk<T>::store_vals(strip, v);
+      if (publish) {
+        // Each lane's store before its fence; the warp's step after all.
+        __threadfence();
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) atomicAdd(publish, 1u);
       }
     }
   }
@@ -772,11 +804,11 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
 // share with c+1 stays in shared memory, so the only wait is on the row
 // above: superblock (r, c)'s horizontal pass reads the row above's bottom
 // strip, final once that row has written superblock c back and filtered the
-// vertical edges of c+1 (which reach 7 samples back into c). Each row
-// publishes its progress as (epoch << 16 | steps): per superblock one step
-// when it is written back and one when the next superblock's vertical pass
-// has finalised its last 8 columns' bottom strip, so superblock c of the row
-// above is ready at 2 (c + 1) steps.
+// first vertical edge of c+1 (the only one that reaches back into c, up to 7
+// samples). Each row publishes its progress as (epoch << 16 | steps): per
+// superblock one step when it is written back and one from each filter warp
+// when the next superblock's first vertical edge has made its last 8 columns
+// final, so superblock c of the row above is ready at kLfSteps (c + 1) steps.
 //
 // Warps 0-3 filter: vertical pass, top strip, horizontal pass. Warps 4-7
 // do the rest off that chain: they stage the next superblock (its 8x8
@@ -790,6 +822,10 @@ constexpr int kLfRowThreads = 256;
 constexpr int kLfFilterThreads = 128;
 constexpr int kLfStageThreads = kLfRowThreads - kLfFilterThreads;
 constexpr int kBarFilter = 1, kBarStage = 2, kBarReady0 = 4, kBarHDone0 = 6;  // READY, HDONE: id + parity
+// Progress steps per superblock: one from the stagers' write-back, one from
+// each filter warp when the next superblock's first vertical edge has made
+// its last 8 columns final.
+constexpr int kLfSteps = 1 + kLfFilterThreads / 32;
 
 struct LfRowSmem {
   int16_t px[2][3][kLfH][kLfW];
@@ -884,7 +920,7 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
       const int r = atomicAdd(&k.counters[1], 1);
       S.row = r;
       S.abort_flag = 0;
-      // This row's progress: two steps per superblock (see below), from 0.
+      // This row's progress: kLfSteps per superblock (see below), from 0.
       if (r < rows) *(volatile uint32_t*)&k.sb_done[r] = ep;
     }
     __syncthreads();
@@ -902,7 +938,7 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
         // The top strip (the row above's bottom 8 rows), loaded into
         // registers before the vertical pass when the row above is already
         // far enough; after the wait below otherwise.
-        const int need = 2 * (sc + 1);
+        const int need = kLfSteps * (sc + 1);
         typename Chunk<T>::Raw top[2];
         bool top_early = false;
         const int top_total = 8 * (W[0] + W[1] + W[2]) / 8;
@@ -930,33 +966,26 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
           }
         }
         if (live) {
-          // Vertical edges, one thread per sample row.
+          // Vertical edges, one thread per sample row. Superblock c-1's last
+          // 8 columns are final for a row once its first edge is filtered:
+          // they go out then, and each warp publishes a progress step after
+          // its last row's (the row below waits for their bottom 8 rows).
           const int total = Hh[0] + Hh[1] + Hh[2];
           for (int task = tf; task < total; task += kLfFilterThreads) {
             int p = task < Hh[0] ? 0 : (task < Hh[0] + Hh[1] ? 1 : 2);
             int r = task - (p == 0 ? 0 : (p == 1 ? Hh[0] : Hh[0] + Hh[1]));
-            lf_row_regs(&S.px[cur][p][8 + r][0], S.edges[cur][p ? 1 : 0][0], 16 >> (p ? k.ss_x : 0), r >> 2, bd);
-          }
-          // Superblock c-1's last 8 columns are final for this row now: they
-          // go out at once (the row below waits for their bottom 8 rows).
-          if (sc > 0) {
-            const int total_l = Hh[0] + Hh[1] + Hh[2];
-            for (int task = tf; task < total_l; task += kLfFilterThreads) {
-              int p = task < Hh[0] ? 0 : (task < Hh[0] + Hh[1] ? 1 : 2);
-              int r = task - (p == 0 ? 0 : (p == 1 ? Hh[0] : Hh[0] + Hh[1]));
+            T* strip = nullptr;
+            uint32_t* pub = nullptr;
+            if (sc > 0) {
               const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
-              Chunk<T>::store(plane_ptr<T>(k.cur[p]) + (size_t)(y0 + r) * k.cur[p].stride + x0 - 8,
-                              &S.px[cur][p][8 + r][0]);
+              strip = plane_ptr<T>(k.cur[p]) + (size_t)(y0 + r) * k.cur[p].stride + x0 - 8;
+              if (task + kLfFilterThreads >= total) pub = prog;
             }
+            lf_row_regs<T>(&S.px[cur][p][8 + r][0], S.edges[cur][p ? 1 : 0][0], 16 >> (p ? k.ss_x : 0), r >> 2, bd,
+                           strip, pub);
           }
         }
         named_sync(kBarFilter, kLfFilterThreads);
-        // The barrier orders every filter thread's stores before this one
-        // thread's fence, which publishes them with the progress step.
-        if (live && sc > 0 && tf == 0) {
-          __threadfence();
-          atomicAdd(prog, 1u);
-        }
         // Wait for the row above: superblock c's bottom strip final there.
         if (live && sr > 0 && tf == 0) {
           const volatile uint32_t* above = k.sb_done + (sr - 1);
@@ -1036,13 +1065,14 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
         }
         named_sync(kBarStage, kLfStageThreads);
         if (ts == 0) __threadfence();
-        // One step of the row's progress per superblock written back (two
-        // at the row's end, whose last strip goes out here); the filters add
-        // the other step when they write the superblock's last 8 columns,
-        // final after the next superblock's vertical pass. (The filters own
+        // One step of the row's progress per superblock written back (all
+        // kLfSteps at the row's end, whose last strip goes out here); the
+        // filter warps add the others when they write the superblock's last
+        // 8 columns, final after the next superblock's first vertical edge.
+        // (The filters own
         // columns 0-7 of a buffer: they overwrite them with the next left
         // strip while this group may still be writing the buffer back.)
-        if (ts == 0) atomicAdd(prog, last ? 2u : 1u);
+        if (ts == 0) atomicAdd(prog, last ? (uint32_t)kLfSteps : 1u);
         // Stage superblock c+2 into this superblock's buffer, now written back.
         if (sc + 2 < cols) {
           lf_row_prepare<T>(k, S, P, sr, sc + 2, cur, ts, kLfStageThreads, kBarStage);
