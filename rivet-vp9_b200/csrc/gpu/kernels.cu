@@ -1044,35 +1044,41 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
       for (int sc = 0, cur = 0; sc < cols; ++sc, cur ^= 1) {
         named_sync(kBarHDone0 + (sc & 1), kLfRowThreads);
         const bool last = sc + 1 == cols;
-        if (!S.abort_flag) {
+        // Write-back of the top strip and the superblock but its last 8
+        // columns (the next superblock's first vertical edge still reaches
+        // them), or with them at the row's end; tile rows [lo, hi) of each
+        // plane (tile row 8 is the superblock's first).
+        auto write_back = [&](bool bottom) {
 #pragma unroll
           for (int p = 0; p < 3; ++p) {
             T* dst = plane_ptr<T>(k.cur[p]);
             const int stride = k.cur[p].stride;
             const int x0 = (sc * 64) >> (p ? k.ss_x : 0), y0 = (sr * 64) >> (p ? k.ss_y : 0);
-            const int nc = W[p] / 8;
-            // The top strip, and the superblock but its last 8 columns (the
-            // next superblock's vertical pass still reaches them), or with
-            // them at the row's end.
-            const int r0 = sr > 0 ? 0 : 8;
-            const int nrow = 8 + Hh[p] - r0;
-            for (int i = ts; i < nrow * nc; i += kLfStageThreads) {
-              int r = r0 + i / nc, c = i % nc;
+            const int lnc = (p && k.ss_x) ? 2 : 3, nc = 1 << lnc;
+            const int lo = bottom ? Hh[p] : (sr > 0 ? 0 : 8), hi = bottom ? Hh[p] + 8 : Hh[p];
+            for (int i = ts; i < (hi - lo) * nc; i += kLfStageThreads) {
+              int r = lo + (i >> lnc), c = i & (nc - 1);
               if (r >= 8 && c == nc - 1 && !last) continue;
               Chunk<T>::store(dst + (size_t)(y0 - 8 + r) * stride + x0 + 8 * c, &S.px[cur][p][r][8 + 8 * c]);
             }
           }
-        }
+        };
+        // The bottom 8 rows first, the only ones the row below reads: one
+        // step of the row's progress as soon as they are out (all kLfSteps
+        // at the row's end, whose last strip goes out here). The filter
+        // warps add the others when they write the superblock's last 8
+        // columns, final after the next superblock's first vertical edge.
+        if (!S.abort_flag) write_back(true);
         named_sync(kBarStage, kLfStageThreads);
-        if (ts == 0) __threadfence();
-        // One step of the row's progress per superblock written back (all
-        // kLfSteps at the row's end, whose last strip goes out here); the
-        // filter warps add the others when they write the superblock's last
-        // 8 columns, final after the next superblock's first vertical edge.
-        // (The filters own
-        // columns 0-7 of a buffer: they overwrite them with the next left
-        // strip while this group may still be writing the buffer back.)
-        if (ts == 0) atomicAdd(prog, last ? (uint32_t)kLfSteps : 1u);
+        if (ts == 0) {
+          __threadfence();
+          atomicAdd(prog, last ? (uint32_t)kLfSteps : 1u);
+        }
+        // Then the rest, none of which the row below touches. (The filters
+        // own columns 0-7 of a buffer: they overwrite them with the next
+        // left strip while this group may still be writing the buffer back.)
+        if (!S.abort_flag) write_back(false);
+        named_sync(kBarStage, kLfStageThreads);
         // Stage superblock c+2 into this superblock's buffer, now written back.
         if (sc + 2 < cols) {
           lf_row_prepare<T>(k, S, P, sr, sc + 2, cur, ts, kLfStageThreads, kBarStage);
