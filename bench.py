@@ -316,6 +316,27 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
     t = time.perf_counter()
     d.decode_packets_to(pk, buf.data_ptr(), cap)
     plain = len(pk) * luma["s1080_8"] / (time.perf_counter() - t) / 1e6
+    # The drop-in path as a plain caller uses it: rv9_decode_all packet by
+    # packet (Decoder::decode_all), each frame parsed (tile columns on
+    # threads), reconstructed and read back before the next.
+    import ctypes
+    lib = d._lib
+    cframes = (rv9.CFrame * 16)()
+    n_out = ctypes.c_size_t()
+    d2 = rv9.Decoder(device=local)
+    n_da = min(60, len(pk) - 2)
+    for i in range(2):  # warm (the stream's first packets, decoded in order)
+        lib.rv9_decode_all(d2._dec, pk[i], len(pk[i]), cframes, 16, ctypes.byref(n_out))
+        for j in range(min(n_out.value, 16)):
+            lib.rv9_frame_release(ctypes.byref(cframes[j]))
+    t = time.perf_counter()
+    for i in range(2, 2 + n_da):
+        if lib.rv9_decode_all(d2._dec, pk[i], len(pk[i]), cframes, 16, ctypes.byref(n_out)) != 0:
+            raise RuntimeError("rv9_decode_all failed")
+        for j in range(min(n_out.value, 16)):
+            lib.rv9_frame_release(ctypes.byref(cframes[j]))
+    plain_da = n_da * luma["s1080_8"] / (time.perf_counter() - t) / 1e6
+    d2.close()
     d.close()
     del buf
     for rate, nfr in rates:
@@ -370,6 +391,10 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
                         f"{CLASS_FRAMES} frames looped to {frames}; Poisson arrivals; HBM budget 120 GB",
             "rates": results, "plain_single_stream_e2e_mpixels_s": round(plain, 1),
             "best_vs_plain": round(best / plain, 2),
+            "plain_decode_all_mpixels_s": round(plain_da, 1), "best_vs_decode_all": round(best / plain_da, 2),
+            "plain_note": ("plain_single_stream_e2e: one 1080p stream through rv9_decode_packets (several frames "
+                           "parsed at once); plain_decode_all: the same stream through rv9_decode_all packet by "
+                           "packet, the drop-in Decoder::decode_all path"),
             "latency": "rv9_submit -> frames in pinned host memory (host-function callback); streams admitted and "
                        "their first frame decoded before the timed arrivals",
             "host_cores": os.cpu_count()}
