@@ -219,6 +219,10 @@ typedef struct rv9_kernel_stat {
 } rv9_kernel_stat;
 /* Per-kernel timing of the per_kernel sequence runs; returns the count. */
 size_t rv9_kernel_stats(rv9_decoder* dec, rv9_kernel_stat* out, size_t cap, int reset);
+/* Which kernels per_kernel runs bracket with events: bit i for the i-th entry
+ * of rv9_kernel_stats (default: all). Each pair of events costs the chain a
+ * little time, so a run timed for one kernel's figures brackets only it. */
+void rv9_decoder_set_event_mask(rv9_decoder* dec, uint32_t mask);
 
 #ifdef __cplusplus
 }

@@ -364,6 +364,8 @@ size_t rv9_kernel_stats(rv9_decoder* d, rv9_kernel_stat* out, size_t cap, int re
   return n;
 }
 
+void rv9_decoder_set_event_mask(rv9_decoder* d, uint32_t mask) { d->engine.event_mask = mask; }
+
 void rv9_decoder_stats(rv9_decoder* d, rv9_stats* out, int reset) {
   out->device_ms = d->engine.device_ms;
   out->parse_ms = d->parse_ms;

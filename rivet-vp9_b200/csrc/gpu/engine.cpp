@@ -362,6 +362,7 @@ bool Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageRe
 
 void Engine::hook(void* ctx, int kernel, int phase) {
   Engine* e = (Engine*)ctx;
+  if (!((e->event_mask >> kernel) & 1)) return;
   if (e->kev_used_ == e->kev_.size()) {
     cudaEvent_t ev;
     cudaEventCreate(&ev);

@@ -177,6 +177,7 @@ class Engine {
   double device_ms = 0;
   uint64_t frames = 0, alg_bytes = 0, launches = 0;
   KernelStat kstats[K_COUNT];
+  uint32_t event_mask = ~0u;  // kernels that per_kernel runs bracket with events
   cudaStream_t stream() const { return stream_; }
 
  private:

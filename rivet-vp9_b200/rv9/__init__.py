@@ -73,7 +73,7 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
            "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_decoder_autotune",
-           "rv9_sequences_autotune")
+           "rv9_sequences_autotune", "rv9_decoder_set_event_mask")
 
 
 class CTuneResult(ctypes.Structure):
@@ -135,6 +135,7 @@ def load_library(path=None):
     lib.rv9_sequence_free.argtypes = [vp, vp]
     lib.rv9_sequence_clone.argtypes = [vp, vp, ctypes.POINTER(vp)]
     lib.rv9_decoder_download_slot.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+    lib.rv9_decoder_set_event_mask.argtypes = [vp, ctypes.c_uint32]
     lib.rv9_kernel_stats.restype = ctypes.c_size_t
     lib.rv9_kernel_stats.argtypes = [vp, ctypes.POINTER(CKernelStat), ctypes.c_size_t, ctypes.c_int]
     if path is None:
@@ -373,6 +374,17 @@ class Decoder:
         if st != RV9_OK:
             _raise(self._lib, self._dec, st)
         return buf.raw[:n.value]
+
+    def set_event_mask(self, names=None):
+        """Kernels that per_kernel runs bracket with events (None: all)."""
+        if names is None:
+            mask = 0xFFFFFFFF
+        else:
+            order = list(self.kernel_stats().keys())
+            mask = 0
+            for n in names:
+                mask |= 1 << order.index(n)
+        self._lib.rv9_decoder_set_event_mask(self._dec, mask)
 
     def kernel_stats(self, reset=False):
         arr = (CKernelStat * 16)()
