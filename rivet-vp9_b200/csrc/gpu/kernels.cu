@@ -216,6 +216,7 @@ __device__ __forceinline__ void inter_unit(const KFrame& k, const InterUnit& u, 
   };
   const rv9_block& b = k.blocks[u.block];
   const int w = u.w4 * 4, h = u.h4 * 4, plane = u.plane;
+  const int lw = 31 - __clz(w);  // widths are powers of two
   const int maxv = (1 << k.bit_depth) - 1;
   const bool compound = b.ref_frame[1] > 0;
   T* dst = plane_ptr<T>(k.cur[plane]) + (size_t)u.y * k.cur[plane].stride + u.x;
@@ -228,27 +229,65 @@ __device__ __forceinline__ void inter_unit(const KFrame& k, const InterUnit& u, 
     const int last_x = rp.width - 1, last_y = rp.height - 1, rstride = rp.stride;
     const int ih = (((h - 1) * p.step_y + 15) >> 4) + 8;
     const int y0 = (p.start_y >> 4) - 3;
-    for (int i = tid; i < ih * w; i += NT) {
-      int r = i / w, c = i - r * w;
-      int ry = clampi(y0 + r, 0, last_y);
-      const T* src = ref + (size_t)ry * rstride;
-      int pos = p.start_x + p.step_x * c;
-      int base = (pos >> 4) - 3;
-      const int16_t* f = c_filters[filter][pos & 15];
-      int32_t sum = 0;
+    if (p.step_x == 16) {
+      // Unscaled: one filter phase for the whole unit, its taps in registers,
+      // and no clamping when the window lies inside the reference.
+      const int16_t* fp = c_filters[filter][p.start_x & 15];
+      const int f0 = fp[0], f1 = fp[1], f2 = fp[2], f3 = fp[3], f4 = fp[4], f5 = fp[5], f6 = fp[6], f7 = fp[7];
+      const int bx = (p.start_x >> 4) - 3;
+      const bool inside = bx >= 0 && bx + w + 6 <= last_x;
+      for (int i = tid; i < ih * w; i += NT) {
+        const int r = i >> lw, c = i & (w - 1);
+        const T* src = ref + (size_t)clampi(y0 + r, 0, last_y) * rstride;
+        int32_t sum;
+        if (inside) {
+          const T* q = src + bx + c;
+          sum = f0 * (int32_t)q[0] + f1 * (int32_t)q[1] + f2 * (int32_t)q[2] + f3 * (int32_t)q[3] +
+                f4 * (int32_t)q[4] + f5 * (int32_t)q[5] + f6 * (int32_t)q[6] + f7 * (int32_t)q[7];
+        } else {
+          const int x = bx + c;
+          sum = f0 * (int32_t)src[clampi(x, 0, last_x)] + f1 * (int32_t)src[clampi(x + 1, 0, last_x)] +
+                f2 * (int32_t)src[clampi(x + 2, 0, last_x)] + f3 * (int32_t)src[clampi(x + 3, 0, last_x)] +
+                f4 * (int32_t)src[clampi(x + 4, 0, last_x)] + f5 * (int32_t)src[clampi(x + 5, 0, last_x)] +
+                f6 * (int32_t)src[clampi(x + 6, 0, last_x)] + f7 * (int32_t)src[clampi(x + 7, 0, last_x)];
+        }
+        tmp[r * tpitch + c] = (uint16_t)clampi((sum + 64) >> 7, 0, maxv);
+      }
+    } else {
+      for (int i = tid; i < ih * w; i += NT) {
+        const int r = i >> lw, c = i & (w - 1);
+        int ry = clampi(y0 + r, 0, last_y);
+        const T* src = ref + (size_t)ry * rstride;
+        int pos = p.start_x + p.step_x * c;
+        int base = (pos >> 4) - 3;
+        const int16_t* f = c_filters[filter][pos & 15];
+        int32_t sum = 0;
 #pragma unroll
-      for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)src[clampi(base + t, 0, last_x)];
-      tmp[r * tpitch + c] = (uint16_t)clampi((sum + 64) >> 7, 0, maxv);
+        for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)src[clampi(base + t, 0, last_x)];
+        tmp[r * tpitch + c] = (uint16_t)clampi((sum + 64) >> 7, 0, maxv);
+      }
     }
     sync();
+    // The vertical pass: unscaled, one phase and rows r..r+7 of tmp.
+    const bool vflat = p.step_y == 16;
+    const int16_t* fv = c_filters[filter][p.start_y & 15];
+    const int g0 = fv[0], g1 = fv[1], g2 = fv[2], g3 = fv[3], g4 = fv[4], g5 = fv[5], g6 = fv[6], g7 = fv[7];
     for (int i = tid; i < h * w; i += NT) {
-      int r = i / w, c = i - r * w;
-      int pos = (p.start_y & 15) + p.step_y * r;
-      int base = pos >> 4;
-      const int16_t* f = c_filters[filter][pos & 15];
-      int32_t sum = 0;
+      const int r = i >> lw, c = i & (w - 1);
+      int32_t sum;
+      if (vflat) {
+        const uint16_t* q = tmp + r * tpitch + c;
+        sum = g0 * (int32_t)q[0] + g1 * (int32_t)q[tpitch] + g2 * (int32_t)q[2 * tpitch] +
+              g3 * (int32_t)q[3 * tpitch] + g4 * (int32_t)q[4 * tpitch] + g5 * (int32_t)q[5 * tpitch] +
+              g6 * (int32_t)q[6 * tpitch] + g7 * (int32_t)q[7 * tpitch];
+      } else {
+        int pos = (p.start_y & 15) + p.step_y * r;
+        int base = pos >> 4;
+        const int16_t* f = c_filters[filter][pos & 15];
+        sum = 0;
 #pragma unroll
-      for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)tmp[(base + t) * tpitch + c];
+        for (int t = 0; t < 8; ++t) sum += f[t] * (int32_t)tmp[(base + t) * tpitch + c];
+      }
       int v = clampi((sum + 64) >> 7, 0, maxv);
       if (!compound)
         dst[(size_t)r * dstride + c] = (T)v;
