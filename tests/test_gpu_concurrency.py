@@ -181,3 +181,29 @@ def test_concurrent_autotune_keeps_results_exact():
         for d, s in zip(decs, seqs):
             s.free()
             d.close()
+
+
+def test_event_mask_brackets_only_the_chosen_kernels():
+    # rv9_decoder_set_event_mask: a per-kernel run with only the loop filter
+    # bracketed times only it, and the frames are the same either way.
+    import rv9
+    name = NAMES[0]
+    d = rv9.Decoder(0)
+    s = d.load_sequence(read_packets(os.path.join(VECTORS_DIR, name)))
+    try:
+        s.run(per_kernel=True)
+        want = _slots(d)
+        full = d.kernel_stats(reset=True)
+        assert all(v["launches"] > 0 for k, v in full.items() if k in ("k_lf", "k_prep"))
+        d.set_event_mask(["k_lf"])
+        s.run(per_kernel=True)
+        only = d.kernel_stats(reset=True)
+        assert only["k_lf"]["launches"] == full["k_lf"]["launches"] and only["k_lf"]["ms"] > 0
+        assert all(v["launches"] == 0 for k, v in only.items() if k != "k_lf")
+        assert _slots(d) == want
+        d.set_event_mask(None)
+        s.run(per_kernel=True)
+        assert d.kernel_stats(reset=True)["k_prep"]["launches"] == full["k_prep"]["launches"]
+    finally:
+        s.free()
+        d.close()
