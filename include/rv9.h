@@ -174,6 +174,18 @@ rv9_status rv9_sequence_run_noalloc(rv9_decoder* dec, rv9_sequence* seq, double*
  * stream's end. A multi-stream throughput form with no reference counterpart. */
 rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int flags,
                              double* device_ms);
+/* The same reconstruction with one launch per stage for all sequences' next
+ * frames: frame i of every sequence is in step i's launches (preparation,
+ * inter prediction, residuals, the intra wavefront, the loop-filter
+ * wavefront), 8-bit and deeper frames in separate launches. Each stage's
+ * kernel walks a work list drawn from all of the step's frames; the
+ * wavefront stages hand out each frame's rows from that frame's own tickets.
+ * The decoders are split round-robin into `groups` groups (1 up to n), each
+ * group's launches on its own CUDA stream, so that one group's loop filter
+ * can run beside another's prediction. Frames are bit-identical to
+ * rv9_sequences_run's. A multi-stream form with no reference counterpart. */
+rv9_status rv9_sequences_run_batched(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int groups,
+                                     double* device_ms);
 uint32_t rv9_sequence_frames(const rv9_sequence* seq);
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* seq);     /* visible luma of shown frames */
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* seq); /* per run */

@@ -286,6 +286,25 @@ rv9_status rv9_sequences_run(rv9_decoder* const* decs, rv9_sequence* const* seqs
   return (rv9_status)st;
 }
 
+rv9_status rv9_sequences_run_batched(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n, int groups,
+                                     double* device_ms) {
+  if (!device_ms || (n && (!decs || !seqs)) || groups < 1) return RV9_INVALID_INPUT;
+  *device_ms = 0;
+  std::vector<rv9g::Engine*> engines(n);
+  std::vector<const rv9g::Sequence*> ss(n);
+  for (size_t i = 0; i < n; ++i) {
+    if (!decs[i] || !seqs[i]) return RV9_INVALID_INPUT;
+    engines[i] = &decs[i]->engine;
+    ss[i] = &seqs[i]->seq;
+  }
+  float ms = 0;
+  std::string err;
+  rv9::Status st = rv9g::Engine::run_batched(engines.data(), ss.data(), n, groups, &ms, &err);
+  if (st != rv9::ST_OK && n) decs[0]->err = err;
+  *device_ms = ms;
+  return (rv9_status)st;
+}
+
 uint32_t rv9_sequence_frames(const rv9_sequence* s) { return (uint32_t)s->seq.frames.size(); }
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* s) { return s->seq.luma_samples; }
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* s) {

@@ -52,6 +52,8 @@ Engine::~Engine() {
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (stream_) cudaStreamDestroy(stream_);
+  cudaFree(batch_d_);
+  cudaFreeHost(batch_h_);
 }
 
 bool Engine::init(int device, std::string* err) {
@@ -387,12 +389,11 @@ void Engine::collect_kernel_events() {
   kev_used_ = 0;
 }
 
-rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
-                              std::string* err) {
-  *shown = nullptr;
+rv9::Status Engine::prepare_frame(const FrameWork& fw, const uint8_t* d_base, cudaStream_t stream, KFrame* kf,
+                                  DevFrame** out, std::string* err) {
+  *out = nullptr;
   if (fw.show_existing) {
-    *shown = slots_[fw.show_slot];
-    if (!*shown) {
+    if (!slots_[fw.show_slot]) {
       *err = "show_existing_frame of an empty slot";
       return rv9::ST_BITSTREAM;
     }
@@ -415,28 +416,28 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
     // Already checked against the array's size; zero the counters and the
     // done flags (flags then compare against epoch 1).
     size_t flags = align256((size_t)d.sb64_cols * d.sb64_rows * 4);
-    CK(cudaMemsetAsync(fixed_, 0, 256 + flags, stream_));
+    CK(cudaMemsetAsync(fixed_, 0, 256 + flags, stream));
   } else if (mi_len > lf_mi_cap_) {
-    CK(cudaStreamSynchronize(stream_));
+    CK(cudaStreamSynchronize(stream));
     cudaFree(d_lf_mi_);
     CK(cudaMalloc(&d_lf_mi_, mi_len * 4));
     lf_mi_cap_ = mi_len;
   }
   size_t n_sb = (size_t)d.sb64_cols * d.sb64_rows;
   if (!fixed_ && n_sb > sb_cap_) {
-    CK(cudaStreamSynchronize(stream_));
+    CK(cudaStreamSynchronize(stream));
     cudaFree(d_sb_done_);
     CK(cudaMalloc(&d_sb_done_, n_sb * 4));
-    CK(cudaMemsetAsync(d_sb_done_, 0, n_sb * 4, stream_));
+    CK(cudaMemsetAsync(d_sb_done_, 0, n_sb * 4, stream));
     sb_cap_ = n_sb;
   }
   // The loop filter's progress words carry the epoch's low 16 bits: clear
   // them when those wrap, so that no stale word can match.
   if (!fixed_ && ((++epoch_) & 0xffff) == 0) {
-    CK(cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream_));
+    CK(cudaMemsetAsync(d_sb_done_, 0, sb_cap_ * 4, stream));
     ++epoch_;
   }
-  KFrame k;
+  KFrame& k = *kf;
   memset(&k, 0, sizeof k);
   for (int p = 0; p < 3; ++p) {
     k.cur[p].data = cur->planes[p];
@@ -547,25 +548,17 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
     k.epoch = epoch_;
     k.counters = d_counters_;
     k.error = d_counters_ + 2;
-    CK(cudaMemsetAsync(d_counters_, 0, 8, stream_));
   }
-  int L = 0;
-  cur_fw_ = &fw;
-  TuneParams tune;
-  if (tune_override_) {
-    tune = *tune_override_;
-  } else {
-    auto it = tuned_.find(geometry_key(d));
-    if (it != tuned_.end()) tune = it->second;
+  *out = cur;
+  return rv9::ST_OK;
+}
+
+void Engine::commit_frame(const FrameWork& fw, DevFrame* cur, DevFrame** shown) {
+  *shown = nullptr;
+  if (fw.show_existing) {
+    *shown = slots_[fw.show_slot];
+    return;
   }
-  // Captured graphs keep every launch on the one stream: replays of graphs
-  // with the fork's branches measured slower than without them.
-  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this, tune,
-                  capturing_ ? nullptr : &aux_));
-  cur_fw_ = nullptr;
-  // The device's error word, read at the next sync.
-  CK(cudaMemcpyAsync(h_error_ + 1, k.error, 4, cudaMemcpyDeviceToHost, stream_));
-  launches += L;
   ++frames;
   alg_bytes += fw.total_bytes;
   // Reference update (8.10 step 1).
@@ -576,6 +569,38 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
       ++cur->refs;
     }
   if (fw.show_frame) *shown = cur;
+}
+
+rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
+                              std::string* err) {
+  *shown = nullptr;
+  KFrame k;
+  DevFrame* cur = nullptr;
+  rv9::Status st = prepare_frame(fw, d_base, stream_, &k, &cur, err);
+  if (st != rv9::ST_OK) return st;
+  if (!cur) {
+    commit_frame(fw, nullptr, shown);
+    return rv9::ST_OK;
+  }
+  if (!fixed_) CK(cudaMemsetAsync(d_counters_, 0, 8, stream_));
+  int L = 0;
+  cur_fw_ = &fw;
+  TuneParams tune;
+  if (tune_override_) {
+    tune = *tune_override_;
+  } else {
+    auto it = tuned_.find(geometry_key(fw.desc));
+    if (it != tuned_.end()) tune = it->second;
+  }
+  // Captured graphs keep every launch on the one stream: replays of graphs
+  // with the fork's branches measured slower than without them.
+  CK(launch_frame(k, (int)fw.n_blocks, stream_, n_sm_, &L, per_kernel ? &Engine::hook : nullptr, this, tune,
+                  capturing_ ? nullptr : &aux_));
+  cur_fw_ = nullptr;
+  // The device's error word, read at the next sync.
+  CK(cudaMemcpyAsync(h_error_ + 1, k.error, 4, cudaMemcpyDeviceToHost, stream_));
+  launches += L;
+  commit_frame(fw, cur, shown);
   return rv9::ST_OK;
 }
 
@@ -936,6 +961,150 @@ rv9::Status Engine::run_concurrent(Engine* const* engines, const Sequence* const
     engines[j]->device_ms += *ms / n;
     if (per_kernel) engines[j]->collect_kernel_events();
   }
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::reserve_scratch(const Sequence& seq, std::string* err) {
+  size_t mi = 0, sb = 0;
+  for (const FrameWork& fw : seq.frames)
+    if (!fw.show_existing) {
+      mi = std::max(mi, (size_t)fw.desc.mi_cols * fw.desc.mi_rows);
+      sb = std::max(sb, (size_t)fw.desc.sb64_cols * fw.desc.sb64_rows);
+    }
+  if (mi <= lf_mi_cap_ && sb <= sb_cap_) return rv9::ST_OK;
+  CK(cudaStreamSynchronize(stream_));
+  if (mi > lf_mi_cap_) {
+    cudaFree(d_lf_mi_);
+    d_lf_mi_ = nullptr;
+    lf_mi_cap_ = 0;
+    CK(cudaMalloc(&d_lf_mi_, mi * 4));
+    lf_mi_cap_ = mi;
+  }
+  if (sb > sb_cap_) {
+    cudaFree(d_sb_done_);
+    d_sb_done_ = nullptr;
+    sb_cap_ = 0;
+    CK(cudaMalloc(&d_sb_done_, sb * 4));
+    CK(cudaMemsetAsync(d_sb_done_, 0, sb * 4, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    sb_cap_ = sb;
+  }
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int groups,
+                                float* ms, std::string* err) {
+  *ms = 0;
+  if (n == 0) return rv9::ST_OK;
+  Engine* e0 = engines[0];
+  for (size_t j = 0; j < n; ++j) {
+    if (engines[j]->device_ != e0->device_) {
+      *err = "decoders on different devices";
+      return rv9::ST_INVALID_INPUT;
+    }
+    for (size_t i = 0; i < j; ++i)
+      if (engines[i] == engines[j]) {
+        *err = "a decoder appears twice";
+        return rv9::ST_INVALID_INPUT;
+      }
+  }
+  const size_t G = std::min<size_t>(std::max(groups, 1), n);
+  size_t most = 0;
+  for (size_t j = 0; j < n; ++j) {
+    rv9::Status st = engines[j]->reserve_scratch(*seqs[j], err);
+    if (st != rv9::ST_OK) return st;
+    CK(cudaStreamSynchronize(engines[j]->stream_));
+    engines[j]->reset_slots();
+    most = std::max(most, seqs[j]->frames.size());
+  }
+  // Every batch of the run has its own region of the tables, so that no
+  // copy waits for an earlier batch's launches.
+  auto batch_class = [](const FrameWork& fw) { return fw.desc.bit_depth > 8 ? 1 : 0; };
+  size_t total = 0;
+  for (size_t i = 0; i < most; ++i)
+    for (size_t g = 0; g < G; ++g) {
+      int cnt[2] = {0, 0};
+      for (size_t j = g; j < n; j += G)
+        if (i < seqs[j]->frames.size() && !seqs[j]->frames[i].show_existing) ++cnt[batch_class(seqs[j]->frames[i])];
+      for (int c = 0; c < 2; ++c)
+        if (cnt[c]) total += batch_table_bytes(cnt[c]);
+    }
+  if (total > e0->batch_cap_) {
+    cudaFree(e0->batch_d_);
+    cudaFreeHost(e0->batch_h_);
+    e0->batch_d_ = e0->batch_h_ = nullptr;
+    e0->batch_cap_ = 0;
+    CK(cudaMalloc(&e0->batch_d_, total));
+    CK(cudaMallocHost(&e0->batch_h_, total));
+    e0->batch_cap_ = total;
+  }
+  // Each group's stream starts after the start event on engines[0]'s.
+  CK(cudaEventRecord(e0->ev0_, e0->stream_));
+  for (size_t g = 1; g < G; ++g) CK(cudaStreamWaitEvent(engines[g]->stream_, e0->ev0_, 0));
+  std::vector<KFrame> ks;
+  std::vector<int> nb;
+  std::vector<DevFrame*> curs;
+  std::vector<size_t> who;
+  size_t off = 0;
+  int L = 0;
+  for (size_t i = 0; i < most; ++i)
+    for (size_t g = 0; g < G; ++g) {
+      cudaStream_t s = engines[g]->stream_;
+      for (int c = 0; c < 2; ++c) {
+        ks.clear();
+        nb.clear();
+        curs.clear();
+        who.clear();
+        for (size_t j = g; j < n; j += G) {
+          if (i >= seqs[j]->frames.size()) continue;
+          const FrameWork& fw = seqs[j]->frames[i];
+          if (fw.show_existing ? c != 0 : batch_class(fw) != c) continue;
+          KFrame k;
+          DevFrame* cur = nullptr;
+          rv9::Status st = engines[j]->prepare_frame(fw, seqs[j]->d_data, s, &k, &cur, err);
+          if (st != rv9::ST_OK) return st;
+          if (!cur) {
+            DevFrame* shown = nullptr;
+            engines[j]->commit_frame(fw, nullptr, &shown);
+            continue;
+          }
+          ks.push_back(k);
+          nb.push_back((int)fw.n_blocks);
+          curs.push_back(cur);
+          who.push_back(j);
+        }
+        if (ks.empty()) continue;
+        const int nf = (int)ks.size();
+        BatchTotals tot;
+        batch_fill(ks.data(), nb.data(), nf, e0->batch_h_ + off, &tot);
+        const size_t bytes = batch_table_bytes(nf);
+        CK(cudaMemcpyAsync(e0->batch_d_ + off, e0->batch_h_ + off, bytes, cudaMemcpyHostToDevice, s));
+        CK(launch_batch(e0->batch_d_ + off, nf, tot, c == 1, s, e0->n_sm_, TuneParams(), &L));
+        off += bytes;
+        for (int q = 0; q < nf; ++q) {
+          DevFrame* shown = nullptr;
+          engines[who[q]]->commit_frame(seqs[who[q]]->frames[i], curs[q], &shown);
+        }
+      }
+    }
+  // engines[0]'s stream waits for every group's end.
+  for (size_t g = 1; g < G; ++g) {
+    CK(cudaEventRecord(engines[g]->ev1_, engines[g]->stream_));
+    CK(cudaStreamWaitEvent(e0->stream_, engines[g]->ev1_, 0));
+  }
+  CK(cudaEventRecord(e0->ev1_, e0->stream_));
+  CK(cudaStreamSynchronize(e0->stream_));
+  e0->launches += L;
+  // Each decoder's error word (its frames' waits), as sync() reports it.
+  rv9::Status first = rv9::ST_OK;
+  for (size_t j = 0; j < n; ++j) {
+    CK(cudaMemcpy(engines[j]->h_error_ + 1, engines[j]->d_counters_ + 2, 4, cudaMemcpyDeviceToHost));
+    rv9::Status st = engines[j]->sync(err);
+    if (first == rv9::ST_OK) first = st;
+  }
+  if (first != rv9::ST_OK) return first;
+  CK(cudaEventElapsedTime(ms, e0->ev0_, e0->ev1_));
+  for (size_t j = 0; j < n; ++j) engines[j]->device_ms += *ms / n;
   return rv9::ST_OK;
 }
 

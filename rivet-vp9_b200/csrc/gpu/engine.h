@@ -40,6 +40,21 @@ cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm
                          void* hook_ctx, const TuneParams& tune = TuneParams(), const LaunchAux* aux = nullptr);
 cudaError_t upload_filters(const int16_t* f);
 
+// Batched launches: one launch per stage for frames of many streams (no
+// frame of a batch may depend on another), all 8-bit or all above 8 bits.
+// The batch's tables (the frames' KFrames, launch splits and CTA prefixes)
+// are filled on the host by batch_fill into batch_table_bytes(n) bytes,
+// copied to the device as they are, and launched from there.
+struct BatchTotals {
+  uint32_t ctas[4];     // preparation, small inter, large inter, residual
+  uint32_t intra_jobs;  // over all frames
+  uint32_t lf_rows;     // superblock rows of the frames with the loop filter on
+};
+size_t batch_table_bytes(int n);
+void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, BatchTotals* tot);
+cudaError_t launch_batch(const uint8_t* dev, int n, const BatchTotals& tot, bool high, cudaStream_t s, int n_sm,
+                         const TuneParams& tune, int* launches);
+
 // The fixed wavefront scratch: a static device array of this many bytes.
 // Layout: [0, 256) counters (the intra ticket, the loop-filter ticket, the
 // error word), then the superblock done flags (4 bytes each, 256-byte
@@ -143,6 +158,16 @@ class Engine {
   // completion, on engines[0]'s stream.
   static rv9::Status run_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
                                     bool per_kernel, float* ms, std::string* err, bool graphs = false);
+  // Reconstructs several sequences at once (one per engine, all distinct, on
+  // one device) with one launch per stage for the next frames of all of
+  // them: frame i of every sequence goes in step i's launches, those of
+  // 8-bit and of deeper sequences apart. The engines are split round-robin
+  // into `groups` groups, each group's launches on its own CUDA stream (the
+  // stream of its first engine), so that one group's loop filter can overlap
+  // another's prediction. *ms is the CUDA-event time from the first launch
+  // to the last completion.
+  static rv9::Status run_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int groups,
+                                 float* ms, std::string* err);
   // The autotuner for sequences reconstructed together: times run_concurrent
   // with each candidate shape applied to every engine, and gives each engine
   // the fastest for its sequence's geometries. Shapes that suit one stream
@@ -188,6 +213,16 @@ class Engine {
   bool build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageReserve& reserve);
   rv9::Status run_frame(const FrameWork& fw, const uint8_t* d_base, bool per_kernel, DevFrame** shown,
                         std::string* err);
+  // The host side of a frame's reconstruction: its frame from the pool, the
+  // scratch it uses (clears queued on `stream`) and the kernels' view of it
+  // in *k. *cur is null for a shown existing frame. commit_frame then
+  // updates the reference slots once the frame's launches are queued.
+  rv9::Status prepare_frame(const FrameWork& fw, const uint8_t* d_base, cudaStream_t stream, KFrame* k,
+                            DevFrame** cur, std::string* err);
+  void commit_frame(const FrameWork& fw, DevFrame* cur, DevFrame** shown);
+  // Loop-filter records and progress words for every frame of `seq`, so
+  // that no frame of a run reallocates them.
+  rv9::Status reserve_scratch(const Sequence& seq, std::string* err);
   void reset_slots();
   bool pool_covers(const Sequence& seq);
   static uint64_t geometry_key(const rv9_frame_desc& d) {
@@ -223,6 +258,10 @@ class Engine {
   uint32_t epoch_ = 0;
   uint8_t* fixed_ = nullptr;  // the fixed scratch, during sequence_run_fixed
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  // run_batched's tables (pinned host, device), on the first engine.
+  uint8_t* batch_h_ = nullptr;
+  uint8_t* batch_d_ = nullptr;
+  size_t batch_cap_ = 0;
   // Per-kernel timing.
   std::vector<cudaEvent_t> kev_;
   std::vector<int> kev_kernel_;

@@ -31,6 +31,7 @@
 // records an error code, sets the abort flag and returns.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <mutex>
 
@@ -115,8 +116,7 @@ struct PrepSplit {
 };
 
 template <class T>
-__global__ void __launch_bounds__(kPrepThreads) k_prep(KFrame k, PrepSplit ps) {
-  int b = blockIdx.x;
+__device__ __forceinline__ void prep_cta(const KFrame& k, const PrepSplit& ps, int b) {
   if (b < ps.zp) {
     zero_pad_part<T>(k, b / ps.zp_per_plane, b % ps.zp_per_plane, ps.zp_per_plane);
     return;
@@ -130,6 +130,11 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(KFrame k, PrepSplit ps) {
   b -= ps.lf;
   const int i = b * kPrepThreads + threadIdx.x;
   if (i < k.n_intra) intra_mark_item(k, i);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPrepThreads) k_prep(KFrame k, PrepSplit ps) {
+  prep_cta<T>(k, ps, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -303,11 +308,16 @@ __device__ __forceinline__ void inter_unit(const KFrame& k, const InterUnit& u, 
 // Regions larger than 16x16 (after the small ones in the list): one CTA of
 // NT threads each.
 template <class T, int NT>
-__global__ void __launch_bounds__(NT) k_inter(KFrame k) {
+__device__ __forceinline__ void inter_large_cta(const KFrame& k, int b) {
   __shared__ uint16_t tmp[kInterTmpRows * 64];
   __shared__ uint16_t pred[64 * 64];
-  const InterUnit u = k.units[k.n_units_small + blockIdx.x];
+  const InterUnit u = k.units[k.n_units_small + b];
   inter_unit<T, NT>(k, u, threadIdx.x, tmp, 64, pred, 64);
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_inter(KFrame k) {
+  inter_large_cta<T, NT>(k, blockIdx.x);
 }
 
 // Regions of at most 16x16 (the first n_units_small of the list): one warp
@@ -315,14 +325,19 @@ __global__ void __launch_bounds__(NT) k_inter(KFrame k) {
 // largest reference step (2:1).
 constexpr int kInterSmallRows = 38;
 template <class T>
-__global__ void __launch_bounds__(kInterThreads) k_inter_small(KFrame k) {
+__device__ __forceinline__ void inter_small_cta(const KFrame& k, int b) {
   __shared__ uint16_t tmp[kInterThreads / 32][kInterSmallRows * 16];
   __shared__ uint16_t pred[kInterThreads / 32][16 * 16];
   const int warp = threadIdx.x >> 5;
-  const int i = blockIdx.x * (kInterThreads / 32) + warp;
+  const int i = b * (kInterThreads / 32) + warp;
   if (i >= k.n_units_small) return;
   const InterUnit u = k.units[i];
   inter_unit<T, 32>(k, u, threadIdx.x & 31, tmp[warp], 16, pred[warp], 16);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kInterThreads) k_inter_small(KFrame k) {
+  inter_small_cta<T>(k, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -510,10 +525,10 @@ __device__ __forceinline__ void res_cta(const KFrame& k, int b, int first, int c
 }
 
 template <class T, class V>
-__global__ void __launch_bounds__(32 * kResWarps) k_inter_res(KFrame k, ResSplit sp) {
+__device__ __forceinline__ void inter_res_cta(const KFrame& k, const ResSplit& sp, int b) {
   // Per warp 32 (n0 + 1) words at most (one 32x32 block, or G smaller ones).
   __shared__ typename V::store_t sc[kResWarps * 32 * 33];
-  int b = blockIdx.x, first = 0;
+  int first = 0;
   if (b < sp.ctas[0]) return res_cta<T, V, 2>(k, b, first, sp.count[0], sc);
   b -= sp.ctas[0];
   first += sp.count[0];
@@ -524,6 +539,11 @@ __global__ void __launch_bounds__(32 * kResWarps) k_inter_res(KFrame k, ResSplit
   b -= sp.ctas[2];
   first += sp.count[2];
   res_cta<T, V, 5>(k, b, first, sp.count[3], sc);
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kResWarps) k_inter_res(KFrame k, ResSplit sp) {
+  inter_res_cta<T, V>(k, sp, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -539,21 +559,15 @@ struct IntraSmem {
   int32_t left[32];
 };
 
+// One intra job of frame `k` by one warp: a row of a block's transform
+// blocks of one plane, done in order, so that the links along the row cost
+// no ticket and no wait on another warp. False when a wait gave up (this
+// warp's or, through the frame's error word, another's).
 template <class T, class V>
-__global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  IntraSmem<V>* sm = reinterpret_cast<IntraSmem<V>*>(smem_raw) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ bool intra_job(const KFrame& k, int job, IntraSmem<V>* sm, int lane) {
   const int maxv = (1 << k.bit_depth) - 1;
   volatile int32_t* err = k.error;
-  for (;;) {
-    // One job per ticket: a row of a block's transform blocks of one plane,
-    // done in order by this warp, so that the links along the row cost no
-    // ticket and no wait on another warp.
-    int job = 0;
-    if (lane == 0) job = atomicAdd(&k.counters[0], 1);
-    job = __shfl_sync(0xffffffffu, job, 0);
-    if (job >= k.n_intra_jobs) return;
+  {
     const int idx_end = (int)k.intra_jobs[job + 1];
     for (int idx = (int)k.intra_jobs[job]; idx < idx_end; ++idx) {
     const IntraItem it = k.intra[idx];
@@ -600,10 +614,10 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
       for (;;) {
         bool pending = cell != nullptr && *cell != 0;
         if (!__any_sync(0xffffffffu, pending)) break;
-        if (__any_sync(0xffffffffu, *err != 0)) return;
+        if (__any_sync(0xffffffffu, *err != 0)) return false;
         if (++polls > kWaitLimit) {
           if (lane == 0) atomicCAS(k.error, 0, 1);
-          return;
+          return false;
         }
         __nanosleep(64);
       }
@@ -672,6 +686,22 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
     }
     __syncwarp();
     }
+  }
+  return true;
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  IntraSmem<V>* sm = reinterpret_cast<IntraSmem<V>*>(smem_raw) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    // One job per ticket.
+    int job = 0;
+    if (lane == 0) job = atomicAdd(&k.counters[0], 1);
+    job = __shfl_sync(0xffffffffu, job, 0);
+    if (job >= k.n_intra_jobs) return;
+    if (!intra_job<T, V>(k, job, sm, lane)) return;
   }
 }
 
@@ -872,6 +902,7 @@ struct LfRowSmem {
   uint32_t mi[2][64];
   uint8_t limit[64], blimit[64], thresh[64];
   int row;
+  int frame;  // batched launches: the frame of `row`, -1 when none is left
   int abort_flag;
 };
 
@@ -934,14 +965,17 @@ __device__ void lf_row_prepare(const KFrame& k, LfRowSmem& S, const LfParams& P,
   }
 }
 
+// Filters superblock row `sr` of frame `k` (the whole CTA), the row's
+// progress word already set to the epoch with no steps and S.abort_flag
+// clear. False when a wait gave up (this row's, or another's through the
+// frame's error word).
 template <class T>
-__global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
-  extern __shared__ __align__(16) unsigned char lf_raw[];
-  LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
+__device__ __forceinline__ bool lf_row(const KFrame& k, LfRowSmem& S, const int sr) {
   const int tid = threadIdx.x;
   const int bd = sizeof(T) == 1 ? 8 : k.bit_depth;  // a constant for 8-bit content
-  const int cols = k.sb64_cols, rows = k.sb64_rows;
+  const int cols = k.sb64_cols;
   const uint32_t ep = (uint32_t)(k.epoch & 0xffff) << 16;
+  // (The previous row's last barrier orders these stores after its reads.)
   for (int i = tid; i < 64; i += kLfRowThreads) {
     S.limit[i] = k.lf_limit[i];
     S.blimit[i] = k.lf_blimit[i];
@@ -954,17 +988,7 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
     W[p] = 64 >> (p ? k.ss_x : 0);
     Hh[p] = 64 >> (p ? k.ss_y : 0);
   }
-  for (;;) {
-    if (tid == 0) {
-      const int r = atomicAdd(&k.counters[1], 1);
-      S.row = r;
-      S.abort_flag = 0;
-      // This row's progress: kLfSteps per superblock (see below), from 0.
-      if (r < rows) *(volatile uint32_t*)&k.sb_done[r] = ep;
-    }
-    __syncthreads();
-    const int sr = S.row;
-    if (sr >= rows) return;
+  {
     uint32_t* const prog = k.sb_done + sr;
     lf_row_prepare<T>(k, S, P, sr, 0, 0, tid, kLfRowThreads, 0);
     __syncthreads();
@@ -1126,7 +1150,167 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
       }
     }
     __syncthreads();
-    if (S.abort_flag) return;
+  }
+  return !S.abort_flag;
+}
+
+// This row's progress: kLfSteps per superblock, from 0 (thread 0, when it
+// takes row r of frame k).
+__device__ __forceinline__ void lf_row_start(const KFrame& k, LfRowSmem& S, int r) {
+  S.row = r;
+  S.abort_flag = 0;
+  if (r < k.sb64_rows) *(volatile uint32_t*)&k.sb_done[r] = (uint32_t)(k.epoch & 0xffff) << 16;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
+  extern __shared__ __align__(16) unsigned char lf_raw[];
+  LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
+  for (;;) {
+    if (threadIdx.x == 0) lf_row_start(k, S, atomicAdd(&k.counters[1], 1));
+    __syncthreads();
+    const int sr = S.row;
+    if (sr >= k.sb64_rows) return;
+    if (!lf_row<T>(k, S, sr)) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched stages: one launch per stage for the next frames of many streams,
+// frames that do not depend on one another. The CTAs of a data-parallel stage
+// are split among the frames by a prefix of their per-frame grids. The two
+// wavefront stages hand out each frame's jobs (intra rows of transform
+// blocks, loop-filter superblock rows) from that frame's own tickets, in the
+// frame's order: a warp (a CTA for the loop filter) takes them from its home
+// frame and moves on to the next frame with tickets left when those are
+// gone. A job waits only for jobs of its own frame with earlier tickets,
+// all held by warps already running, so every wait ends. A job of a frame
+// whose wait gave up is abandoned quickly (the frame's error word is set)
+// and the warp goes on with the other frames.
+
+struct BatchArgs {
+  const KFrame* frames;
+  const PrepSplit* prep;
+  const ResSplit* res;
+  const uint32_t* base;  // [4][n + 1] CTA prefixes: preparation, small inter, large inter, residual
+  int n;
+};
+enum { kBasePrep = 0, kBaseSmall, kBaseLarge, kBaseRes };
+
+// The frame whose CTA range holds CTA b: the last f with base[f] <= b.
+__device__ __forceinline__ int batch_frame(const uint32_t* base, int n, uint32_t b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Warp-collective: a ticket of counter `which` (0 intra jobs, 1 loop-filter
+// rows) from the first frame at or after `home` (cyclically) that has any
+// left; returns that frame, or -1 when no frame has any.
+__device__ __forceinline__ int batch_take(const BatchArgs& a, int home, int which, int* ticket) {
+  const int lane = threadIdx.x & 31;
+  for (int s = 0; s < a.n; s += 32) {
+    int f = home + s + lane;
+    if (f >= a.n) f -= a.n;
+    const bool mine = s + lane < a.n;
+    int limit = 0;
+    if (mine) {
+      const KFrame& k = a.frames[f];
+      limit = which ? (k.lf_on ? k.sb64_rows : 0) : k.n_intra_jobs;
+    }
+    for (;;) {
+      const bool left = mine && *(volatile int32_t*)&a.frames[f].counters[which] < limit;
+      const unsigned m = __ballot_sync(0xffffffffu, left);
+      if (!m) break;  // none among these 32 frames
+      const int src = __ffs(m) - 1;
+      int t = 0;
+      if (lane == src) t = atomicAdd(&a.frames[f].counters[which], 1);
+      t = __shfl_sync(0xffffffffu, t, src);
+      const int lim = __shfl_sync(0xffffffffu, limit, src);
+      const int fr = __shfl_sync(0xffffffffu, f, src);
+      if (t < lim) {
+        *ticket = t;
+        return fr;
+      }
+      // Another warp took that frame's last ticket first: look again.
+    }
+  }
+  return -1;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kPrepThreads) k_prep_batch(BatchArgs a) {
+  // The frames' wavefront tickets start at zero; the later stages take them.
+  if (blockIdx.x == 0)
+    for (int f = threadIdx.x; f < a.n; f += kPrepThreads) {
+      a.frames[f].counters[0] = 0;
+      a.frames[f].counters[1] = 0;
+    }
+  const uint32_t* base = a.base + kBasePrep * (a.n + 1);
+  if (blockIdx.x >= base[a.n]) return;
+  const int f = batch_frame(base, a.n, blockIdx.x);
+  prep_cta<T>(a.frames[f], a.prep[f], blockIdx.x - base[f]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kInterThreads) k_inter_small_batch(BatchArgs a) {
+  const uint32_t* base = a.base + kBaseSmall * (a.n + 1);
+  const int f = batch_frame(base, a.n, blockIdx.x);
+  inter_small_cta<T>(a.frames[f], blockIdx.x - base[f]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kInterThreads) k_inter_batch(BatchArgs a) {
+  const uint32_t* base = a.base + kBaseLarge * (a.n + 1);
+  const int f = batch_frame(base, a.n, blockIdx.x);
+  inter_large_cta<T, kInterThreads>(a.frames[f], blockIdx.x - base[f]);
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kResWarps) k_inter_res_batch(BatchArgs a) {
+  const uint32_t* base = a.base + kBaseRes * (a.n + 1);
+  const int f = batch_frame(base, a.n, blockIdx.x);
+  inter_res_cta<T, V>(a.frames[f], a.res[f], blockIdx.x - base[f]);
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(32 * kIntraWarps) k_intra_batch(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  IntraSmem<V>* sm = reinterpret_cast<IntraSmem<V>*>(smem_raw) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const int home = (int)((blockIdx.x * kIntraWarps + (threadIdx.x >> 5)) % (unsigned)a.n);
+  for (;;) {
+    int job = 0;
+    const int f = batch_take(a, home, 0, &job);
+    if (f < 0) return;
+    intra_job<T, V>(a.frames[f], job, sm, lane);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kLfRowThreads) k_lf_rows_batch(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char lf_raw[];
+  LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
+  const int home = (int)(blockIdx.x % (unsigned)a.n);
+  for (;;) {
+    if (threadIdx.x < 32) {
+      int r = 0;
+      const int f = batch_take(a, home, 1, &r);
+      if (threadIdx.x == 0) {
+        S.frame = f;
+        if (f >= 0) lf_row_start(a.frames[f], S, r);
+      }
+    }
+    __syncthreads();
+    const int f = S.frame, sr = S.row;
+    if (f < 0) return;
+    lf_row<T>(a.frames[f], S, sr);
   }
 }
 
@@ -1134,6 +1318,137 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
 // Host-side launch of one frame's chain.
 
 cudaError_t upload_filters(const int16_t* f) { return cudaMemcpyToSymbol(c_filters, f, sizeof(int16_t) * 4 * 16 * 8); }
+
+// The preparation launch's parts for a frame of n_blocks blocks.
+static PrepSplit prep_split(const KFrame& k, int n_blocks) {
+  const int aw = k.sb64_cols * 64, ah = k.sb64_rows * 64;
+  PrepSplit ps;
+  ps.zp_per_plane = 64;
+  ps.zp = (k.mi_cols * 8 < aw || k.mi_rows * 8 < ah) ? 3 * ps.zp_per_plane : 0;
+  ps.n_blocks = (k.lf_on && n_blocks > 0) ? n_blocks : 0;
+  ps.lf = (ps.n_blocks + kPrepThreads - 1) / kPrepThreads;
+  ps.mark = (k.n_intra + kPrepThreads - 1) / kPrepThreads;
+  return ps;
+}
+
+// The residual launch's CTAs per transform size; *grid receives their sum.
+static ResSplit res_split(const KFrame& k, int* grid) {
+  ResSplit rs;
+  *grid = 0;
+  for (int z = 0; z < 4; ++z) {
+    const int per_cta = kResWarps * (32 >> (z + 2));
+    rs.count[z] = (int)k.n_res_by_size[z];
+    rs.ctas[z] = (rs.count[z] + per_cta - 1) / per_cta;
+    *grid += rs.ctas[z];
+  }
+  return rs;
+}
+
+// The batch tables in one buffer: the frames' KFrames, their launch splits
+// and the four CTA prefixes, each at a 16-byte boundary.
+struct BatchLayout {
+  size_t o_frames, o_prep, o_res, o_base, bytes;
+};
+static BatchLayout batch_layout(int n) {
+  auto up = [](size_t v) { return (v + 15) & ~(size_t)15; };
+  BatchLayout l;
+  l.o_frames = 0;
+  l.o_prep = up(l.o_frames + sizeof(KFrame) * n);
+  l.o_res = up(l.o_prep + sizeof(PrepSplit) * n);
+  l.o_base = up(l.o_res + sizeof(ResSplit) * n);
+  l.bytes = up(l.o_base + sizeof(uint32_t) * 4 * (n + 1));
+  return l;
+}
+
+size_t batch_table_bytes(int n) { return batch_layout(n).bytes; }
+
+void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, BatchTotals* tot) {
+  const BatchLayout l = batch_layout(n);
+  KFrame* fr = reinterpret_cast<KFrame*>(host + l.o_frames);
+  PrepSplit* pp = reinterpret_cast<PrepSplit*>(host + l.o_prep);
+  ResSplit* rr = reinterpret_cast<ResSplit*>(host + l.o_res);
+  uint32_t* base = reinterpret_cast<uint32_t*>(host + l.o_base);
+  memset(tot, 0, sizeof *tot);
+  for (int f = 0; f < n; ++f) {
+    const KFrame& k = ks[f];
+    fr[f] = k;
+    pp[f] = prep_split(k, n_blocks[f]);
+    int res_grid = 0;
+    rr[f] = res_split(k, &res_grid);
+    const uint32_t grids[4] = {(uint32_t)(pp[f].zp + pp[f].lf + pp[f].mark),
+                               (uint32_t)((k.n_units_small + kInterThreads / 32 - 1) / (kInterThreads / 32)),
+                               (uint32_t)(k.n_units - k.n_units_small), (uint32_t)res_grid};
+    for (int st = 0; st < 4; ++st) {
+      base[st * (n + 1) + f] = tot->ctas[st];
+      tot->ctas[st] += grids[st];
+    }
+    tot->intra_jobs += (uint32_t)k.n_intra_jobs;
+    tot->lf_rows += k.lf_on ? (uint32_t)k.sb64_rows : 0;
+  }
+  for (int st = 0; st < 4; ++st) base[st * (n + 1) + n] = tot->ctas[st];
+}
+
+template <class T, class V>
+static cudaError_t launch_batch_t(const uint8_t* dev, int n, const BatchTotals& tot, cudaStream_t s, int n_sm,
+                                  const TuneParams& tune, int* launches) {
+  const BatchLayout l = batch_layout(n);
+  BatchArgs a;
+  a.frames = reinterpret_cast<const KFrame*>(dev + l.o_frames);
+  a.prep = reinterpret_cast<const PrepSplit*>(dev + l.o_prep);
+  a.res = reinterpret_cast<const ResSplit*>(dev + l.o_res);
+  a.base = reinterpret_cast<const uint32_t*>(dev + l.o_base);
+  a.n = n;
+  int L = 0;
+  // The preparation launch always runs: its first CTA clears the tickets.
+  k_prep_batch<T><<<tot.ctas[kBasePrep] ? tot.ctas[kBasePrep] : 1, kPrepThreads, 0, s>>>(a);
+  ++L;
+  if (tot.ctas[kBaseSmall]) {
+    k_inter_small_batch<T><<<tot.ctas[kBaseSmall], kInterThreads, 0, s>>>(a);
+    ++L;
+  }
+  if (tot.ctas[kBaseLarge]) {
+    k_inter_batch<T><<<tot.ctas[kBaseLarge], kInterThreads, 0, s>>>(a);
+    ++L;
+  }
+  if (tot.ctas[kBaseRes]) {
+    k_inter_res_batch<T, V><<<tot.ctas[kBaseRes], 32 * kResWarps, 0, s>>>(a);
+    ++L;
+  }
+  if (tot.intra_jobs) {
+    const size_t smem = sizeof(IntraSmem<V>) * kIntraWarps;
+    static bool attr_set = false;
+    if (!attr_set) {
+      cudaFuncSetAttribute(k_intra_batch<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr_set = true;
+    }
+    const int want = (int)((tot.intra_jobs + kIntraWarps - 1) / kIntraWarps);
+    const int cap = (n_sm * tune.intra_ctas_per_sm_x4 + 3) / 4;
+    k_intra_batch<T, V><<<want < cap ? want : cap, 32 * kIntraWarps, smem, s>>>(a);
+    ++L;
+  }
+  if (tot.lf_rows) {
+    // As many row CTAs as fit on the device at once (more would only wait).
+    static int per_sm = 0;
+    if (!per_sm) {
+      cudaFuncSetAttribute(k_lf_rows_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LfRowSmem));
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lf_rows_batch<T>, kLfRowThreads,
+                                                        sizeof(LfRowSmem)) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+    }
+    const int cap = n_sm * per_sm;
+    k_lf_rows_batch<T><<<(int)tot.lf_rows < cap ? (int)tot.lf_rows : cap, kLfRowThreads, sizeof(LfRowSmem), s>>>(a);
+    ++L;
+  }
+  *launches += L;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const uint8_t* dev, int n, const BatchTotals& tot, bool high, cudaStream_t s, int n_sm,
+                         const TuneParams& tune, int* launches) {
+  if (high) return launch_batch_t<uint16_t, L64>(dev, n, tot, s, n_sm, tune, launches);
+  return launch_batch_t<uint8_t, L32>(dev, n, tot, s, n_sm, tune, launches);
+}
 
 template <class T, class V>
 static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches,
@@ -1143,13 +1458,7 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
     if (hook) hook(hctx, id, phase);
   };
   {
-    const int aw = k.sb64_cols * 64, ah = k.sb64_rows * 64;
-    PrepSplit ps;
-    ps.zp_per_plane = 64;
-    ps.zp = (k.mi_cols * 8 < aw || k.mi_rows * 8 < ah) ? 3 * ps.zp_per_plane : 0;
-    ps.n_blocks = (k.lf_on && n_blocks > 0) ? n_blocks : 0;
-    ps.lf = (ps.n_blocks + kPrepThreads - 1) / kPrepThreads;
-    ps.mark = (k.n_intra + kPrepThreads - 1) / kPrepThreads;
+    const PrepSplit ps = prep_split(k, n_blocks);
     const int grid = ps.zp + ps.lf + ps.mark;
     if (grid > 0) {
       mark(K_PREP, 0);
@@ -1191,14 +1500,8 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
   }
   if (k.n_res > 0) {
     mark(K_INTER_RES, 0);
-    ResSplit rs;
     int grid = 0;
-    for (int z = 0; z < 4; ++z) {
-      const int per_cta = kResWarps * (32 >> (z + 2));
-      rs.count[z] = (int)k.n_res_by_size[z];
-      rs.ctas[z] = (rs.count[z] + per_cta - 1) / per_cta;
-      grid += rs.ctas[z];
-    }
+    const ResSplit rs = res_split(k, &grid);
     k_inter_res<T, V><<<grid, 32 * kResWarps, 0, s>>>(k, rs);
     ++L;
     mark(K_INTER_RES, 1);

@@ -72,7 +72,7 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
-           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_decoder_autotune",
+           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_sequences_run_batched", "rv9_decoder_autotune",
            "rv9_sequences_autotune", "rv9_decoder_set_event_mask")
 
 
@@ -127,6 +127,8 @@ def load_library(path=None):
                                            ctypes.POINTER(CTuneResult)]
     lib.rv9_sequences_run.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_double)]
+    lib.rv9_sequences_run_batched.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t,
+                                              ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
         getattr(lib, name).restype = ctypes.c_uint64
         getattr(lib, name).argtypes = [vp]
@@ -218,6 +220,24 @@ def run_concurrent(pairs, per_kernel=False, graph=False):
     ms = ctypes.c_double()
     flags = (RV9_RUN_PER_KERNEL if per_kernel else 0) | (RV9_RUN_GRAPH if graph else 0)
     st = lib.rv9_sequences_run(decs, seqs, n, flags, ctypes.byref(ms))
+    if st != RV9_OK:
+        _raise(lib, pairs[0][0]._dec, st)
+    return ms.value
+
+
+def run_batched(pairs, groups=1):
+    """Reconstructs several (decoder, sequence) pairs with one launch per stage
+    for all sequences' next frames (rv9_sequences_run_batched), the decoders
+    split into `groups` groups on their own CUDA streams; returns the
+    CUDA-event milliseconds of the run."""
+    if not pairs:
+        return 0.0
+    lib = pairs[0][0]._lib
+    n = len(pairs)
+    decs = (ctypes.c_void_p * n)(*[d._dec for d, _ in pairs])
+    seqs = (ctypes.c_void_p * n)(*[s._h for _, s in pairs])
+    ms = ctypes.c_double()
+    st = lib.rv9_sequences_run_batched(decs, seqs, n, int(groups), ctypes.byref(ms))
     if st != RV9_OK:
         _raise(lib, pairs[0][0]._dec, st)
     return ms.value
