@@ -1049,8 +1049,9 @@ __device__ __forceinline__ bool lf_row(const KFrame& k, LfRowSmem& S, const int 
           }
         }
         named_sync(kBarFilter, kLfFilterThreads);
-        // Wait for the row above: superblock c's bottom strip final there.
-        if (live && sr > 0 && tf == 0) {
+        // Wait for the row above: superblock c's bottom strip final there
+        // (already seen, by an acquiring load, when the strip came early).
+        if (live && sr > 0 && tf == 0 && !top_early) {
           const volatile uint32_t* above = k.sb_done + (sr - 1);
           int polls = 0;
           for (;;) {
