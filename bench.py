@@ -269,15 +269,16 @@ def run_batched(local, dev, n_streams=64, frames=60):
     torch.cuda.synchronize(dev)
     ms_batched_graph = min(rv9.run_concurrent(pairs, graph=True) for _ in range(2))
     # One launch per stage for all streams' next frames, the streams split
-    # into G groups on their own CUDA streams.
-    staged = {}
-    for g in (1, 2, 4, 8):
-        rv9.run_batched(pairs, groups=g)
-        flush.zero_()
-        torch.cuda.synchronize(dev)
-        ms_g = min(rv9.run_batched(pairs, groups=g) for _ in range(2))
-        staged[str(g)] = {"value": round(luma / (ms_g / 1e3) / 1e6, 2), "ms": round(ms_g, 3),
-                          "speedup_vs_plain": round(ms_plain / ms_g, 2)}
+    # into G groups on their own CUDA streams; G and the intra grain by the
+    # batched autotuner (untimed here).
+    staged_tune = rv9.autotune_batched(pairs)
+    g = staged_tune["groups"]
+    flush.zero_()
+    torch.cuda.synchronize(dev)
+    ms_g = min(rv9.run_batched(pairs, groups=g) for _ in range(2))
+    staged = {"value": round(luma / (ms_g / 1e3) / 1e6, 2), "ms": round(ms_g, 3),
+              "speedup_vs_plain": round(ms_plain / ms_g, 2),
+              "autotune": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in staged_tune.items()}}
     out = {
         "workload": f"{n_streams} streams over 8 generated contents {{320x240, 640x360, 1280x720, 1920x1080}} x "
                     f"{{8, 10}}-bit 4:2:0, q per content in [35, 85], {CLASS_FRAMES} frames looped to {frames}",
@@ -289,7 +290,7 @@ def run_batched(local, dev, n_streams=64, frames=60):
         "graph_replay": {"value": round(luma / (ms_batched_graph / 1e3) / 1e6, 2),
                          "speedup_vs_plain": round(ms_plain / ms_batched_graph, 2),
                          "ms": round(ms_batched_graph, 3)},
-        "stage_batched": {"groups": staged,
+        "stage_batched": {**staged,
                           "how": "rv9_sequences_run_batched: one launch per stage for all 64 streams' next frames, "
                                  "the streams split round-robin into G groups, each on its own CUDA stream"},
         "how": "rv9_sequences_run over 64 decoders (own CUDA stream and slots each) vs rv9_sequence_run one by one",

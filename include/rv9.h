@@ -219,6 +219,13 @@ rv9_status rv9_decoder_autotune(rv9_decoder* dec, rv9_sequence* seq, rv9_tune_re
  * batch's; graphs captured before tuning keep their old shapes. */
 rv9_status rv9_sequences_autotune(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n,
                                   rv9_tune_result* out);
+/* The autotuner for rv9_sequences_run_batched: times the batch with 1, 2, 4
+ * and 8 groups (at most n) under each intra wavefront grain, keeps the
+ * fastest grain on decs[0] (used by batched runs whose first decoder it is)
+ * and returns it in *out with the fastest number of groups in *groups.
+ * out->default_ms is one group with the default grain. */
+rv9_status rv9_sequences_autotune_batched(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n,
+                                          int32_t* groups, rv9_tune_result* out);
 
 /* The frame in reference slot `slot` (0..7), packed like rv9_frame data. */
 rv9_status rv9_decoder_download_slot(rv9_decoder* dec, int slot, uint8_t* out, size_t cap, size_t* bytes);

@@ -305,6 +305,32 @@ rv9_status rv9_sequences_run_batched(rv9_decoder* const* decs, rv9_sequence* con
   return (rv9_status)st;
 }
 
+rv9_status rv9_sequences_autotune_batched(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n,
+                                          int32_t* groups, rv9_tune_result* out) {
+  if (!out || !groups || (n && (!decs || !seqs))) return RV9_INVALID_INPUT;
+  std::vector<rv9g::Engine*> engines(n);
+  std::vector<const rv9g::Sequence*> ss(n);
+  for (size_t i = 0; i < n; ++i) {
+    if (!decs[i] || !seqs[i]) return RV9_INVALID_INPUT;
+    engines[i] = &decs[i]->engine;
+    ss[i] = &seqs[i]->seq;
+  }
+  rv9g::TuneParams best;
+  float best_ms = 0, default_ms = 0;
+  int g = 1;
+  std::string err;
+  rv9::Status st =
+      rv9g::Engine::autotune_batched(engines.data(), ss.data(), n, &g, &best, &best_ms, &default_ms, &err);
+  if (st != rv9::ST_OK && n) decs[0]->err = err;
+  *groups = g;
+  out->intra_ctas_per_sm_x4 = best.intra_ctas_per_sm_x4;
+  out->inter_threads = best.inter_threads;
+  out->best_ms = best_ms;
+  out->default_ms = default_ms;
+  out->inter_fork = best.inter_fork ? 1 : 0;
+  return (rv9_status)st;
+}
+
 uint32_t rv9_sequence_frames(const rv9_sequence* s) { return (uint32_t)s->seq.frames.size(); }
 uint64_t rv9_sequence_luma_samples(const rv9_sequence* s) { return s->seq.luma_samples; }
 uint64_t rv9_sequence_algorithmic_bytes(const rv9_sequence* s) {

@@ -1079,7 +1079,7 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
         batch_fill(ks.data(), nb.data(), nf, e0->batch_h_ + off, &tot);
         const size_t bytes = batch_table_bytes(nf);
         CK(cudaMemcpyAsync(e0->batch_d_ + off, e0->batch_h_ + off, bytes, cudaMemcpyHostToDevice, s));
-        CK(launch_batch(e0->batch_d_ + off, nf, tot, c == 1, s, e0->n_sm_, TuneParams(), &L));
+        CK(launch_batch(e0->batch_d_ + off, nf, tot, c == 1, s, e0->n_sm_, e0->batch_tune_, &L));
         off += bytes;
         for (int q = 0; q < nf; ++q) {
           DevFrame* shown = nullptr;
@@ -1105,6 +1105,51 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
   if (first != rv9::ST_OK) return first;
   CK(cudaEventElapsedTime(ms, e0->ev0_, e0->ev1_));
   for (size_t j = 0; j < n; ++j) engines[j]->device_ms += *ms / n;
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::autotune_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int* groups,
+                                    TuneParams* best, float* best_ms, float* default_ms, std::string* err) {
+  *groups = 1;
+  *best = TuneParams();
+  *best_ms = *default_ms = 0;
+  if (n == 0) return rv9::ST_OK;
+  Engine* e0 = engines[0];
+  // The batch's time with given shapes: the better of two runs after one
+  // untimed run.
+  auto time_with = [&](int g, const TuneParams& tp, float* out) -> rv9::Status {
+    e0->batch_tune_ = tp;
+    float ms = 0, bestr = 0;
+    rv9::Status st = rv9::ST_OK;
+    for (int r = 0; r < 3 && st == rv9::ST_OK; ++r) {
+      st = run_batched(engines, seqs, n, g, &ms, err);
+      if (r == 1 || (r > 1 && ms < bestr)) bestr = ms;
+    }
+    *out = bestr;
+    return st;
+  };
+  rv9::Status st = time_with(1, TuneParams(), default_ms);
+  if (st != rv9::ST_OK) return st;
+  *best_ms = *default_ms;
+  const int group_counts[] = {1, 2, 4, 8};
+  const int grains[] = {2, 4, 8};
+  for (int g : group_counts) {
+    if ((size_t)g > n) break;
+    for (int gr : grains) {
+      if (g == 1 && gr == TuneParams().intra_ctas_per_sm_x4) continue;  // the defaults, timed above
+      TuneParams tp;
+      tp.intra_ctas_per_sm_x4 = gr;
+      float ms = 0;
+      st = time_with(g, tp, &ms);
+      if (st != rv9::ST_OK) return st;
+      if (ms < *best_ms) {
+        *best_ms = ms;
+        *best = tp;
+        *groups = g;
+      }
+    }
+  }
+  e0->batch_tune_ = *best;
   return rv9::ST_OK;
 }
 

@@ -168,6 +168,12 @@ class Engine {
   // to the last completion.
   static rv9::Status run_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int groups,
                                  float* ms, std::string* err);
+  // The autotuner for run_batched: times the batch with each number of
+  // groups (1, 2, 4, 8, at most n) and each intra wavefront grain, and keeps
+  // the fastest grain on engines[0], which run_batched then uses for batches
+  // led by it. *groups receives the fastest number of groups.
+  static rv9::Status autotune_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int* groups,
+                                      TuneParams* best, float* best_ms, float* default_ms, std::string* err);
   // The autotuner for sequences reconstructed together: times run_concurrent
   // with each candidate shape applied to every engine, and gives each engine
   // the fastest for its sequence's geometries. Shapes that suit one stream
@@ -258,7 +264,9 @@ class Engine {
   uint32_t epoch_ = 0;
   uint8_t* fixed_ = nullptr;  // the fixed scratch, during sequence_run_fixed
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
-  // run_batched's tables (pinned host, device), on the first engine.
+  // run_batched's launch shapes and tables (pinned host, device), on the
+  // first engine of the batch.
+  TuneParams batch_tune_;
   uint8_t* batch_h_ = nullptr;
   uint8_t* batch_d_ = nullptr;
   size_t batch_cap_ = 0;

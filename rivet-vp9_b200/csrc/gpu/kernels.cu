@@ -1193,10 +1193,14 @@ struct BatchArgs {
   const KFrame* frames;
   const PrepSplit* prep;
   const ResSplit* res;
-  const uint32_t* base;  // [4][n + 1] CTA prefixes: preparation, small inter, large inter, residual
+  // [6][n + 1] prefixes over the frames: the CTAs of the preparation, small
+  // inter, large inter and residual launches, then the intra jobs and the
+  // loop-filter rows (which place the wavefront stages' home frames).
+  const uint32_t* base;
   int n;
 };
-enum { kBasePrep = 0, kBaseSmall, kBaseLarge, kBaseRes };
+enum { kBasePrep = 0, kBaseSmall, kBaseLarge, kBaseRes, kBaseIntraJobs, kBaseLfRows, kBases };
+
 
 // The frame whose CTA range holds CTA b: the last f with base[f] <= b.
 __device__ __forceinline__ int batch_frame(const uint32_t* base, int n, uint32_t b) {
@@ -1209,6 +1213,12 @@ __device__ __forceinline__ int batch_frame(const uint32_t* base, int n, uint32_t
       hi = mid - 1;
   }
   return lo;
+}
+
+// The home frame of worker w of `workers`: workers are spread over the
+// frames in proportion to their share of the work prefix `base`.
+__device__ __forceinline__ int batch_home(const uint32_t* base, int n, uint32_t w, uint32_t workers) {
+  return batch_frame(base, n, (uint32_t)(((uint64_t)w * base[n]) / workers));
 }
 
 // Warp-collective: a ticket of counter `which` (0 intra jobs, 1 loop-filter
@@ -1285,7 +1295,8 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra_batch(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   IntraSmem<V>* sm = reinterpret_cast<IntraSmem<V>*>(smem_raw) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  const int home = (int)((blockIdx.x * kIntraWarps + (threadIdx.x >> 5)) % (unsigned)a.n);
+  const int home = batch_home(a.base + kBaseIntraJobs * (a.n + 1), a.n, blockIdx.x * kIntraWarps + (threadIdx.x >> 5),
+                              gridDim.x * kIntraWarps);
   for (;;) {
     int job = 0;
     const int f = batch_take(a, home, 0, &job);
@@ -1298,7 +1309,7 @@ template <class T>
 __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows_batch(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char lf_raw[];
   LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
-  const int home = (int)(blockIdx.x % (unsigned)a.n);
+  const int home = batch_home(a.base + kBaseLfRows * (a.n + 1), a.n, blockIdx.x, gridDim.x);
   for (;;) {
     if (threadIdx.x < 32) {
       int r = 0;
@@ -1357,7 +1368,7 @@ static BatchLayout batch_layout(int n) {
   l.o_prep = up(l.o_frames + sizeof(KFrame) * n);
   l.o_res = up(l.o_prep + sizeof(PrepSplit) * n);
   l.o_base = up(l.o_res + sizeof(ResSplit) * n);
-  l.bytes = up(l.o_base + sizeof(uint32_t) * 4 * (n + 1));
+  l.bytes = up(l.o_base + sizeof(uint32_t) * kBases * (n + 1));
   return l;
 }
 
@@ -1383,10 +1394,14 @@ void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, Bat
       base[st * (n + 1) + f] = tot->ctas[st];
       tot->ctas[st] += grids[st];
     }
+    base[kBaseIntraJobs * (n + 1) + f] = tot->intra_jobs;
+    base[kBaseLfRows * (n + 1) + f] = tot->lf_rows;
     tot->intra_jobs += (uint32_t)k.n_intra_jobs;
     tot->lf_rows += k.lf_on ? (uint32_t)k.sb64_rows : 0;
   }
   for (int st = 0; st < 4; ++st) base[st * (n + 1) + n] = tot->ctas[st];
+  base[kBaseIntraJobs * (n + 1) + n] = tot->intra_jobs;
+  base[kBaseLfRows * (n + 1) + n] = tot->lf_rows;
 }
 
 template <class T, class V>

@@ -72,7 +72,7 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_decode", "rv9_frame_release", "rv9_decode_packets", "rv9_decoder_stats", "rv9_sequence_load",
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
-           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_sequences_run_batched", "rv9_decoder_autotune",
+           "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_sequences_run_batched", "rv9_sequences_autotune_batched", "rv9_decoder_autotune",
            "rv9_sequences_autotune", "rv9_decoder_set_event_mask")
 
 
@@ -129,6 +129,8 @@ def load_library(path=None):
                                       ctypes.POINTER(ctypes.c_double)]
     lib.rv9_sequences_run_batched.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t,
                                               ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.rv9_sequences_autotune_batched.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_size_t,
+                                                   ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(CTuneResult)]
     for name in ("rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes", "rv9_sequence_record_bytes"):
         getattr(lib, name).restype = ctypes.c_uint64
         getattr(lib, name).argtypes = [vp]
@@ -241,6 +243,23 @@ def run_batched(pairs, groups=1):
     if st != RV9_OK:
         _raise(lib, pairs[0][0]._dec, st)
     return ms.value
+
+
+def autotune_batched(pairs):
+    """The autotuner for run_batched (rv9_sequences_autotune_batched): the
+    fastest number of groups and intra grain for these pairs; the grain is
+    kept on the first decoder."""
+    lib = pairs[0][0]._lib
+    n = len(pairs)
+    decs = (ctypes.c_void_p * n)(*[d._dec for d, _ in pairs])
+    seqs = (ctypes.c_void_p * n)(*[s._h for _, s in pairs])
+    groups = ctypes.c_int32()
+    r = CTuneResult()
+    st = lib.rv9_sequences_autotune_batched(decs, seqs, n, ctypes.byref(groups), ctypes.byref(r))
+    if st != RV9_OK:
+        _raise(lib, pairs[0][0]._dec, st)
+    return {"groups": groups.value, "intra_ctas_per_sm_x4": r.intra_ctas_per_sm_x4, "best_ms": r.best_ms,
+            "default_ms": r.default_ms}
 
 
 class Plane:

@@ -110,3 +110,23 @@ def test_batched_rejects_bad_calls():
         s1.free()
         s2.free()
         d.close()
+
+
+def test_batched_autotune_keeps_results_exact():
+    import rv9
+    decs, seqs = _load(NAMES[:5])
+    try:
+        alone = []
+        for d, s in zip(decs, seqs):
+            s.run()
+            alone.append(_slots(d))
+        pairs = list(zip(decs, seqs))
+        tuned = rv9.autotune_batched(pairs)
+        assert 1 <= tuned["groups"] <= len(pairs)
+        assert tuned["intra_ctas_per_sm_x4"] in (2, 4, 8)
+        assert 0 < tuned["best_ms"] <= tuned["default_ms"]
+        rv9.run_batched(pairs, groups=tuned["groups"])
+        for d, want in zip(decs, alone):
+            assert _slots(d) == want
+    finally:
+        _close(decs, seqs)
