@@ -29,6 +29,17 @@ const char* const kKernelNames[K_COUNT] = {"k_prep", "k_inter", "k_inter_res", "
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Waits, when it goes out of scope, for the streams of engines[0..n): a run
+// over several engines' streams that returns early (an error part-way
+// through) leaves none of its launches running behind it.
+struct StreamsDrain {
+  Engine* const* engines;
+  size_t n;
+  ~StreamsDrain() {
+    for (size_t j = 0; j < n; ++j) cudaStreamSynchronize(engines[j]->stream());
+  }
+};
+
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (DevFrame* f : pool_) {
@@ -918,6 +929,7 @@ rv9::Status Engine::run_concurrent(Engine* const* engines, const Sequence* const
       rv9::Status st = engines[j]->sequence_graph(*seqs[j], err);
       if (st != rv9::ST_OK) return st;
     }
+  StreamsDrain drain{engines, n};
   // Every stream starts after the start event on engines[0]'s stream.
   CK(cudaEventRecord(e0->ev0_, e0->stream_));
   for (size_t j = 0; j < n; ++j) {
@@ -1038,6 +1050,7 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
     CK(cudaMallocHost(&e0->batch_h_, total));
     e0->batch_cap_ = total;
   }
+  StreamsDrain drain{engines, G};
   // Each group's stream starts after the start event on engines[0]'s.
   CK(cudaEventRecord(e0->ev0_, e0->stream_));
   for (size_t g = 1; g < G; ++g) CK(cudaStreamWaitEvent(engines[g]->stream_, e0->ev0_, 0));
