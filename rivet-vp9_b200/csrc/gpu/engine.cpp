@@ -1089,7 +1089,7 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
         if (ks.empty()) continue;
         const int nf = (int)ks.size();
         BatchTotals tot;
-        batch_fill(ks.data(), nb.data(), nf, e0->batch_h_ + off, &tot);
+        batch_fill(ks.data(), nb.data(), nf, e0->batch_h_ + off, &tot, e0->n_sm_, e0->batch_tune_);
         const size_t bytes = batch_table_bytes(nf);
         CK(cudaMemcpyAsync(e0->batch_d_ + off, e0->batch_h_ + off, bytes, cudaMemcpyHostToDevice, s));
         CK(launch_batch(e0->batch_d_ + off, nf, tot, c == 1, s, e0->n_sm_, e0->batch_tune_, &L));

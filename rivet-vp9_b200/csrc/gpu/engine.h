@@ -48,10 +48,12 @@ cudaError_t upload_filters(const int16_t* f);
 struct BatchTotals {
   uint32_t ctas[4];     // preparation, small inter, large inter, residual
   uint32_t intra_jobs;  // over all frames
+  uint32_t intra_ctas;  // the intra wavefront CTAs the frames would take each alone (with `tune`)
   uint32_t lf_rows;     // superblock rows of the frames with the loop filter on
 };
 size_t batch_table_bytes(int n);
-void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, BatchTotals* tot);
+void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, BatchTotals* tot, int n_sm,
+                const TuneParams& tune);
 cudaError_t launch_batch(const uint8_t* dev, int n, const BatchTotals& tot, bool high, cudaStream_t s, int n_sm,
                          const TuneParams& tune, int* launches);
 

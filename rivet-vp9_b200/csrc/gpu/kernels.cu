@@ -33,6 +33,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "dsp_math.cuh"
@@ -1374,7 +1375,9 @@ static BatchLayout batch_layout(int n) {
 
 size_t batch_table_bytes(int n) { return batch_layout(n).bytes; }
 
-void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, BatchTotals* tot) {
+void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, BatchTotals* tot, int n_sm,
+                const TuneParams& tune) {
+  const uint32_t intra_cap = (uint32_t)((n_sm * tune.intra_ctas_per_sm_x4 + 3) / 4);
   const BatchLayout l = batch_layout(n);
   KFrame* fr = reinterpret_cast<KFrame*>(host + l.o_frames);
   PrepSplit* pp = reinterpret_cast<PrepSplit*>(host + l.o_prep);
@@ -1397,6 +1400,7 @@ void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, Bat
     base[kBaseIntraJobs * (n + 1) + f] = tot->intra_jobs;
     base[kBaseLfRows * (n + 1) + f] = tot->lf_rows;
     tot->intra_jobs += (uint32_t)k.n_intra_jobs;
+    tot->intra_ctas += std::min<uint32_t>(((uint32_t)k.n_intra_jobs + kIntraWarps - 1) / kIntraWarps, intra_cap);
     tot->lf_rows += k.lf_on ? (uint32_t)k.sb64_rows : 0;
   }
   for (int st = 0; st < 4; ++st) base[st * (n + 1) + n] = tot->ctas[st];
@@ -1431,15 +1435,20 @@ static cudaError_t launch_batch_t(const uint8_t* dev, int n, const BatchTotals& 
     ++L;
   }
   if (tot.intra_jobs) {
+    // As many CTAs as the frames would take on their own streams (a wide
+    // keyframe wavefront needs its warps whatever else is in the batch), up
+    // to what fits on the device at once.
     const size_t smem = sizeof(IntraSmem<V>) * kIntraWarps;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static int per_sm = 0;
+    if (!per_sm) {
       cudaFuncSetAttribute(k_intra_batch<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_set = true;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_intra_batch<T, V>, 32 * kIntraWarps, smem) !=
+              cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
     }
-    const int want = (int)((tot.intra_jobs + kIntraWarps - 1) / kIntraWarps);
-    const int cap = (n_sm * tune.intra_ctas_per_sm_x4 + 3) / 4;
-    k_intra_batch<T, V><<<want < cap ? want : cap, 32 * kIntraWarps, smem, s>>>(a);
+    const int grid = (int)std::min<uint32_t>(tot.intra_ctas, (uint32_t)(n_sm * per_sm));
+    k_intra_batch<T, V><<<grid > 0 ? grid : 1, 32 * kIntraWarps, smem, s>>>(a);
     ++L;
   }
   if (tot.lf_rows) {
