@@ -83,8 +83,28 @@ void rv9_decoder_set_threads(rv9_decoder* dec, uint32_t threads);
  * parse (adapted contexts, previous motion vectors) still wait for it; key
  * and error-resilient frames do not. Results are identical either way. */
 void rv9_decoder_set_parse_depth(rv9_decoder* dec, uint32_t frames);
+/* The number of host threads parsing uses (replaces Decoder::threads,
+ * src/decoder/mod.rs:179-181): the set_threads value, or the core count when
+ * it is 0. */
+uint32_t rv9_decoder_threads(const rv9_decoder* dec);
 /* Frames of more than `pixels` luma samples are refused (RV9_UNSUPPORTED). */
 void rv9_decoder_set_max_pixels(rv9_decoder* dec, uint64_t pixels);
+
+/* Failure detection (no counterpart in the reference, whose waits are host
+ * threads joining; its abort model is src/decoder/loopfilter.rs:300-338).
+ * Every device-side wait of the intra and loop-filter wavefronts is bounded:
+ * after `polls` polls of an unready neighbour the kernel records a code in
+ * the frame's error word, the other jobs of the frame give up as they next
+ * wait, and the call that synchronises returns RV9_DEVICE. The decoder's
+ * device state is then reset (cell maps, tickets) and stays usable; its
+ * reference slots hold what the failed frames left, as after any error.
+ * 0 restores the default (about a second of polling). */
+void rv9_decoder_set_wait_limit(rv9_decoder* dec, uint32_t polls);
+/* Failure injection for tests: bit 0 leaves the first intra job of every
+ * frame untaken, bit 1 the first loop-filter row, so that the jobs that
+ * depend on it wait until the wait limit runs out. Nothing faults and every
+ * wait ends. 0 (the default) turns it off. */
+void rv9_decoder_set_test_fault(rv9_decoder* dec, uint32_t mask);
 uint64_t rv9_decoder_frames_decoded(const rv9_decoder* dec);
 /* Message of the decoder's last error (valid until the next call). */
 const char* rv9_last_error(const rv9_decoder* dec);
@@ -160,9 +180,13 @@ rv9_status rv9_sequence_run(rv9_decoder* dec, rv9_sequence* seq, int flags, doub
  *
  * The first call on a device looks the array's address up with
  * cudaGetSymbolAddress; make that first call before any CUDA stream capture
- * begins. The counters and done flags must start at zero for each frame: the
- * call clears them with cudaMemsetAsync on the decoder's stream before each
- * frame; the loop-filter records are rewritten whole by each frame. All
+ * begins. The address is kept for the life of the process, so the device's
+ * primary context must stay alive (no cudaDeviceReset between calls). The
+ * tickets and done flags must start at zero for each frame: the call clears
+ * them with cudaMemsetAsync on the decoder's stream before each frame. The
+ * error word is cleared once, before the call's first frame, so a wait that
+ * gave up in any frame of the run is reported (RV9_DEVICE). The loop-filter
+ * records are rewritten whole by each frame. All
  * calls on one device share the one array, so calls that overlap in time on
  * the same device (two decoders, or two host threads) race on it and must be
  * serialised by the caller. */
@@ -226,6 +250,19 @@ rv9_status rv9_sequences_autotune(rv9_decoder* const* decs, rv9_sequence* const*
  * out->default_ms is one group with the default grain. */
 rv9_status rv9_sequences_autotune_batched(rv9_decoder* const* decs, rv9_sequence* const* seqs, size_t n,
                                           int32_t* groups, rv9_tune_result* out);
+
+/* A frame sink, for checking replays frame by frame (no counterpart in the
+ * reference): while it is set, every frame the decoder shows — in
+ * rv9_sequence_run (not graph replays), rv9_sequence_run_noalloc,
+ * rv9_sequences_run, rv9_sequences_run_batched and the decode calls — is
+ * copied, packed like rv9_frame data, into `buf` one after another. `buf`
+ * may be host memory (pinned or not) or device memory of the decoder's
+ * device; the copies are complete when the call that showed the frames
+ * returns. Frames that would overrun `cap` bytes are not copied but counted.
+ * buf == NULL turns the sink off; each set starts it empty. */
+void rv9_decoder_set_frame_sink(rv9_decoder* dec, uint8_t* buf, size_t cap);
+/* Frames and bytes the sink holds, and frames dropped for want of room. */
+void rv9_decoder_frame_sink_state(const rv9_decoder* dec, uint64_t* frames, size_t* bytes, uint64_t* dropped);
 
 /* The frame in reference slot `slot` (0..7), packed like rv9_frame data. */
 rv9_status rv9_decoder_download_slot(rv9_decoder* dec, int slot, uint8_t* out, size_t cap, size_t* bytes);

@@ -41,6 +41,7 @@ typedef struct rv9_gen_config {
   uint32_t rectangles;       /* moving 32x24 rectangles */
   uint32_t noise;            /* uniform noise amplitude at 8 bits */
   uint32_t threads;          /* encoder threads (tile columns); 0 = cores */
+  uint32_t color_space;      /* coded colour space: 0 = BT.709 (2), else the VP9 code (1 BT.601 ...) */
 } rv9_gen_config;
 
 /* Generates and encodes a stream: packets back to back into `out` (`cap`

@@ -7,6 +7,7 @@ cross-compiles, so this runs on a machine without a GPU.
 
 Usage: python rivet-vp9_b200/build.py [--force]
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -88,7 +89,7 @@ def build(force=False, verbose=False):
     if not force and not stale():
         return LIB
     os.makedirs(OUT, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for s in SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(OUT, os.path.basename(s) + ".o")
@@ -100,8 +101,12 @@ def build(force=False, verbose=False):
             cmd += os.environ["RV9_NVCC_FLAGS"].split()
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # The translation units compile independently, side by side.
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+        for f in [ex.submit(subprocess.run, c, check=True) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     subprocess.run([nvcc(), "-shared", *ARCH, "-o", tmp, *objs, "-lcudart", "-lpthread"], check=True)
     os.replace(tmp, LIB)

@@ -22,6 +22,7 @@ struct rv9_decoder {
   rv9::ParsedFrame pf;
   double parse_ms = 0;
   uint32_t parse_depth = 0;  // frames parsed at once; 0: one per two host threads
+  uint32_t threads = 0;      // set_threads value; 0: one per core
 };
 
 // Frames parsed at once by the multi-packet calls.
@@ -79,9 +80,23 @@ rv9_decoder* rv9_decoder_new(int device) {
 }
 
 void rv9_decoder_free(rv9_decoder* d) { delete d; }
-void rv9_decoder_set_threads(rv9_decoder* d, uint32_t t) { d->parser.set_threads((int)t); }
+void rv9_decoder_set_threads(rv9_decoder* d, uint32_t t) {
+  d->threads = t;
+  d->parser.set_threads((int)t);
+}
 void rv9_decoder_set_parse_depth(rv9_decoder* d, uint32_t frames) { d->parse_depth = frames; }
 void rv9_decoder_set_max_pixels(rv9_decoder* d, uint64_t p) { d->parser.set_max_pixels(p); }
+uint32_t rv9_decoder_threads(const rv9_decoder* d) {
+  if (!d) return 0;
+  if (d->threads) return d->threads;
+  return std::max(1u, std::thread::hardware_concurrency());
+}
+void rv9_decoder_set_wait_limit(rv9_decoder* d, uint32_t polls) {
+  if (d) d->engine.set_wait_limit(polls);
+}
+void rv9_decoder_set_test_fault(rv9_decoder* d, uint32_t mask) {
+  if (d) d->engine.set_test_skip(mask);
+}
 uint64_t rv9_decoder_frames_decoded(const rv9_decoder* d) { return d->parser.frames_decoded(); }
 const char* rv9_last_error(const rv9_decoder* d) { return d->err.c_str(); }
 const char* rv9_last_global_error(void) { return g_global_err.c_str(); }
@@ -410,6 +425,16 @@ size_t rv9_kernel_stats(rv9_decoder* d, rv9_kernel_stat* out, size_t cap, int re
 }
 
 void rv9_decoder_set_event_mask(rv9_decoder* d, uint32_t mask) { d->engine.event_mask = mask; }
+
+void rv9_decoder_set_frame_sink(rv9_decoder* d, uint8_t* buf, size_t cap) {
+  if (d) d->engine.set_sink(buf, buf ? cap : 0);
+}
+
+void rv9_decoder_frame_sink_state(const rv9_decoder* d, uint64_t* frames, size_t* bytes, uint64_t* dropped) {
+  if (frames) *frames = d ? d->engine.sink_frames() : 0;
+  if (bytes) *bytes = d ? d->engine.sink_used() : 0;
+  if (dropped) *dropped = d ? d->engine.sink_dropped() : 0;
+}
 
 void rv9_decoder_stats(rv9_decoder* d, rv9_stats* out, int reset) {
   out->device_ms = d->engine.device_ms;

@@ -329,6 +329,17 @@ int64_t TileHooks::motion_search(uint32_t r, uint32_t c, uint8_t bsize, int ref,
   int ew = std::max(1, std::min(w, s.width - x0)), eh = std::max(1, std::min(h, s.height - y0));
   auto sad_int = [&](int dx, int dy) {
     int64_t acc = 0;
+    if (x0 + dx >= 0 && x0 + dx + ew <= rp.width && y0 + dy >= 0 && y0 + dy + eh <= rp.height) {
+      // The window inside the reference: the same sums without the clamps.
+      for (int i = 0; i < eh; ++i) {
+        const uint16_t* ps = s.p[0].row(y0 + i) + x0;
+        const uint16_t* pr = rp.p[0].row(y0 + i + dy) + x0 + dx;
+        int32_t row = 0;  // at most 64 samples of 12 bits
+        for (int j = 0; j < ew; ++j) row += std::abs((int)ps[j] - (int)pr[j]);
+        acc += row;
+      }
+      return acc;
+    }
     for (int i = 0; i < eh; ++i) {
       const uint16_t* ps = s.p[0].row(y0 + i) + x0;
       const uint16_t* pr = rp.p[0].row(std::min(std::max(y0 + i + dy, 0), rp.height - 1));
@@ -626,7 +637,7 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
     w.f(0x83, 8);
     w.f(0x42, 8);
     if (profile >= 2) w.f(cfg.bit_depth == 12 ? 1 : 0, 1);
-    w.f(2, 3);  // BT.709
+    w.f(cfg.color_space ? std::min<uint32_t>(cfg.color_space, 6) : 2, 3);  // BT.709 unless asked (7, sRGB, is not written)
     w.f(0, 1);  // studio swing
     if (profile == 1 || profile == 3) {
       w.f(cfg.ss_x, 1);

@@ -88,6 +88,10 @@ bool Engine::init(int device, std::string* err) {
     return false;
   }
   n_sm_ = prop.multiProcessorCount;
+  if ((e = kernels_init_device(device)) != cudaSuccess) {
+    *err = std::string("setting up the kernels on the device: ") + cudaGetErrorString(e);
+    return false;
+  }
   if ((e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreate(&ev0_)) != cudaSuccess || (e = cudaEventCreate(&ev1_)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&stage_ev_[0], cudaEventDisableTiming)) != cudaSuccess ||
@@ -117,7 +121,7 @@ size_t Engine::packed_bytes(const DevFrame* f) {
   return ((size_t)f->width * f->height + 2 * cw * ch) * f->bps();
 }
 
-DevFrame* Engine::alloc_frame(const rv9_frame_desc& d) {
+DevFrame* Engine::alloc_frame(const rv9_frame_desc& d, cudaStream_t stream) {
   uint32_t aw = d.sb64_cols * 64, ah = d.sb64_rows * 64;
   // A frame no slot holds is free: every use of it is queued on the stream
   // before the work that overwrites it.
@@ -157,7 +161,13 @@ DevFrame* Engine::alloc_frame(const rv9_frame_desc& d) {
     f->planes[p] = (uint8_t*)f->base + plane_off[p];
     f->cells[p] = (uint8_t*)f->base + cell_off[p];
   }
-  cudaMemsetAsync(f->base, 0, off, stream_);
+  // Zeroed on the stream whose launches use the frame first (the cell map
+  // must read zero before that frame's preparation kernel marks it).
+  if (cudaMemsetAsync(f->base, 0, off, stream) != cudaSuccess) {
+    cudaFree(f->base);
+    delete f;
+    return nullptr;
+  }
   pool_.push_back(f);
   return f;
 }
@@ -411,7 +421,7 @@ rv9::Status Engine::prepare_frame(const FrameWork& fw, const uint8_t* d_base, cu
     return rv9::ST_OK;
   }
   const rv9_frame_desc& d = fw.desc;
-  DevFrame* cur = alloc_frame(d);
+  DevFrame* cur = alloc_frame(d, stream);
   if (!cur) {
     *err = "out of device memory for a frame";
     return rv9::ST_DEVICE;
@@ -424,10 +434,13 @@ rv9::Status Engine::prepare_frame(const FrameWork& fw, const uint8_t* d_base, cu
   cur->render_h = d.render_height;
   size_t mi_len = (size_t)d.mi_cols * d.mi_rows;
   if (fixed_) {
-    // Already checked against the array's size; zero the counters and the
-    // done flags (flags then compare against epoch 1).
+    // Already checked against the array's size; zero the two tickets and
+    // the done flags (flags then compare against epoch 1). The error word
+    // (the third counter) is cleared once per run, before its first frame,
+    // so that a wait that gave up in any frame stays reported.
     size_t flags = align256((size_t)d.sb64_cols * d.sb64_rows * 4);
-    CK(cudaMemsetAsync(fixed_, 0, 256 + flags, stream));
+    CK(cudaMemsetAsync(fixed_, 0, 2 * sizeof(int32_t), stream));
+    CK(cudaMemsetAsync(fixed_ + 256, 0, flags, stream));
   } else if (mi_len > lf_mi_cap_) {
     CK(cudaStreamSynchronize(stream));
     cudaFree(d_lf_mi_);
@@ -560,6 +573,8 @@ rv9::Status Engine::prepare_frame(const FrameWork& fw, const uint8_t* d_base, cu
     k.counters = d_counters_;
     k.error = d_counters_ + 2;
   }
+  k.wait_limit = wait_limit_;
+  k.test_skip = (int32_t)test_skip_;
   *out = cur;
   return rv9::ST_OK;
 }
@@ -591,7 +606,7 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   if (st != rv9::ST_OK) return st;
   if (!cur) {
     commit_frame(fw, nullptr, shown);
-    return rv9::ST_OK;
+    return sink_frame(*shown, stream_, err);
   }
   if (!fixed_) CK(cudaMemsetAsync(d_counters_, 0, 8, stream_));
   int L = 0;
@@ -612,7 +627,7 @@ rv9::Status Engine::run_frame(const FrameWork& fw, const uint8_t* d_base, bool p
   CK(cudaMemcpyAsync(h_error_ + 1, k.error, 4, cudaMemcpyDeviceToHost, stream_));
   launches += L;
   commit_frame(fw, cur, shown);
-  return rv9::ST_OK;
+  return sink_frame(*shown, stream_, err);
 }
 
 rv9::Status Engine::recon(const rv9::ParsedFrame& pf, DevFrame** shown, std::string* err) {
@@ -658,13 +673,31 @@ rv9::Status Engine::recon(const rv9::ParsedFrame& pf, DevFrame** shown, std::str
 }
 
 rv9::Status Engine::download_async(DevFrame* f, uint8_t* dst, std::string* err) {
+  return download_on(f, dst, stream_, err);
+}
+
+rv9::Status Engine::sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err) {
+  if (!sink_ || !shown || capturing_) return rv9::ST_OK;
+  const size_t nb = packed_bytes(shown);
+  if (sink_used_ + nb > sink_cap_) {
+    ++sink_dropped_;
+    return rv9::ST_OK;
+  }
+  rv9::Status st = download_on(shown, sink_ + sink_used_, stream, err);
+  if (st != rv9::ST_OK) return st;
+  sink_used_ += nb;
+  ++sink_frames_;
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::download_on(DevFrame* f, uint8_t* dst, cudaStream_t stream, std::string* err) {
   size_t bps = f->bps();
   size_t off = 0;
   for (int p = 0; p < 3; ++p) {
     size_t w = p ? (f->width + f->ss_x) >> f->ss_x : f->width;
     size_t h = p ? (f->height + f->ss_y) >> f->ss_y : f->height;
     CK(cudaMemcpy2DAsync(dst + off, w * bps, f->planes[p], (size_t)f->stride[p] * bps, w * bps, h,
-                         cudaMemcpyDeviceToHost, stream_));
+                         cudaMemcpyDefault, stream));
     off += w * h * bps;
   }
   return rv9::ST_OK;
@@ -1079,6 +1112,8 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
           if (!cur) {
             DevFrame* shown = nullptr;
             engines[j]->commit_frame(fw, nullptr, &shown);
+            st = engines[j]->sink_frame(shown, s, err);
+            if (st != rv9::ST_OK) return st;
             continue;
           }
           ks.push_back(k);
@@ -1097,6 +1132,8 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
         for (int q = 0; q < nf; ++q) {
           DevFrame* shown = nullptr;
           engines[who[q]]->commit_frame(seqs[who[q]]->frames[i], curs[q], &shown);
+          rv9::Status st = engines[who[q]]->sink_frame(shown, s, err);
+          if (st != rv9::ST_OK) return st;
         }
       }
     }
@@ -1200,7 +1237,7 @@ rv9::Status Engine::reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint
   // Distinct frames: hold each one while taking the next.
   std::vector<DevFrame*> held;
   for (int i = 0; i < n_frames; ++i) {
-    DevFrame* f = alloc_frame(d);
+    DevFrame* f = alloc_frame(d, stream_);
     if (!f) {
       for (DevFrame* h : held) --h->refs;
       *err = "out of device memory reserving frames";
@@ -1297,19 +1334,20 @@ rv9::Status Engine::sequence_run_fixed(const Sequence& seq, float* ms, std::stri
   if (rc != cudaSuccess) {
     *err = std::string("cudaGetSymbolAddress of the fixed scratch: ") + cudaGetErrorString(rc);
     st = rv9::ST_DEVICE;
-  } else {
-    // Slots are emptied first, as in sequence_run; the pool is checked
-    // against the frames the run will take.
-    reset_slots();
-    if (!pool_covers(seq)) {
-      *err = "the frame pool lacks frames this sequence needs (allocating nothing, it reuses the frames an "
-             "earlier rv9_sequence_run of the sequence left in the pool)";
-      st = rv9::ST_INVALID_INPUT;
-    }
+  } else if (!pool_covers(seq)) {
+    // Checked before anything changes: the pool is simulated with every
+    // frame free, as it is once the slots are emptied below.
+    *err = "the frame pool lacks frames this sequence needs (allocating nothing, it reuses the frames an "
+           "earlier rv9_sequence_run of the sequence left in the pool)";
+    st = rv9::ST_INVALID_INPUT;
   }
   if (st == rv9::ST_OK) {
+    // Slots are emptied first, as in sequence_run; the run's tickets and
+    // error word start at zero.
+    reset_slots();
     fixed_ = (uint8_t*)scratch;
-    rc = cudaEventRecord(ev0_, stream_);
+    rc = cudaMemsetAsync(fixed_, 0, 256, stream_);
+    if (rc == cudaSuccess) rc = cudaEventRecord(ev0_, stream_);
     for (size_t i = 0; rc == cudaSuccess && st == rv9::ST_OK && i < seq.frames.size(); ++i) {
       DevFrame* shown = nullptr;
       st = run_frame(seq.frames[i], seq.d_data, false, &shown, err);

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <atomic>
 #include <functional>
 #include <map>
 #include <string>
@@ -39,6 +41,17 @@ struct LaunchAux {
 cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm, int* launches, LaunchHook hook,
                          void* hook_ctx, const TuneParams& tune = TuneParams(), const LaunchAux* aux = nullptr);
 cudaError_t upload_filters(const int16_t* f);
+
+// Per-device kernel set-up: the shared-memory opt-ins of the wavefront
+// kernels and the batched launches' occupancy on that device. Once per
+// device (thread-safe), with `device` current; Engine::init calls it.
+struct DeviceKernels {
+  std::atomic<bool> ready{false};
+  int intra_batch_per_sm[2] = {1, 1};  // [8-bit, deeper]
+  int lf_batch_per_sm[2] = {1, 1};
+};
+cudaError_t kernels_init_device(int device);
+const DeviceKernels& device_kernels(int device);
 
 // Batched launches: one launch per stage for frames of many streams (no
 // frame of a batch may depend on another), all 8-bit or all above 8 bits.
@@ -184,6 +197,11 @@ class Engine {
   static rv9::Status autotune_concurrent(Engine* const* engines, const Sequence* const* seqs, size_t n,
                                          TuneParams* best, float* best_ms, float* default_ms, std::string* err);
   int device() const { return device_; }
+  // Polls before a wavefront wait gives up (0: the default, about a second
+  // of polling), and failure injection for tests (KFrame::test_skip; 0 in
+  // normal use). Both apply to frames launched after the call.
+  void set_wait_limit(uint32_t polls) { wait_limit_ = polls ? (int32_t)std::min<uint32_t>(polls, 1u << 30) : kDefaultWaitLimit; }
+  void set_test_skip(uint32_t mask) { test_skip_ = mask & 3; }
   // The device error word as last copied back (nonzero after a wavefront
   // wait gave up; sync() reports and clears it).
   int32_t error_word() const { return h_error_ ? *(volatile int32_t*)(h_error_ + 1) : 0; }
@@ -205,6 +223,23 @@ class Engine {
   // A device copy of `src` on this engine's device.
   rv9::Status sequence_clone(const Sequence& src, Sequence* seq, std::string* err);
   DevFrame* slot(int i) const { return slots_[i]; }
+  // A frame sink: while it is set, every frame the engine shows (sequence
+  // runs, concurrent and batched runs, the fixed-scratch run and recon();
+  // not graph replays) is copied, packed like rv9_frame data, to `buf`, one
+  // after another, queued on the stream of the frame's launches. `cap`
+  // bytes; frames that would not fit are counted in sink_dropped and not
+  // copied. Null turns it off. For checking what a run computed, frame by
+  // frame.
+  void set_sink(uint8_t* buf, size_t cap) {
+    sink_ = buf;
+    sink_cap_ = cap;
+    sink_used_ = 0;
+    sink_frames_ = 0;
+    sink_dropped_ = 0;
+  }
+  size_t sink_used() const { return sink_used_; }
+  uint64_t sink_frames() const { return sink_frames_; }
+  uint64_t sink_dropped() const { return sink_dropped_; }
 
   // Stats.
   double device_ms = 0;
@@ -214,7 +249,8 @@ class Engine {
   cudaStream_t stream() const { return stream_; }
 
  private:
-  DevFrame* alloc_frame(const rv9_frame_desc& d);
+  // A frame of d's geometry from the pool, or a new one zeroed on `stream`.
+  DevFrame* alloc_frame(const rv9_frame_desc& d, cudaStream_t stream);
   // Room for a frame's `n` staged bytes; *base receives their offset in the
   // buffer that the frame's offsets refer to. nullptr when it can't be had.
   using StageReserve = std::function<uint8_t*(size_t n, size_t* base)>;
@@ -228,6 +264,9 @@ class Engine {
   rv9::Status prepare_frame(const FrameWork& fw, const uint8_t* d_base, cudaStream_t stream, KFrame* k,
                             DevFrame** cur, std::string* err);
   void commit_frame(const FrameWork& fw, DevFrame* cur, DevFrame** shown);
+  // The shown frame's copy into the sink, if one is set (queued on `stream`).
+  rv9::Status sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err);
+  rv9::Status download_on(DevFrame* f, uint8_t* dst, cudaStream_t stream, std::string* err);
   // Loop-filter records and progress words for every frame of `seq`, so
   // that no frame of a run reallocates them.
   rv9::Status reserve_scratch(const Sequence& seq, std::string* err);
@@ -242,6 +281,9 @@ class Engine {
   static void hook(void* ctx, int kernel, int phase);
   void collect_kernel_events();
 
+  static constexpr int32_t kDefaultWaitLimit = 1 << 22;
+  int32_t wait_limit_ = kDefaultWaitLimit;
+  uint32_t test_skip_ = 0;
   int device_ = 0;
   int n_sm_ = 148;
   cudaStream_t stream_ = nullptr;
@@ -265,6 +307,9 @@ class Engine {
   int32_t* h_error_ = nullptr;     // pinned copy of the error word
   uint32_t epoch_ = 0;
   uint8_t* fixed_ = nullptr;  // the fixed scratch, during sequence_run_fixed
+  uint8_t* sink_ = nullptr;
+  size_t sink_cap_ = 0, sink_used_ = 0;
+  uint64_t sink_frames_ = 0, sink_dropped_ = 0;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   // run_batched's launch shapes and tables (pinned host, device), on the
   // first engine of the batch.

@@ -81,6 +81,12 @@ struct KFrame {
   uint32_t epoch;
   int32_t* counters;        // [0] intra tickets, [1] lf tickets
   int32_t* error;           // nonzero: a device wait timed out (code)
+  int32_t wait_limit;       // polls before a wavefront wait gives up
+  // Failure injection for tests (0 in normal use): bit 0 leaves the first
+  // intra job untaken, bit 1 the first loop-filter row, so that the jobs
+  // that depend on it wait until wait_limit runs out. No access goes out of
+  // bounds and every wait still ends.
+  int32_t test_skip;
 };
 
 }  // namespace rv9g

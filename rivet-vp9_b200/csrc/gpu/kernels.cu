@@ -44,7 +44,6 @@ namespace rv9g {
 
 __constant__ int16_t c_filters[4][16][8];
 
-static constexpr int kWaitLimit = 1 << 22;  // polls before a wait gives up
 
 template <class T>
 __device__ __forceinline__ T* plane_ptr(const PlanePtr& p) {
@@ -616,7 +615,7 @@ __device__ __forceinline__ bool intra_job(const KFrame& k, int job, IntraSmem<V>
         bool pending = cell != nullptr && *cell != 0;
         if (!__any_sync(0xffffffffu, pending)) break;
         if (__any_sync(0xffffffffu, *err != 0)) return false;
-        if (++polls > kWaitLimit) {
+        if (++polls > k.wait_limit) {
           if (lane == 0) atomicCAS(k.error, 0, 1);
           return false;
         }
@@ -700,7 +699,7 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
     // One job per ticket.
     int job = 0;
     if (lane == 0) job = atomicAdd(&k.counters[0], 1);
-    job = __shfl_sync(0xffffffffu, job, 0);
+    job = __shfl_sync(0xffffffffu, job, 0) + (k.test_skip & 1);
     if (job >= k.n_intra_jobs) return;
     if (!intra_job<T, V>(k, job, sm, lane)) return;
   }
@@ -1058,7 +1057,7 @@ __device__ __forceinline__ bool lf_row(const KFrame& k, LfRowSmem& S, const int 
           for (;;) {
             uint32_t v = *above;
             if ((v & 0xffff0000u) == ep && (int)(v & 0xffffu) >= need) break;
-            if (*(volatile int32_t*)k.error || ++polls > kWaitLimit) {
+            if (*(volatile int32_t*)k.error || ++polls > k.wait_limit) {
               atomicCAS(k.error, 0, 2);
               S.abort_flag = 1;
               break;
@@ -1169,7 +1168,7 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows(KFrame k) {
   extern __shared__ __align__(16) unsigned char lf_raw[];
   LfRowSmem& S = *reinterpret_cast<LfRowSmem*>(lf_raw);
   for (;;) {
-    if (threadIdx.x == 0) lf_row_start(k, S, atomicAdd(&k.counters[1], 1));
+    if (threadIdx.x == 0) lf_row_start(k, S, atomicAdd(&k.counters[1], 1) + ((k.test_skip >> 1) & 1));
     __syncthreads();
     const int sr = S.row;
     if (sr >= k.sb64_rows) return;
@@ -1302,7 +1301,8 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra_batch(BatchArgs a) {
     int job = 0;
     const int f = batch_take(a, home, 0, &job);
     if (f < 0) return;
-    intra_job<T, V>(a.frames[f], job, sm, lane);
+    job += a.frames[f].test_skip & 1;
+    if (job < a.frames[f].n_intra_jobs) intra_job<T, V>(a.frames[f], job, sm, lane);
   }
 }
 
@@ -1317,13 +1317,16 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows_batch(BatchArgs a) {
       const int f = batch_take(a, home, 1, &r);
       if (threadIdx.x == 0) {
         S.frame = f;
-        if (f >= 0) lf_row_start(a.frames[f], S, r);
+        if (f >= 0) lf_row_start(a.frames[f], S, r + ((a.frames[f].test_skip >> 1) & 1));
       }
     }
     __syncthreads();
     const int f = S.frame, sr = S.row;
     if (f < 0) return;
-    lf_row<T>(a.frames[f], S, sr);
+    if (sr < a.frames[f].sb64_rows)
+      lf_row<T>(a.frames[f], S, sr);
+    else
+      __syncthreads();  // (a skipped row: S is rewritten only after every thread has read it)
   }
 }
 
@@ -1331,6 +1334,54 @@ __global__ void __launch_bounds__(kLfRowThreads) k_lf_rows_batch(BatchArgs a) {
 // Host-side launch of one frame's chain.
 
 cudaError_t upload_filters(const int16_t* f) { return cudaMemcpyToSymbol(c_filters, f, sizeof(int16_t) * 4 * 16 * 8); }
+
+// Kernel attributes are per device: the shared-memory opt-ins of the intra
+// and loop-filter kernels (above the 48 KB default) are set on each device
+// an engine starts on, and the batched launches' grids come from that
+// device's occupancy.
+constexpr int kMaxDevices = 64;
+static DeviceKernels g_devices[kMaxDevices];
+static std::mutex g_devices_mu;
+
+const DeviceKernels& device_kernels(int device) {
+  static const DeviceKernels none;
+  return device >= 0 && device < kMaxDevices ? g_devices[device] : none;
+}
+
+template <class T, class V>
+static cudaError_t init_device_t(DeviceKernels* d) {
+  const int i = sizeof(T) - 1;
+  const int intra_smem = (int)(sizeof(IntraSmem<V>) * kIntraWarps), lf_smem = (int)sizeof(LfRowSmem);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_intra<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, intra_smem)) ||
+      (e = cudaFuncSetAttribute(k_intra_batch<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, intra_smem)) ||
+      (e = cudaFuncSetAttribute(k_lf_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lf_smem)) ||
+      (e = cudaFuncSetAttribute(k_lf_rows_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lf_smem)))
+    return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d->intra_batch_per_sm[i], k_intra_batch<T, V>,
+                                                         32 * kIntraWarps, intra_smem)) ||
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d->lf_batch_per_sm[i], k_lf_rows_batch<T>, kLfRowThreads,
+                                                         lf_smem)))
+    return e;
+  d->intra_batch_per_sm[i] = std::max(d->intra_batch_per_sm[i], 1);
+  d->lf_batch_per_sm[i] = std::max(d->lf_batch_per_sm[i], 1);
+  return cudaSuccess;
+}
+
+cudaError_t kernels_init_device(int device) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_devices_mu);
+  DeviceKernels& d = g_devices[device];
+  if (d.ready.load(std::memory_order_acquire)) return cudaSuccess;
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return e;
+  if (cur != device) return cudaErrorInvalidDevice;  // the caller makes `device` current
+  if ((e = init_device_t<uint8_t, L32>(&d)) != cudaSuccess || (e = init_device_t<uint16_t, L64>(&d)) != cudaSuccess)
+    return e;
+  d.ready.store(true, std::memory_order_release);
+  return cudaSuccess;
+}
 
 // The preparation launch's parts for a frame of n_blocks blocks.
 static PrepSplit prep_split(const KFrame& k, int n_blocks) {
@@ -1409,15 +1460,20 @@ void batch_fill(const KFrame* ks, const int* n_blocks, int n, uint8_t* host, Bat
 }
 
 template <class T, class V>
-static cudaError_t launch_batch_t(const uint8_t* dev, int n, const BatchTotals& tot, cudaStream_t s, int n_sm,
+static cudaError_t launch_batch_t(const uint8_t* tables, int n, const BatchTotals& tot, cudaStream_t s, int n_sm,
                                   const TuneParams& tune, int* launches) {
   const BatchLayout l = batch_layout(n);
   BatchArgs a;
-  a.frames = reinterpret_cast<const KFrame*>(dev + l.o_frames);
-  a.prep = reinterpret_cast<const PrepSplit*>(dev + l.o_prep);
-  a.res = reinterpret_cast<const ResSplit*>(dev + l.o_res);
-  a.base = reinterpret_cast<const uint32_t*>(dev + l.o_base);
+  a.frames = reinterpret_cast<const KFrame*>(tables + l.o_frames);
+  a.prep = reinterpret_cast<const PrepSplit*>(tables + l.o_prep);
+  a.res = reinterpret_cast<const ResSplit*>(tables + l.o_res);
+  a.base = reinterpret_cast<const uint32_t*>(tables + l.o_base);
   a.n = n;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return e;
+  const DeviceKernels& dev = device_kernels(device);
+  if (!dev.ready.load(std::memory_order_acquire)) return cudaErrorInitializationError;
   int L = 0;
   // The preparation launch always runs: its first CTA clears the tickets.
   k_prep_batch<T><<<tot.ctas[kBasePrep] ? tot.ctas[kBasePrep] : 1, kPrepThreads, 0, s>>>(a);
@@ -1439,29 +1495,14 @@ static cudaError_t launch_batch_t(const uint8_t* dev, int n, const BatchTotals& 
     // keyframe wavefront needs its warps whatever else is in the batch), up
     // to what fits on the device at once.
     const size_t smem = sizeof(IntraSmem<V>) * kIntraWarps;
-    static int per_sm = 0;
-    if (!per_sm) {
-      cudaFuncSetAttribute(k_intra_batch<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_intra_batch<T, V>, 32 * kIntraWarps, smem) !=
-              cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-    }
+    const int per_sm = dev.intra_batch_per_sm[sizeof(T) - 1];
     const int grid = (int)std::min<uint32_t>(tot.intra_ctas, (uint32_t)(n_sm * per_sm));
     k_intra_batch<T, V><<<grid > 0 ? grid : 1, 32 * kIntraWarps, smem, s>>>(a);
     ++L;
   }
   if (tot.lf_rows) {
     // As many row CTAs as fit on the device at once (more would only wait).
-    static int per_sm = 0;
-    if (!per_sm) {
-      cudaFuncSetAttribute(k_lf_rows_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LfRowSmem));
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lf_rows_batch<T>, kLfRowThreads,
-                                                        sizeof(LfRowSmem)) != cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-    }
-    const int cap = n_sm * per_sm;
+    const int cap = n_sm * dev.lf_batch_per_sm[sizeof(T) - 1];
     k_lf_rows_batch<T><<<(int)tot.lf_rows < cap ? (int)tot.lf_rows : cap, kLfRowThreads, sizeof(LfRowSmem), s>>>(a);
     ++L;
   }
@@ -1533,11 +1574,6 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
   }
   if (k.n_intra > 0) {
     size_t smem = sizeof(IntraSmem<V>) * kIntraWarps;
-    static bool attr_set = false;
-    if (!attr_set) {
-      cudaFuncSetAttribute(k_intra<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_set = true;
-    }
     // One CTA per SM at most: a warp per job of the wavefront's width (a
     // diagonal of superblocks, a few rows of transform blocks each) with
     // room to spare; more warps would only poll further ahead, taking issue
@@ -1553,11 +1589,6 @@ static cudaError_t launch_frame_t(const KFrame& k, int n_blocks, cudaStream_t s,
   }
   if (k.lf_on) {
     // One CTA per superblock row (rows are taken in order from a ticket).
-    static bool lf_attr_set = false;
-    if (!lf_attr_set) {
-      cudaFuncSetAttribute(k_lf_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LfRowSmem));
-      lf_attr_set = true;
-    }
     int grid = k.sb64_rows < n_sm ? k.sb64_rows : n_sm;
     mark(K_LF, 0);
     k_lf_rows<T><<<grid, kLfRowThreads, sizeof(LfRowSmem), s>>>(k);
@@ -1587,8 +1618,11 @@ cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm
 static __device__ __align__(256) uint8_t g_fixed_scratch[kFixedScratchBytes];
 
 cudaError_t fixed_scratch_address(int device, void** ptr) {
-  // Resolved once per device, with that device current.
-  constexpr int kMaxDevices = 64;
+  // Resolved once per device, with that device current, and kept for the
+  // life of the process: the address belongs to the device's primary
+  // context, so a host application that destroys that context
+  // (cudaDeviceReset) must not call the no-allocation entry point again in
+  // this process.
   static std::mutex mu;
   static void* addr[kMaxDevices] = {nullptr};
   *ptr = nullptr;

@@ -73,7 +73,8 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_sequence_run", "rv9_sequence_frames", "rv9_sequence_luma_samples", "rv9_sequence_algorithmic_bytes",
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
            "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_sequences_run_batched", "rv9_sequences_autotune_batched", "rv9_decoder_autotune",
-           "rv9_sequences_autotune", "rv9_decoder_set_event_mask")
+           "rv9_sequences_autotune", "rv9_decoder_set_event_mask", "rv9_decoder_threads", "rv9_decoder_set_wait_limit",
+           "rv9_decoder_set_test_fault", "rv9_decoder_set_frame_sink", "rv9_decoder_frame_sink_state")
 
 
 class CTuneResult(ctypes.Structure):
@@ -140,6 +141,13 @@ def load_library(path=None):
     lib.rv9_sequence_clone.argtypes = [vp, vp, ctypes.POINTER(vp)]
     lib.rv9_decoder_download_slot.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
     lib.rv9_decoder_set_event_mask.argtypes = [vp, ctypes.c_uint32]
+    lib.rv9_decoder_set_frame_sink.argtypes = [vp, vp, ctypes.c_size_t]
+    lib.rv9_decoder_frame_sink_state.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_size_t),
+                                                 ctypes.POINTER(ctypes.c_uint64)]
+    lib.rv9_decoder_threads.restype = ctypes.c_uint32
+    lib.rv9_decoder_threads.argtypes = [vp]
+    lib.rv9_decoder_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
+    lib.rv9_decoder_set_test_fault.argtypes = [vp, ctypes.c_uint32]
     lib.rv9_kernel_stats.restype = ctypes.c_size_t
     lib.rv9_kernel_stats.argtypes = [vp, ctypes.POINTER(CKernelStat), ctypes.c_size_t, ctypes.c_int]
     if path is None:
@@ -325,8 +333,22 @@ class Decoder:
         """Frames parsed at once by decode_packets / load_sequence (0: auto)."""
         self._lib.rv9_decoder_set_parse_depth(self._dec, frames)
 
+    def threads(self):
+        """Host threads parsing uses (Decoder::threads)."""
+        return self._lib.rv9_decoder_threads(self._dec)
+
     def set_max_pixels(self, n):
         self._lib.rv9_decoder_set_max_pixels(self._dec, n)
+
+    def set_wait_limit(self, polls):
+        """Polls before a device-side wavefront wait gives up (0: default)."""
+        self._lib.rv9_decoder_set_wait_limit(self._dec, polls)
+
+    def set_test_fault(self, mask):
+        """Failure injection for tests (rv9_decoder_set_test_fault): bit 0
+        leaves each frame's first intra job untaken, bit 1 its first
+        loop-filter row; 0 turns it off."""
+        self._lib.rv9_decoder_set_test_fault(self._dec, mask)
 
     def frames_decoded(self):
         return self._lib.rv9_decoder_frames_decoded(self._dec)
@@ -413,6 +435,17 @@ class Decoder:
         if st != RV9_OK:
             _raise(self._lib, self._dec, st)
         return buf.raw[:n.value]
+
+    def set_frame_sink(self, ptr, cap):
+        """Every frame shown from now on is copied, packed, to `cap` bytes at
+        address `ptr` (host or device memory); ptr 0 turns the sink off."""
+        self._lib.rv9_decoder_set_frame_sink(self._dec, ptr or None, cap if ptr else 0)
+
+    def frame_sink_state(self):
+        """(frames, bytes, dropped) of the frame sink."""
+        f, b, d = ctypes.c_uint64(), ctypes.c_size_t(), ctypes.c_uint64()
+        self._lib.rv9_decoder_frame_sink_state(self._dec, ctypes.byref(f), ctypes.byref(b), ctypes.byref(d))
+        return f.value, b.value, d.value
 
     def set_event_mask(self, names=None):
         """Kernels that per_kernel runs bracket with events (None: all)."""

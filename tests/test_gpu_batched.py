@@ -48,49 +48,68 @@ def _close(decs, seqs):
         d.close()
 
 
-def test_batched_equals_alone():
+def test_batched_equals_alone(oracle_lib):
+    # Every shown frame of every batched run (through the frame sinks) is the
+    # oracle's, and the reference slots end as after the sequence alone.
     import rv9
+    from conftest import FrameSinks, oracle_frames
     decs, seqs = _load(NAMES)
+    want = [oracle_frames(oracle_lib, read_packets(os.path.join(VECTORS_DIR, n))) for n in NAMES]
+    sinks = FrameSinks(decs, 64 << 20)
     try:
         alone = []
-        for d, s in zip(decs, seqs):
+        for i, (d, s) in enumerate(zip(decs, seqs)):
             s.run()
             alone.append(_slots(d))
+            assert sinks.md5s(i, [sz for _, sz in want[i]]) == [m for m, _ in want[i]], NAMES[i]
         for groups in (1, 2, 3, len(NAMES)):
+            sinks.reset()
             ms = rv9.run_batched(list(zip(decs, seqs)), groups=groups)
             assert ms > 0
-            for d, want in zip(decs, alone):
-                assert _slots(d) == want, groups
+            for i, (d, slots) in enumerate(zip(decs, alone)):
+                assert sinks.md5s(i, [sz for _, sz in want[i]]) == [m for m, _ in want[i]], (groups, NAMES[i])
+                assert _slots(d) == slots, groups
         # An ordinary run after batched ones still matches.
         seqs[1].run()
         assert _slots(decs[1]) == alone[1]
     finally:
+        sinks.detach()
         _close(decs, seqs)
 
 
-def test_batched_large_frames_equal_alone():
+def test_batched_large_frames_equal_alone(oracle_lib):
     # Generated streams at the benchmark shapes (1080p 8-bit with 4 tile
     # columns, 2160p 10-bit, 720p 12-bit 4:4:4, 720p 10-bit 4:2:2), several
     # decoders per content, so that the wavefront stages share each launch
-    # among many large frames.
+    # among many large frames. Every shown frame is the oracle's.
     import rv9
+    from conftest import FrameSinks, oracle_frames
     contents = [generate(name)[0] for name in ("1080p_8bit_q40", "2160p_10bit_q30", "720p_12bit_444_q30",
                                                "720p_10bit_422_q50", "cif_8bit_q60")]
-    decs, seqs = [], []
+    want = [oracle_frames(oracle_lib, pk) for pk in contents]
+    decs, seqs, which = [], [], []
     try:
         for rep in range(3):
-            for pk in contents:
+            for k, pk in enumerate(contents):
                 d = rv9.Decoder(0)
                 decs.append(d)
                 seqs.append(d.load_sequence(pk))
+                which.append(k)
         alone = []
         for d, s in zip(decs, seqs):
             s.run()
             alone.append(_slots(d))
-        for groups in (1, 4):
-            rv9.run_batched(list(zip(decs, seqs)), groups=groups)
-            for i, (d, want) in enumerate(zip(decs, alone)):
-                assert _slots(d) == want, (groups, i)
+        sinks = FrameSinks(decs, 96 << 20)
+        try:
+            for groups in (1, 4):
+                sinks.reset()
+                rv9.run_batched(list(zip(decs, seqs)), groups=groups)
+                for i, (d, slots) in enumerate(zip(decs, alone)):
+                    w = want[which[i]]
+                    assert sinks.md5s(i, [sz for _, sz in w]) == [m for m, _ in w], (groups, i)
+                    assert _slots(d) == slots, (groups, i)
+        finally:
+            sinks.detach()
     finally:
         _close(decs, seqs)
 
@@ -129,4 +148,27 @@ def test_batched_autotune_keeps_results_exact():
         for d, want in zip(decs, alone):
             assert _slots(d) == want
     finally:
+        _close(decs, seqs)
+
+
+def test_batched_on_fresh_decoders(oracle_lib):
+    # Decoders that have never run: their frames are allocated (and zeroed)
+    # by the batched run itself, on the group streams that first use them,
+    # with fewer groups than decoders so that most decoders' launches go on
+    # another decoder's stream. Every shown frame is checked, through the
+    # frame sink, against the oracle and the published MD5s.
+    import rv9
+    from conftest import FrameSinks, expected_md5s, oracle_frames
+    names = NAMES[:6]
+    decs, seqs = _load(names)
+    sinks = FrameSinks(decs, 64 << 20)
+    try:
+        rv9.run_batched(list(zip(decs, seqs)), groups=2)
+        for i, n in enumerate(names):
+            path = os.path.join(VECTORS_DIR, n)
+            want = oracle_frames(oracle_lib, read_packets(path))
+            got = sinks.md5s(i, [sz for _, sz in want])
+            assert got == [m for m, _ in want] == expected_md5s(path), n
+    finally:
+        sinks.detach()
         _close(decs, seqs)

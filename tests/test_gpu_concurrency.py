@@ -33,21 +33,29 @@ def _slots(dec):
     return out
 
 
-def test_concurrent_equals_alone():
+def test_concurrent_equals_alone(oracle_lib):
+    # Every shown frame of each concurrent run (through the frame sinks) is
+    # the oracle's, and the reference slots end as after the sequence alone.
     import rv9
+    from conftest import FrameSinks, oracle_frames
     decs = [rv9.Decoder(0) for _ in NAMES]
     seqs = [d.load_sequence(read_packets(os.path.join(VECTORS_DIR, n))) for d, n in zip(decs, NAMES)]
+    want = [oracle_frames(oracle_lib, read_packets(os.path.join(VECTORS_DIR, n))) for n in NAMES]
+    sinks = FrameSinks(decs, 64 << 20)
     try:
         alone = []
         for d, s in zip(decs, seqs):
             s.run()
             alone.append(_slots(d))
         for rep in range(3):
+            sinks.reset()
             ms = rv9.run_concurrent(list(zip(decs, seqs)), per_kernel=(rep == 1))
             assert ms > 0
-            for d, want in zip(decs, alone):
-                assert _slots(d) == want
+            for i, (d, slots) in enumerate(zip(decs, alone)):
+                assert sinks.md5s(i, [sz for _, sz in want[i]]) == [m for m, _ in want[i]], (rep, NAMES[i])
+                assert _slots(d) == slots
     finally:
+        sinks.detach()
         for d, s in zip(decs, seqs):
             s.free()
             d.close()
