@@ -70,11 +70,12 @@ class Completion:
     """A finished request. `frames` holds Frame objects copied out of the
     engine's pinned buffers, which go back to the stream at once."""
 
-    def __init__(self, c, frames):
+    def __init__(self, c, frames, md5s=None):
         self.stream, self.tag, self.status = c.stream, c.tag, c.status
         self.submit_ms, self.latency_ms = c.submit_ms, c.latency_ms
         self.n_frames = c.n_frames
         self.frames = frames
+        self.md5s = md5s  # hex MD5 of each frame's packed planes, when asked for
 
     @property
     def ok(self):
@@ -106,15 +107,22 @@ class Engine:
         if st != RV9_OK:
             raise _ERRORS.get(st, Rv9Error)(f"rv9_submit: status {st}")
 
-    def poll(self, max_items=64, timeout_ms=0, keep_frames=True):
+    def poll(self, max_items=64, timeout_ms=0, keep_frames=True, digest=None):
         """Finished requests; with keep_frames False only their metadata is
-        kept (the frames are not copied out)."""
+        kept (the frames are not copied out). `digest(tag)` -> True asks for
+        the MD5 of that request's frames, hashed in place in the engine's
+        buffer before it is released (Completion.md5s)."""
+        import hashlib
         arr = (CCompletion * max_items)()
         n = self._lib.rv9_poll(self._e, arr, max_items, timeout_ms)
         out = []
         for c in arr[:n]:
             frames = [Frame(c.frames[i]) for i in range(c.n_frames)] if keep_frames else []
-            out.append(Completion(c, frames))
+            md5s = None
+            if digest is not None and digest(c.tag) and c.status == RV9_OK:
+                md5s = [hashlib.md5(memoryview((ctypes.c_char * c.frames[i].size).from_address(
+                    ctypes.cast(c.frames[i].data, ctypes.c_void_p).value))).hexdigest() for i in range(c.n_frames)]
+            out.append(Completion(c, frames, md5s))
             self._lib.rv9_completion_release(self._e, ctypes.byref(c))
         return out
 

@@ -70,10 +70,11 @@ def _ref_rank(rank, world, port, out):
         steps, warmup, frames = 1, 3, 2
     ran = []
 
-    def stop(spec):  # the first thing the reference arm does on its rank
-        ran.append(spec["name"])
+    def stop(specs):  # the first thing the reference arm does on its rank
+        ran.extend(s["name"] for s in specs)
         raise RuntimeError("stop")
-    bench.stream_packets = stop
+    from rv9 import workloads
+    workloads.ensure_cached = stop
     w, r, _ = bench.dist_setup("gloo")
     try:
         bench.run_reference(Args, w, r)
