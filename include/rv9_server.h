@@ -31,8 +31,18 @@ typedef struct rv9_engine rv9_engine;
 
 /* An engine on `device` (-1: current) admitting streams within
  * `hbm_budget_bytes`, with `workers` host threads parsing (0: one per core).
- * NULL when no usable device is present (rv9_last_global_error says why). */
+ * NULL when no usable device is present (rv9_last_global_error says why).
+ * Each stream's frames are reconstructed on its own CUDA stream. */
 rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers);
+/* The same engine with the streams' reconstruction batched on the device:
+ * the streams are split round-robin into `groups` groups (0: one), and each
+ * group's launcher reconstructs the next parsed frame of every stream of the
+ * group that has one together, one launch per stage (the stage kernels take
+ * their work from all of those frames), on the group's CUDA stream. A
+ * launcher keeps at most two steps queued on the device, so frames that
+ * arrive while the GPU is busy join the next step. Results are bit-identical
+ * to the plain engine's. */
+rv9_engine* rv9_engine_create_batched(int device, uint64_t hbm_budget_bytes, uint32_t workers, uint32_t groups);
 /* Closes every stream, waits for their submitted requests, then frees the
  * engine, with any completions not yet released. */
 void rv9_engine_free(rv9_engine* eng);
@@ -86,8 +96,42 @@ typedef struct rv9_engine_stats {
   uint64_t requests_submitted, requests_completed;
   uint64_t frames_decoded;
   uint64_t reserved_bytes, budget_bytes;
+  uint64_t batched_steps, batched_frames; /* batched form: steps launched and frames in them */
 } rv9_engine_stats;
 void rv9_engine_get_stats(rv9_engine* eng, rv9_engine_stats* out);
+
+/* ---- Several GPUs of one node ----
+ *
+ * A cluster is a serving engine per device. Streams are independent and a
+ * stream's frames chain through its own reference slots, so each stream is
+ * placed whole on one device and stays there; devices exchange nothing (no
+ * collective, no peer memory). A new stream goes to the device with the
+ * fewest reserved bytes among those whose budget has room for its
+ * reservation (rv9_stream_reservation), else to the least loaded device that
+ * could ever hold it, where it waits pending. Stream ids are the cluster's;
+ * completions of every device come back through rv9_cluster_poll. */
+typedef struct rv9_cluster rv9_cluster;
+/* Engines on devices[0..n) (each as rv9_engine_create(devices[i],
+ * hbm_budget_per_device, workers_per_device)). NULL when any fails. */
+rv9_cluster* rv9_cluster_create(const int* devices, size_t n, uint64_t hbm_budget_per_device,
+                                uint32_t workers_per_device);
+void rv9_cluster_free(rv9_cluster* c);
+/* Opens a stream on the device the placement rule picks; *device receives
+ * that device's ordinal (may be NULL). RV9_UNSUPPORTED when no device's
+ * budget could ever hold the stream. */
+rv9_status rv9_cluster_stream_open(rv9_cluster* c, const rv9_stream_spec* spec, int64_t* id, int* device);
+rv9_status rv9_cluster_stream_close(rv9_cluster* c, int64_t id);
+rv9_status rv9_cluster_submit(rv9_cluster* c, int64_t id, const uint8_t* packet, size_t len, uint64_t tag);
+/* Finished requests of all devices (completion.stream is the cluster's id);
+ * waits up to timeout_ms for the first. */
+size_t rv9_cluster_poll(rv9_cluster* c, rv9_completion* out, size_t cap, int timeout_ms);
+void rv9_cluster_completion_release(rv9_cluster* c, rv9_completion* comp);
+/* The engine statistics of the cluster's device_index-th device. */
+void rv9_cluster_get_stats(rv9_cluster* c, int device_index, rv9_engine_stats* out);
+/* The placement rule on its own (no device needed): the index of the device
+ * a stream needing `need` bytes goes to, given each device's reserved bytes
+ * and budget; -1 when none could ever hold it. */
+int rv9_place_least_loaded(const uint64_t* load, const uint64_t* budget, size_t n, uint64_t need);
 
 #ifdef __cplusplus
 }

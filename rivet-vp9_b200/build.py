@@ -22,6 +22,7 @@ SOURCES = [
     "gpu/engine.cpp",
     "api/rv9_api.cpp",
     "serve/server.cpp",
+    "serve/cluster.cpp",
     "host/parser.cpp",
     "host/probs.cpp",
 ]

@@ -1037,6 +1037,108 @@ rv9::Status Engine::reserve_scratch(const Sequence& seq, std::string* err) {
   return rv9::ST_OK;
 }
 
+size_t Engine::step_table_bytes(size_t n) { return 2 * batch_table_bytes((int)n); }
+
+rv9::Status Engine::launch_step(Engine* const* engines, const FrameWork* const* fws, const uint8_t* const* bases,
+                                size_t n, cudaStream_t s, const TuneParams& tune, uint8_t* h_tables,
+                                uint8_t* d_tables, size_t* table_bytes, DevFrame** shown, int* launches,
+                                std::string* err) {
+  *table_bytes = 0;
+  std::vector<KFrame> ks;
+  std::vector<int> nb;
+  std::vector<DevFrame*> curs;
+  std::vector<size_t> who;
+  const int n_sm = n ? engines[0]->n_sm_ : 0;
+  for (int c = 0; c < 2; ++c) {
+    ks.clear();
+    nb.clear();
+    curs.clear();
+    who.clear();
+    for (size_t q = 0; q < n; ++q) {
+      const FrameWork& fw = *fws[q];
+      // Kernels are typed by sample size: 8-bit frames (and frames that only
+      // show an existing one) in the first launch set, deeper ones in the second.
+      if ((fw.show_existing ? 0 : (fw.desc.bit_depth > 8 ? 1 : 0)) != c) continue;
+      Engine* e = engines[q];
+      KFrame k;
+      DevFrame* cur = nullptr;
+      rv9::Status st = e->prepare_frame(fw, bases[q], s, &k, &cur, err);
+      if (st != rv9::ST_OK) return st;
+      if (!cur) {
+        e->commit_frame(fw, nullptr, &shown[q]);
+        st = e->sink_frame(shown[q], s, err);
+        if (st != rv9::ST_OK) return st;
+        continue;
+      }
+      ks.push_back(k);
+      nb.push_back((int)fw.n_blocks);
+      curs.push_back(cur);
+      who.push_back(q);
+    }
+    if (ks.empty()) continue;
+    const int nf = (int)ks.size();
+    BatchTotals tot;
+    batch_fill(ks.data(), nb.data(), nf, h_tables + *table_bytes, &tot, n_sm, tune);
+    const size_t bytes = batch_table_bytes(nf);
+    CK(cudaMemcpyAsync(d_tables + *table_bytes, h_tables + *table_bytes, bytes, cudaMemcpyHostToDevice, s));
+    CK(launch_batch(d_tables + *table_bytes, nf, tot, c == 1, s, n_sm, tune, launches));
+    *table_bytes += bytes;
+    for (int f = 0; f < nf; ++f) {
+      Engine* e = engines[who[f]];
+      e->commit_frame(*fws[who[f]], curs[f], &shown[who[f]]);
+      // The frame's error word, for sync() and error_word().
+      CK(cudaMemcpyAsync(e->h_error_ + 1, e->d_counters_ + 2, 4, cudaMemcpyDeviceToHost, s));
+      rv9::Status st = e->sink_frame(shown[who[f]], s, err);
+      if (st != rv9::ST_OK) return st;
+    }
+  }
+  return rv9::ST_OK;
+}
+
+rv9::Status Engine::stage(const rv9::ParsedFrame& pf, cudaStream_t s, FrameWork* fw, const uint8_t** d_base,
+                          std::string* err) {
+  *d_base = nullptr;
+  if (pf.show_existing) {
+    build_work(pf, fw, StageReserve());
+    return rv9::ST_OK;
+  }
+  // As recon(): the frame's bytes straight into the pinned buffer of this
+  // turn (its previous copy done), then one copy to the device, on `s`.
+  int b = stage_;
+  stage_ ^= 1;
+  CK(cudaEventSynchronize(stage_ev_[b]));
+  cudaError_t alloc_err = cudaSuccess;
+  auto reserve = [&](size_t bytes, size_t* base) -> uint8_t* {
+    *base = 0;
+    if (bytes > h_stage_cap_[b]) {
+      size_t cap = std::max(bytes, h_stage_cap_[b] * 3 / 2);
+      cudaFreeHost(h_stage_[b]);
+      h_stage_[b] = nullptr;
+      h_stage_cap_[b] = 0;
+      if ((alloc_err = cudaMallocHost(&h_stage_[b], cap)) != cudaSuccess) return nullptr;
+      h_stage_cap_[b] = cap;
+    }
+    return h_stage_[b];
+  };
+  if (!build_work(pf, fw, reserve)) {
+    *err = std::string("pinned staging buffer: ") + cudaGetErrorString(alloc_err);
+    return rv9::ST_DEVICE;
+  }
+  if (fw->bytes > stage_cap_[b]) {
+    size_t cap = std::max(fw->bytes, stage_cap_[b] * 3 / 2);
+    CK(cudaStreamSynchronize(s));
+    cudaFree(d_stage_[b]);
+    d_stage_[b] = nullptr;
+    stage_cap_[b] = 0;
+    CK(cudaMalloc(&d_stage_[b], cap));
+    stage_cap_[b] = cap;
+  }
+  CK(cudaMemcpyAsync(d_stage_[b], h_stage_[b], fw->bytes, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(stage_ev_[b], s));
+  *d_base = d_stage_[b];
+  return rv9::ST_OK;
+}
+
 rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int groups,
                                 float* ms, std::string* err) {
   *ms = 0;
@@ -1062,17 +1164,15 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
     engines[j]->reset_slots();
     most = std::max(most, seqs[j]->frames.size());
   }
-  // Every batch of the run has its own region of the tables, so that no
-  // copy waits for an earlier batch's launches.
-  auto batch_class = [](const FrameWork& fw) { return fw.desc.bit_depth > 8 ? 1 : 0; };
+  // Every step of the run has its own region of the tables, so that no
+  // copy waits for an earlier step's launches.
   size_t total = 0;
   for (size_t i = 0; i < most; ++i)
     for (size_t g = 0; g < G; ++g) {
-      int cnt[2] = {0, 0};
+      size_t cnt = 0;
       for (size_t j = g; j < n; j += G)
-        if (i < seqs[j]->frames.size() && !seqs[j]->frames[i].show_existing) ++cnt[batch_class(seqs[j]->frames[i])];
-      for (int c = 0; c < 2; ++c)
-        if (cnt[c]) total += batch_table_bytes(cnt[c]);
+        if (i < seqs[j]->frames.size()) ++cnt;
+      if (cnt) total += step_table_bytes(cnt);
     }
   if (total > e0->batch_cap_) {
     cudaFree(e0->batch_d_);
@@ -1087,55 +1187,31 @@ rv9::Status Engine::run_batched(Engine* const* engines, const Sequence* const* s
   // Each group's stream starts after the start event on engines[0]'s.
   CK(cudaEventRecord(e0->ev0_, e0->stream_));
   for (size_t g = 1; g < G; ++g) CK(cudaStreamWaitEvent(engines[g]->stream_, e0->ev0_, 0));
-  std::vector<KFrame> ks;
-  std::vector<int> nb;
-  std::vector<DevFrame*> curs;
-  std::vector<size_t> who;
+  std::vector<Engine*> step_engines;
+  std::vector<const FrameWork*> step_fws;
+  std::vector<const uint8_t*> step_bases;
+  std::vector<DevFrame*> shown;
   size_t off = 0;
   int L = 0;
   for (size_t i = 0; i < most; ++i)
     for (size_t g = 0; g < G; ++g) {
-      cudaStream_t s = engines[g]->stream_;
-      for (int c = 0; c < 2; ++c) {
-        ks.clear();
-        nb.clear();
-        curs.clear();
-        who.clear();
-        for (size_t j = g; j < n; j += G) {
-          if (i >= seqs[j]->frames.size()) continue;
-          const FrameWork& fw = seqs[j]->frames[i];
-          if (fw.show_existing ? c != 0 : batch_class(fw) != c) continue;
-          KFrame k;
-          DevFrame* cur = nullptr;
-          rv9::Status st = engines[j]->prepare_frame(fw, seqs[j]->d_data, s, &k, &cur, err);
-          if (st != rv9::ST_OK) return st;
-          if (!cur) {
-            DevFrame* shown = nullptr;
-            engines[j]->commit_frame(fw, nullptr, &shown);
-            st = engines[j]->sink_frame(shown, s, err);
-            if (st != rv9::ST_OK) return st;
-            continue;
-          }
-          ks.push_back(k);
-          nb.push_back((int)fw.n_blocks);
-          curs.push_back(cur);
-          who.push_back(j);
-        }
-        if (ks.empty()) continue;
-        const int nf = (int)ks.size();
-        BatchTotals tot;
-        batch_fill(ks.data(), nb.data(), nf, e0->batch_h_ + off, &tot, e0->n_sm_, e0->batch_tune_);
-        const size_t bytes = batch_table_bytes(nf);
-        CK(cudaMemcpyAsync(e0->batch_d_ + off, e0->batch_h_ + off, bytes, cudaMemcpyHostToDevice, s));
-        CK(launch_batch(e0->batch_d_ + off, nf, tot, c == 1, s, e0->n_sm_, e0->batch_tune_, &L));
-        off += bytes;
-        for (int q = 0; q < nf; ++q) {
-          DevFrame* shown = nullptr;
-          engines[who[q]]->commit_frame(seqs[who[q]]->frames[i], curs[q], &shown);
-          rv9::Status st = engines[who[q]]->sink_frame(shown, s, err);
-          if (st != rv9::ST_OK) return st;
-        }
+      step_engines.clear();
+      step_fws.clear();
+      step_bases.clear();
+      for (size_t j = g; j < n; j += G) {
+        if (i >= seqs[j]->frames.size()) continue;
+        step_engines.push_back(engines[j]);
+        step_fws.push_back(&seqs[j]->frames[i]);
+        step_bases.push_back(seqs[j]->d_data);
       }
+      if (step_engines.empty()) continue;
+      shown.assign(step_engines.size(), nullptr);
+      size_t used = 0;
+      rv9::Status st = launch_step(step_engines.data(), step_fws.data(), step_bases.data(), step_engines.size(),
+                                   engines[g]->stream_, e0->batch_tune_, e0->batch_h_ + off, e0->batch_d_ + off,
+                                   &used, shown.data(), &L, err);
+      if (st != rv9::ST_OK) return st;
+      off += used;
     }
   // engines[0]'s stream waits for every group's end.
   for (size_t g = 1; g < G; ++g) {

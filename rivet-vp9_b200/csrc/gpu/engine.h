@@ -183,6 +183,29 @@ class Engine {
   // to the last completion.
   static rv9::Status run_batched(Engine* const* engines, const Sequence* const* seqs, size_t n, int groups,
                                  float* ms, std::string* err);
+  // One launch per stage for one frame of each of engines[0..n) (all
+  // distinct, on one device, frames independent of one another) on stream
+  // s: each frame's records are at bases[q] in device memory (ordered before
+  // on s). Frames are prepared, the batch tables filled at h_tables (pinned)
+  // and copied to d_tables (at least step_table_bytes(n) bytes each, not in
+  // use by earlier launches still running), the stages launched, the frames
+  // committed to their engines' slots and each engine's error word queued
+  // for copying back. shown[q] receives frame q's shown frame (or null); its
+  // pixels are final in stream order on s.
+  static rv9::Status launch_step(Engine* const* engines, const FrameWork* const* fws, const uint8_t* const* bases,
+                                 size_t n, cudaStream_t s, const TuneParams& tune, uint8_t* h_tables,
+                                 uint8_t* d_tables, size_t* table_bytes, DevFrame** shown, int* launches,
+                                 std::string* err);
+  static size_t step_table_bytes(size_t n);
+  // The host side of recon() without the launches: the frame's work lists
+  // built into this engine's pinned staging and copied to its device staging
+  // on stream s (*d_base: their device address; null for a shown existing
+  // frame). At most two frames staged this way may await their launches.
+  rv9::Status stage(const rv9::ParsedFrame& pf, cudaStream_t s, FrameWork* fw, const uint8_t** d_base,
+                    std::string* err);
+  // Copies the visible planes of `f`, packed, to `dst` (host or device
+  // memory) on stream `stream` (queued).
+  rv9::Status download_on(DevFrame* f, uint8_t* dst, cudaStream_t stream, std::string* err);
   // The autotuner for run_batched: times the batch with each number of
   // groups (1, 2, 4, 8, at most n) and each intra wavefront grain, and keeps
   // the fastest grain on engines[0], which run_batched then uses for batches
@@ -266,7 +289,6 @@ class Engine {
   void commit_frame(const FrameWork& fw, DevFrame* cur, DevFrame** shown);
   // The shown frame's copy into the sink, if one is set (queued on `stream`).
   rv9::Status sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err);
-  rv9::Status download_on(DevFrame* f, uint8_t* dst, cudaStream_t stream, std::string* err);
   // Loop-filter records and progress words for every frame of `seq`, so
   // that no frame of a run reallocates them.
   rv9::Status reserve_scratch(const Sequence& seq, std::string* err);

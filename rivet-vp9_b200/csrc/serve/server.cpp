@@ -2,12 +2,25 @@
 //
 // Each stream owns a host parser and a reconstruction engine (reference
 // slots, pooled frames, its own CUDA stream). Host workers take one request
-// at a time from streams that are ready, parse it, launch its frames'
-// reconstruction on the stream's CUDA stream and queue the copies of the
-// shown frames into pinned buffers; a host function queued after them on the
-// same CUDA stream completes the request. One stream is only ever worked on
-// by one worker at a time, so its requests complete in order, while requests
-// of different streams overlap on the device.
+// at a time from streams that are ready and parse it. Then, in the plain
+// form, the worker launches its frames' reconstruction on the stream's CUDA
+// stream and queues the copies of the shown frames into pinned buffers; a
+// host function queued after them on the same CUDA stream completes the
+// request. One stream is only ever worked on by one worker at a time, so its
+// requests complete in order, while requests of different streams overlap
+// on the device.
+//
+// In the batched form (rv9_engine_create_batched) the worker only stages the
+// parsed frames (work lists built and copied to the device) and hands them
+// to its stream's group. A launcher thread per group forms steps as frames
+// arrive: the next staged frame of every stream of the group that has one,
+// reconstructed together with one launch per stage (Engine::launch_step),
+// then the shown frames' copies and the completions, all on the group's CUDA
+// stream. A launcher keeps at most kStepsAhead steps queued on the device,
+// so that while the GPU is busy, frames arriving meanwhile join the next
+// step. Requests of a stream still complete in order (one CUDA stream per
+// group), and requests arriving while others are on the GPU join the next
+// step: continuous batching on the device.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -35,6 +48,8 @@ using Clock = std::chrono::steady_clock;
 constexpr int kReservedFrames = 10;  // eight slots, the frame being built, one spare
 constexpr int kOutBuffers = 4;       // pinned output buffers per stream
 constexpr int kMaxShown = 2;         // shown frames one request may carry
+constexpr int kStepsAhead = 2;       // batched form: steps queued on the device per group
+constexpr int kTableRing = kStepsAhead + 2;  // batch-table buffers per group
 
 struct OutBuf {
   uint8_t* data = nullptr;
@@ -59,6 +74,7 @@ struct Done {
   double submit_ms = 0, latency_ms = 0;
   int out = -1;  // index of the stream's output buffer, or -1
   uint32_t n_frames = 0;
+  size_t out_used = 0;  // bytes of the output buffer its frames fill
   rv9_frame frames[kMaxShown];
 };
 
@@ -74,6 +90,19 @@ struct Stream {
   bool needs_reset = false;  // a device error: reset the engine's scratch first
   int inflight = 0;          // requests launched, not yet completed
   std::deque<Request> queue;
+  // Batched form: the stream's group, its staged frames awaiting a step
+  // (in order; an entry without a frame only completes its request), and
+  // whether the group's launcher is using the stream's engine now.
+  int group = 0;
+  struct Staged {
+    bool has_frame = false;
+    rv9g::FrameWork fw;
+    const uint8_t* d_base = nullptr;
+    Done* done = nullptr;  // set on a request's last entry: completes it
+  };
+  std::deque<Staged> ready;
+  bool launching = false;
+  Done* open_done = nullptr;  // launcher: the request whose frames it is launching
   rv9::Parser parser;
   std::unique_ptr<rv9g::Engine> engine;
   std::vector<OutBuf> outs;
@@ -100,9 +129,58 @@ size_t packed_cap(const rv9_stream_spec& s) {
 
 }  // namespace
 
+namespace {
+
+// A group of the batched form: its CUDA stream, launcher thread and the
+// pinned / device batch tables of its steps in flight (a ring).
+struct Group {
+  cudaStream_t stream = nullptr;
+  std::thread launcher;
+  struct Tables {
+    uint8_t* h = nullptr;
+    uint8_t* d = nullptr;
+    size_t cap = 0;
+    cudaEvent_t done = nullptr;  // the step that last used them
+  } ring[kTableRing];
+  int next = 0;
+  cudaEvent_t step_done[kStepsAhead] = {};
+  int step = 0;
+  uint64_t steps = 0, frames = 0;  // statistics
+};
+
+// The rv9_frame of a shown frame whose packed planes go to `data`.
+void fill_frame(const rv9g::DevFrame* shown, uint8_t* data, size_t nb, rv9_frame* f) {
+  memset(f, 0, sizeof *f);
+  f->width = shown->width;
+  f->height = shown->height;
+  f->bit_depth = shown->bit_depth;
+  f->chroma = shown->ss_x ? (shown->ss_y ? RV9_YUV420 : RV9_YUV422) : (shown->ss_y ? RV9_YUV440 : RV9_YUV444);
+  f->color_space = shown->color_space;
+  f->full_range = shown->color_range;
+  f->render_width = shown->render_w;
+  f->render_height = shown->render_h;
+  f->data = data;
+  f->size = nb;
+  size_t poff = 0, bps = shown->bps();
+  for (int p = 0; p < 3; ++p) {
+    uint32_t w = p ? (shown->width + shown->ss_x) >> shown->ss_x : shown->width;
+    uint32_t h = p ? (shown->height + shown->ss_y) >> shown->ss_y : shown->height;
+    f->planes[p].offset = poff;
+    f->planes[p].width = w;
+    f->planes[p].height = h;
+    poff += (size_t)w * h * bps;
+  }
+}
+
+}  // namespace
+
 struct rv9_engine {
   int device = 0;
   uint64_t budget = 0, reserved = 0;
+  // Batched form: launch groups (empty in the plain form).
+  std::vector<std::unique_ptr<Group>> groups;
+  std::condition_variable ready_cv;
+  int next_group = 0;
   Clock::time_point t0 = Clock::now();
   std::mutex mu;
   std::condition_variable work_cv, done_cv, idle_cv;
@@ -112,6 +190,7 @@ struct rv9_engine {
   std::set<Done*> polled;  // handed out by rv9_poll, not yet released
   int64_t next_id = 1;
   bool stop = false;
+  bool stop_launchers = false;
   std::vector<std::thread> workers;
   size_t cursor = 0;
   uint64_t n_submitted = 0, n_completed = 0, n_frames = 0;
@@ -168,11 +247,15 @@ struct rv9_engine {
       auto& s = order[(cursor + k) % n];
       if (s->busy) continue;
       Action a = NONE;
+      // In the batched form a stream's next request is parsed once its
+      // staged frames have gone to the device (the engine's two staging
+      // buffers bound what may wait) and its launcher is done with it.
+      const bool staged_free = s->ready.empty() && !s->launching;
       if (s->state == ADMITTING)
         a = ADMIT;
-      else if (s->state == ACTIVE && !s->queue.empty() && !s->free_outs.empty())
+      else if (s->state == ACTIVE && !s->queue.empty() && !s->free_outs.empty() && staged_free)
         a = DECODE;
-      else if (s->state == ACTIVE && s->closing && s->queue.empty() && s->inflight == 0)
+      else if (s->state == ACTIVE && s->closing && s->queue.empty() && s->inflight == 0 && staged_free)
         a = CLOSE;
       if (a != NONE) {
         cursor = (cursor + k + 1) % n;
@@ -263,6 +346,7 @@ struct rv9_engine {
     if (ok) {
       s.engine = std::move(engine);
       for (int i = 0; i < (int)s.outs.size(); ++i) s.free_outs.push_back(i);
+      if (!groups.empty()) s.group = next_group++ % (int)groups.size();
       s.state = ACTIVE;
     } else {
       // Fail the stream's requests and drop it; its reservation returns.
@@ -300,8 +384,14 @@ struct rv9_engine {
     Stream& s = *sp;
     if (s.needs_reset) {
       std::string err;
+      // Nothing of the stream is in flight on its group's stream after this.
+      if (!groups.empty()) cudaStreamSynchronize(groups[(size_t)s.group]->stream);
       s.engine->sync(&err);  // reports the error once more and resets the scratch
       s.needs_reset = false;
+    }
+    if (!groups.empty()) {
+      stage_request(sp);
+      return;
     }
     Request req;
     int out;
@@ -345,26 +435,7 @@ struct rv9_engine {
         break;
       }
       rv9_frame& f = d->frames[d->n_frames++];
-      memset(&f, 0, sizeof f);
-      f.width = shown->width;
-      f.height = shown->height;
-      f.bit_depth = shown->bit_depth;
-      f.chroma = shown->ss_x ? (shown->ss_y ? RV9_YUV420 : RV9_YUV422) : (shown->ss_y ? RV9_YUV440 : RV9_YUV444);
-      f.color_space = shown->color_space;
-      f.full_range = shown->color_range;
-      f.render_width = shown->render_w;
-      f.render_height = shown->render_h;
-      f.data = s.outs[out].data + off;
-      f.size = nb;
-      size_t poff = 0, bps = shown->bps();
-      for (int p = 0; p < 3; ++p) {
-        uint32_t w = p ? (shown->width + shown->ss_x) >> shown->ss_x : shown->width;
-        uint32_t h = p ? (shown->height + shown->ss_y) >> shown->ss_y : shown->height;
-        f.planes[p].offset = poff;
-        f.planes[p].width = w;
-        f.planes[p].height = h;
-        poff += (size_t)w * h * bps;
-      }
+      fill_frame(shown, s.outs[out].data + off, nb, &f);
       rv9::Status s2 = s.engine->download_async(shown, f.data, &err);
       if (s2 != rv9::ST_OK) {
         d->status = (rv9_status)s2;
@@ -377,6 +448,230 @@ struct rv9_engine {
     std::lock_guard<std::mutex> lock(mu);
     s.busy = false;
     work_cv.notify_all();
+  }
+
+  // Batched form, worker side: parses the stream's next request and stages
+  // its frames for the group's launcher; the request's last entry carries
+  // its completion (alone, when parsing failed before any frame).
+  void stage_request(const std::shared_ptr<Stream>& sp) {
+    Stream& s = *sp;
+    Request req;
+    int out;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      req = std::move(s.queue.front());
+      s.queue.pop_front();
+      out = s.free_outs.back();
+      s.free_outs.pop_back();
+      s.inflight += 1;
+    }
+    Done* d = new Done;
+    d->stream = sp;
+    d->stream_id = s.id;
+    d->tag = req.tag;
+    d->submit_ms = req.submit_ms;
+    d->out = out;
+    std::vector<Stream::Staged> staged;
+    std::string err;
+    std::vector<std::pair<size_t, size_t>> frames;
+    rv9::superframe_split(req.packet.data(), req.packet.size(), &frames);
+    if (req.packet.empty()) {
+      d->status = RV9_BITSTREAM;
+      d->err = "empty packet";
+    }
+    const cudaStream_t gs = groups[(size_t)s.group]->stream;
+    rv9::ParsedFrame pf;
+    for (auto& fr : frames) {
+      rv9::Status st = s.parser.parse_frame(req.packet.data() + fr.first, fr.second, &pf, &err);
+      Stream::Staged it;
+      if (st == rv9::ST_OK) st = s.engine->stage(pf, gs, &it.fw, &it.d_base, &err);
+      if (st != rv9::ST_OK) {
+        d->status = (rv9_status)st;
+        d->err = err;
+        break;
+      }
+      it.has_frame = true;
+      staged.push_back(std::move(it));
+    }
+    if (staged.empty()) staged.emplace_back();
+    staged.back().done = d;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto& it : staged) s.ready.push_back(std::move(it));
+    s.busy = false;
+    work_cv.notify_all();
+    ready_cv.notify_all();
+  }
+
+  // Batched form, launcher side: one step at a time for group g.
+  void launcher_loop(int g) {
+    cudaSetDevice(device);
+    Group& G = *groups[(size_t)g];
+    std::vector<std::shared_ptr<Stream>> taken;
+    std::vector<Stream::Staged> items;
+    std::vector<rv9g::Engine*> engines;
+    std::vector<const rv9g::FrameWork*> fws;
+    std::vector<const uint8_t*> bases;
+    std::vector<rv9g::DevFrame*> shown;
+    std::vector<size_t> frame_of;  // item -> index in the step's frames, or -1
+    for (;;) {
+      // At most kStepsAhead steps queued: wait for the oldest to finish, so
+      // that frames arriving meanwhile join the next step.
+      cudaEventSynchronize(G.step_done[G.step]);
+      taken.clear();
+      items.clear();
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        ready_cv.wait(lock, [&] {
+          if (stop_launchers) return true;
+          for (auto& kv : streams)
+            if (kv.second->group == g && !kv.second->ready.empty() && !kv.second->launching) return true;
+          return false;
+        });
+        if (stop_launchers) return;
+        // The next staged entry of every stream of the group that has one.
+        for (auto& kv : streams) {
+          Stream& st = *kv.second;
+          if (st.group != g || st.ready.empty() || st.launching) continue;
+          st.launching = true;
+          taken.push_back(kv.second);
+          items.push_back(std::move(st.ready.front()));
+          st.ready.pop_front();
+        }
+      }
+      engines.clear();
+      fws.clear();
+      bases.clear();
+      frame_of.assign(items.size(), (size_t)-1);
+      for (size_t i = 0; i < items.size(); ++i) {
+        if (!items[i].has_frame) continue;
+        frame_of[i] = engines.size();
+        engines.push_back(taken[i]->engine.get());
+        fws.push_back(&items[i].fw);
+        bases.push_back(items[i].d_base);
+      }
+      std::string err;
+      rv9::Status st = rv9::ST_OK;
+      if (!engines.empty()) {
+        Group::Tables& tb = G.ring[G.next];
+        G.next = (G.next + 1) % kTableRing;
+        cudaEventSynchronize(tb.done);  // the step that used them last has finished
+        const size_t need = rv9g::Engine::step_table_bytes(engines.size());
+        if (need > tb.cap) {
+          cudaFree(tb.d);
+          cudaFreeHost(tb.h);
+          tb.d = tb.h = nullptr;
+          tb.cap = 0;
+          const size_t cap = std::max(need, (size_t)64 << 10);
+          if (cudaMalloc(&tb.d, cap) == cudaSuccess && cudaMallocHost(&tb.h, cap) == cudaSuccess) {
+            tb.cap = cap;
+          } else {
+            st = rv9::ST_DEVICE;
+            err = "out of memory for a step's batch tables";
+          }
+        }
+        shown.assign(engines.size(), nullptr);
+        if (st == rv9::ST_OK) {
+          size_t used = 0;
+          int launches = 0;
+          st = rv9g::Engine::launch_step(engines.data(), fws.data(), bases.data(), engines.size(), G.stream,
+                                         rv9g::TuneParams(), tb.h, tb.d, &used, shown.data(), &launches, &err);
+          cudaEventRecord(tb.done, G.stream);
+          G.steps += 1;
+          G.frames += engines.size();
+        }
+      }
+      // Shown frames to their requests' output buffers, then completions,
+      // in stream order behind the step.
+      for (size_t i = 0; i < items.size(); ++i) {
+        Stream& sm = *taken[i];
+        Done* d = items[i].done;
+        if (frame_of[i] != (size_t)-1) {
+          Done* owner = d ? d : pending_done(sm);
+          rv9g::DevFrame* f = st == rv9::ST_OK ? shown[frame_of[i]] : nullptr;
+          if (st != rv9::ST_OK && owner->status == RV9_OK) {
+            owner->status = (rv9_status)st;
+            owner->err = err;
+          }
+          if (f && owner->status == RV9_OK) place_frame(sm, owner, f, G.stream);
+        }
+        if (d) {
+          sm.open_done = nullptr;
+          complete_on(G.stream, d);
+        }
+      }
+      cudaEventRecord(G.step_done[G.step], G.stream);
+      G.step = (G.step + 1) % kStepsAhead;
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        for (auto& sp : taken) sp->launching = false;
+        work_cv.notify_all();
+        ready_cv.notify_all();
+      }
+      taken.clear();  // (streams may be freed once released)
+    }
+  }
+
+  // The Done of the stream's request whose frames are being launched (a
+  // request's entries before its last carry none): the last entry's, found
+  // ahead in the stream's ready queue.
+  Done* pending_done(Stream& s) {
+    if (s.open_done) return s.open_done;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto& it : s.ready)
+      if (it.done) {
+        s.open_done = it.done;
+        break;
+      }
+    return s.open_done;
+  }
+
+  // A shown frame's copy into its request's output buffer (queued on `gs`).
+  void place_frame(Stream& s, Done* d, rv9g::DevFrame* shown, cudaStream_t gs) {
+    const size_t nb = rv9g::Engine::packed_bytes(shown);
+    if (d->n_frames >= (uint32_t)kMaxShown || d->out_used + nb > s.outs[(size_t)d->out].cap) {
+      d->status = RV9_UNSUPPORTED;
+      d->err = "a request showed more frames, or larger ones, than its stream spec allows";
+      return;
+    }
+    rv9_frame& f = d->frames[d->n_frames++];
+    fill_frame(shown, s.outs[(size_t)d->out].data + d->out_used, nb, &f);
+    std::string err;
+    if (s.engine->download_on(shown, f.data, gs, &err) != rv9::ST_OK) {
+      d->status = RV9_DEVICE;
+      d->err = err;
+      return;
+    }
+    d->out_used += nb;
+  }
+
+  // Queues the completion behind the work on `gs`.
+  void complete_on(cudaStream_t gs, Done* d) {
+    Callback* cb = new Callback{this, d};
+    if (cudaLaunchHostFunc(gs, host_fn, cb) == cudaSuccess) return;
+    delete cb;
+    if (d->status == RV9_OK) {
+      d->status = RV9_DEVICE;
+      d->err = "could not queue the completion";
+    }
+    finish(d);
+  }
+
+  // Joins the launchers (stop_launchers set) and frees the groups' streams,
+  // events and tables.
+  void destroy_groups() {
+    for (auto& G : groups) {
+      if (G->launcher.joinable()) G->launcher.join();
+      if (G->stream) cudaStreamSynchronize(G->stream);
+      for (auto& tb : G->ring) {
+        cudaFree(tb.d);
+        cudaFreeHost(tb.h);
+        if (tb.done) cudaEventDestroy(tb.done);
+      }
+      for (auto& ev : G->step_done)
+        if (ev) cudaEventDestroy(ev);
+      if (G->stream) cudaStreamDestroy(G->stream);
+    }
+    groups.clear();
   }
 
   void worker_loop() {
@@ -403,7 +698,17 @@ extern "C" {
 
 uint64_t rv9_stream_reservation(const rv9_stream_spec* spec) { return spec ? reservation_of(*spec) : 0; }
 
+static rv9_engine* engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers, uint32_t n_groups);
+
 rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers) {
+  return engine_create(device, hbm_budget_bytes, workers, 0);
+}
+
+rv9_engine* rv9_engine_create_batched(int device, uint64_t hbm_budget_bytes, uint32_t workers, uint32_t groups) {
+  return engine_create(device, hbm_budget_bytes, workers, groups ? groups : 1);
+}
+
+static rv9_engine* engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers, uint32_t n_groups) {
   if (!rv9api::host_isa_ok()) return nullptr;
   {
     // The same device check as rv9_decoder_new, with its message.
@@ -418,6 +723,26 @@ rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t wo
   rv9_engine* e = new rv9_engine;
   e->device = device;
   e->budget = hbm_budget_bytes;
+  if (n_groups) {
+    cudaSetDevice(device);
+    for (uint32_t g = 0; g < n_groups; ++g) {
+      std::unique_ptr<Group> G(new Group);
+      bool ok = cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking) == cudaSuccess;
+      for (int i = 0; ok && i < kTableRing; ++i)
+        ok = cudaEventCreateWithFlags(&G->ring[i].done, cudaEventDisableTiming) == cudaSuccess;
+      for (int i = 0; ok && i < kStepsAhead; ++i)
+        ok = cudaEventCreateWithFlags(&G->step_done[i], cudaEventDisableTiming) == cudaSuccess;
+      e->groups.push_back(std::move(G));
+      if (!ok) {
+        rv9api::set_global_error("creating the launch groups' CUDA streams and events failed");
+        e->destroy_groups();
+        delete e;
+        return nullptr;
+      }
+    }
+    for (uint32_t g = 0; g < n_groups; ++g)
+      e->groups[g]->launcher = std::thread([e, g] { e->launcher_loop((int)g); });
+  }
   int n = workers ? (int)workers : (int)std::max(1u, std::thread::hardware_concurrency());
   for (int i = 0; i < n; ++i) e->workers.emplace_back([e] { e->worker_loop(); });
   return e;
@@ -457,6 +782,12 @@ void rv9_engine_free(rv9_engine* e) {
     dropped.clear();
   }
   for (auto& t : e->workers) t.join();
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    e->stop_launchers = true;
+    e->ready_cv.notify_all();
+  }
+  e->destroy_groups();
   for (Done* d : e->done) delete d;
   delete e;
 }
@@ -570,6 +901,10 @@ void rv9_engine_get_stats(rv9_engine* e, rv9_engine_stats* out) {
   out->frames_decoded = e->n_frames;
   out->reserved_bytes = e->reserved;
   out->budget_bytes = e->budget;
+  for (auto& G : e->groups) {
+    out->batched_steps += G->steps;
+    out->batched_frames += G->frames;
+  }
 }
 
 }  // extern "C"

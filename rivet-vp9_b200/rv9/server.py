@@ -27,11 +27,13 @@ class CCompletion(ctypes.Structure):
 class CEngineStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("streams_open", "streams_pending", "requests_submitted",
                                               "requests_completed", "frames_decoded", "reserved_bytes",
-                                              "budget_bytes")]
+                                              "budget_bytes", "batched_steps", "batched_frames")]
 
 
-EXPORTS = ("rv9_engine_create", "rv9_engine_free", "rv9_stream_reservation", "rv9_stream_open", "rv9_stream_close",
-           "rv9_submit", "rv9_poll", "rv9_completion_release", "rv9_engine_get_stats")
+EXPORTS = ("rv9_engine_create", "rv9_engine_create_batched", "rv9_engine_free", "rv9_stream_reservation", "rv9_stream_open", "rv9_stream_close",
+           "rv9_submit", "rv9_poll", "rv9_completion_release", "rv9_engine_get_stats", "rv9_cluster_create",
+           "rv9_cluster_free", "rv9_cluster_stream_open", "rv9_cluster_stream_close", "rv9_cluster_submit",
+           "rv9_cluster_poll", "rv9_cluster_completion_release", "rv9_cluster_get_stats", "rv9_place_least_loaded")
 
 
 def _bind(lib):
@@ -40,6 +42,8 @@ def _bind(lib):
     vp = ctypes.c_void_p
     lib.rv9_engine_create.restype = vp
     lib.rv9_engine_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32]
+    lib.rv9_engine_create_batched.restype = vp
+    lib.rv9_engine_create_batched.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
     lib.rv9_engine_free.argtypes = [vp]
     lib.rv9_stream_reservation.restype = ctypes.c_uint64
     lib.rv9_stream_reservation.argtypes = [ctypes.POINTER(CStreamSpec)]
@@ -50,6 +54,20 @@ def _bind(lib):
     lib.rv9_poll.argtypes = [vp, ctypes.POINTER(CCompletion), ctypes.c_size_t, ctypes.c_int]
     lib.rv9_completion_release.argtypes = [vp, ctypes.POINTER(CCompletion)]
     lib.rv9_engine_get_stats.argtypes = [vp, ctypes.POINTER(CEngineStats)]
+    lib.rv9_cluster_create.restype = vp
+    lib.rv9_cluster_create.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint32]
+    lib.rv9_cluster_free.argtypes = [vp]
+    lib.rv9_cluster_stream_open.argtypes = [vp, ctypes.POINTER(CStreamSpec), ctypes.POINTER(ctypes.c_int64),
+                                            ctypes.POINTER(ctypes.c_int)]
+    lib.rv9_cluster_stream_close.argtypes = [vp, ctypes.c_int64]
+    lib.rv9_cluster_submit.argtypes = [vp, ctypes.c_int64, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint64]
+    lib.rv9_cluster_poll.restype = ctypes.c_size_t
+    lib.rv9_cluster_poll.argtypes = [vp, ctypes.POINTER(CCompletion), ctypes.c_size_t, ctypes.c_int]
+    lib.rv9_cluster_completion_release.argtypes = [vp, ctypes.POINTER(CCompletion)]
+    lib.rv9_cluster_get_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CEngineStats)]
+    lib.rv9_place_least_loaded.restype = ctypes.c_int
+    lib.rv9_place_least_loaded.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                           ctypes.c_size_t, ctypes.c_uint64]
     lib._rv9_server_bound = True
     return lib
 
@@ -70,12 +88,11 @@ class Completion:
     """A finished request. `frames` holds Frame objects copied out of the
     engine's pinned buffers, which go back to the stream at once."""
 
-    def __init__(self, c, frames, md5s=None):
+    def __init__(self, c, frames):
         self.stream, self.tag, self.status = c.stream, c.tag, c.status
         self.submit_ms, self.latency_ms = c.submit_ms, c.latency_ms
         self.n_frames = c.n_frames
         self.frames = frames
-        self.md5s = md5s  # hex MD5 of each frame's packed planes, when asked for
 
     @property
     def ok(self):
@@ -83,9 +100,16 @@ class Completion:
 
 
 class Engine:
-    def __init__(self, device=-1, hbm_budget=120 << 30, workers=0, lib_path=None):
+    """A serving engine (rv9_engine). `groups` > 0 makes the batched form
+    (rv9_engine_create_batched): the streams' frames reconstructed together,
+    one launch per stage per step, in that many launch groups."""
+
+    def __init__(self, device=-1, hbm_budget=120 << 30, workers=0, lib_path=None, groups=0):
         self._lib = _bind(load_library(lib_path))
-        self._e = self._lib.rv9_engine_create(device, hbm_budget, workers)
+        if groups:
+            self._e = self._lib.rv9_engine_create_batched(device, hbm_budget, workers, groups)
+        else:
+            self._e = self._lib.rv9_engine_create(device, hbm_budget, workers)
         if not self._e:
             raise DeviceError(self._lib.rv9_last_global_error().decode(errors="replace"))
 
@@ -107,22 +131,18 @@ class Engine:
         if st != RV9_OK:
             raise _ERRORS.get(st, Rv9Error)(f"rv9_submit: status {st}")
 
-    def poll(self, max_items=64, timeout_ms=0, keep_frames=True, digest=None):
-        """Finished requests; with keep_frames False only their metadata is
-        kept (the frames are not copied out). `digest(tag)` -> True asks for
-        the MD5 of that request's frames, hashed in place in the engine's
-        buffer before it is released (Completion.md5s)."""
-        import hashlib
+    def poll(self, max_items=64, timeout_ms=0, keep_frames=True):
+        """Finished requests. keep_frames: True copies every request's frames
+        out of the engine's buffers (Completion.frames), False none, or a
+        predicate on the request's tag picks the requests whose frames are
+        copied."""
         arr = (CCompletion * max_items)()
         n = self._lib.rv9_poll(self._e, arr, max_items, timeout_ms)
         out = []
         for c in arr[:n]:
-            frames = [Frame(c.frames[i]) for i in range(c.n_frames)] if keep_frames else []
-            md5s = None
-            if digest is not None and digest(c.tag) and c.status == RV9_OK:
-                md5s = [hashlib.md5(memoryview((ctypes.c_char * c.frames[i].size).from_address(
-                    ctypes.cast(c.frames[i].data, ctypes.c_void_p).value))).hexdigest() for i in range(c.n_frames)]
-            out.append(Completion(c, frames, md5s))
+            keep = keep_frames(c.tag) if callable(keep_frames) else keep_frames
+            frames = [Frame(c.frames[i]) for i in range(c.n_frames)] if keep else []
+            out.append(Completion(c, frames))
             self._lib.rv9_completion_release(self._e, ctypes.byref(c))
         return out
 
@@ -135,6 +155,75 @@ class Engine:
         if getattr(self, "_e", None):
             self._lib.rv9_engine_free(self._e)
             self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def place_least_loaded(load, budget, need, lib_path=None):
+    """The cluster's placement rule (rv9_place_least_loaded), no device
+    needed: the index of the device a stream of `need` bytes goes to, given
+    each device's reserved bytes and budget; -1 when none could hold it."""
+    lib = _bind(load_library(lib_path))
+    n = len(load)
+    a = (ctypes.c_uint64 * n)(*load)
+    b = (ctypes.c_uint64 * n)(*budget)
+    return lib.rv9_place_least_loaded(a, b, n, need)
+
+
+class Cluster:
+    """A serving engine per device (rv9_cluster): each stream placed whole on
+    the least loaded device by reserved bytes; one poll for all devices."""
+
+    def __init__(self, devices, hbm_budget=120 << 30, workers=0, lib_path=None):
+        self._lib = _bind(load_library(lib_path))
+        arr = (ctypes.c_int * len(devices))(*devices)
+        self._c = self._lib.rv9_cluster_create(arr, len(devices), hbm_budget, workers)
+        if not self._c:
+            raise DeviceError(self._lib.rv9_last_global_error().decode(errors="replace"))
+        self.n_devices = len(devices)
+
+    def open_stream(self, width, height, bit_depth=8, chroma=(1, 1)):
+        """Returns (stream id, device ordinal it was placed on)."""
+        s = spec(width, height, bit_depth, chroma)
+        sid, dev = ctypes.c_int64(), ctypes.c_int()
+        st = self._lib.rv9_cluster_stream_open(self._c, ctypes.byref(s), ctypes.byref(sid), ctypes.byref(dev))
+        if st != RV9_OK:
+            raise _ERRORS.get(st, Rv9Error)(f"rv9_cluster_stream_open: status {st}")
+        return sid.value, dev.value
+
+    def close_stream(self, sid):
+        st = self._lib.rv9_cluster_stream_close(self._c, sid)
+        if st != RV9_OK:
+            raise _ERRORS.get(st, Rv9Error)(f"rv9_cluster_stream_close: status {st}")
+
+    def submit(self, sid, packet, tag=0):
+        st = self._lib.rv9_cluster_submit(self._c, sid, packet, len(packet), tag)
+        if st != RV9_OK:
+            raise _ERRORS.get(st, Rv9Error)(f"rv9_cluster_submit: status {st}")
+
+    def poll(self, max_items=64, timeout_ms=0, keep_frames=True):
+        arr = (CCompletion * max_items)()
+        n = self._lib.rv9_cluster_poll(self._c, arr, max_items, timeout_ms)
+        out = []
+        for c in arr[:n]:
+            frames = [Frame(c.frames[i]) for i in range(c.n_frames)] if keep_frames else []
+            out.append(Completion(c, frames))
+            self._lib.rv9_cluster_completion_release(self._c, ctypes.byref(c))
+        return out
+
+    def stats(self, device_index):
+        s = CEngineStats()
+        self._lib.rv9_cluster_get_stats(self._c, device_index, ctypes.byref(s))
+        return {n: getattr(s, n) for n, _ in CEngineStats._fields_}
+
+    def close(self):
+        if getattr(self, "_c", None):
+            self._lib.rv9_cluster_free(self._c)
+            self._c = None
 
     def __del__(self):
         try:

@@ -7,13 +7,15 @@ tests/data/README.md); the reference decoder passes all of them
 (tests/committed_vectors.rs). They are copied byte for byte so that the tests
 can run where the reference tree is not mounted.
 
-Usage: python tests/golden/copy_vectors.py [/path/to/rivet-vp9]
+Usage: python tests/golden/copy_vectors.py /path/to/rivet-vp9
 """
 import os
 import shutil
 import sys
 
-src = os.path.join(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", "tests", "data")
+if len(sys.argv) != 2:
+    sys.exit("usage: copy_vectors.py /path/to/rivet-vp9 (a checkout of the reference project)")
+src = os.path.join(sys.argv[1], "tests", "data")
 dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "vectors")
 os.makedirs(dst, exist_ok=True)
 n = 0

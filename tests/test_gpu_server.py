@@ -1,7 +1,9 @@
 """The serving engine (include/rv9_server.h): each stream's frames are the
 same in the mix as alone (the published MD5s), requests complete in order
 per stream, admission waits for the HBM budget, and a bad packet fails only
-its own request."""
+its own request. Every test runs on the plain engine (each stream on its own
+CUDA stream) and on the batched one (rv9_engine_create_batched: the streams'
+frames reconstructed together, one launch per stage per step)."""
 import hashlib
 import os
 import time
@@ -24,6 +26,11 @@ MIX = [
 ]
 
 
+@pytest.fixture(params=[0, 1, 3], ids=["plain", "batched_1group", "batched_3groups"])
+def groups(request):
+    return request.param
+
+
 def _drain(eng, expect, timeout_s=120):
     got = []
     t0 = time.time()
@@ -36,9 +43,9 @@ def _md5s(done, sid):
     return [hashlib.md5(f.packed()).hexdigest() for c in done if c.stream == sid for f in c.frames]
 
 
-def test_mix_equals_alone():
+def test_mix_equals_alone(groups):
     from rv9 import server
-    eng = server.Engine(0, workers=8)
+    eng = server.Engine(0, workers=8, groups=groups)
     try:
         sids, packets = {}, {}
         for name, bd in MIX:
@@ -64,14 +71,18 @@ def test_mix_equals_alone():
         st = eng.stats()
         assert st["streams_open"] == 0 and st["reserved_bytes"] == 0
         assert st["requests_completed"] == st["requests_submitted"] == total
+        if groups:
+            # Every reconstructed frame went through a step (steps of one
+            # frame or more, as the frames arrived).
+            assert 0 < st["batched_steps"] <= st["batched_frames"]
     finally:
         eng.close()
 
 
-def test_admission_waits_for_the_budget():
+def test_admission_waits_for_the_budget(groups):
     from rv9 import server
     one = server.reservation(1920, 1080, 12, (0, 0))
-    eng = server.Engine(0, hbm_budget=int(one * 1.5), workers=4)
+    eng = server.Engine(0, hbm_budget=int(one * 1.5), workers=4, groups=groups)
     try:
         names = MIX[:3]
         sids = [eng.open_stream(1920, 1080, bit_depth=12, chroma=(0, 0)) for _ in names]
@@ -93,10 +104,10 @@ def test_admission_waits_for_the_budget():
         eng.close()
 
 
-def test_spec_over_budget_is_refused():
+def test_spec_over_budget_is_refused(groups):
     import rv9
     from rv9 import server
-    eng = server.Engine(0, hbm_budget=1 << 20, workers=1)
+    eng = server.Engine(0, hbm_budget=1 << 20, workers=1, groups=groups)
     try:
         with pytest.raises(rv9.UnsupportedError):
             eng.open_stream(1920, 1080)
@@ -104,10 +115,10 @@ def test_spec_over_budget_is_refused():
         eng.close()
 
 
-def test_a_bad_packet_fails_only_its_request():
+def test_a_bad_packet_fails_only_its_request(groups):
     from rv9 import server
     name = "vp90-2-02-size-130x132.webm"
-    eng = server.Engine(0, workers=4)
+    eng = server.Engine(0, workers=4, groups=groups)
     try:
         good = eng.open_stream(352, 288)
         bad = eng.open_stream(352, 288)
@@ -126,10 +137,10 @@ def test_a_bad_packet_fails_only_its_request():
         eng.close()
 
 
-def test_free_with_requests_in_flight():
+def test_free_with_requests_in_flight(groups):
     # Freeing the engine drains every stream, with completions never polled.
     from rv9 import server
-    eng = server.Engine(0, workers=2)
+    eng = server.Engine(0, workers=2, groups=groups)
     sid = eng.open_stream(352, 288)
     for i, p in enumerate(read_packets(os.path.join(VECTORS_DIR, "vp90-2-02-size-130x132.webm"))):
         eng.submit(sid, p, tag=i)
