@@ -264,6 +264,21 @@ void rv9_decoder_set_frame_sink(rv9_decoder* dec, uint8_t* buf, size_t cap);
 /* Frames and bytes the sink holds, and frames dropped for want of room. */
 void rv9_decoder_frame_sink_state(const rv9_decoder* dec, uint64_t* frames, size_t* bytes, uint64_t* dropped);
 
+/* On-device frame digests (no counterpart in the reference, whose tests hash
+ * Frame::packed() on the host, tests/common/mod.rs:151): while on, the MD5 of
+ * every frame the decoder shows — of the bytes rv9_frame data would hold — is
+ * computed on the GPU from the frame's device planes, for up to `cap_frames`
+ * frames, and nothing but the 16-byte digests is read back. Shown frames of
+ * the same calls as the frame sink's are covered. 0 turns it off; each call
+ * starts the list empty. The digest of a frame is a serial chain of 64-byte
+ * blocks (about 40 ms for a 1080p 8-bit frame on one warp), so this is a
+ * checking aid, not a throughput path. */
+rv9_status rv9_decoder_set_frame_digests(rv9_decoder* dec, size_t cap_frames);
+/* Copies the digests computed so far (16 bytes each, in show order) into
+ * `out` (room for `cap` of them); returns how many there are. Call after the
+ * decode or run call that showed the frames has returned. */
+size_t rv9_decoder_frame_digests(rv9_decoder* dec, uint8_t* out, size_t cap);
+
 /* The frame in reference slot `slot` (0..7), packed like rv9_frame data. */
 rv9_status rv9_decoder_download_slot(rv9_decoder* dec, int slot, uint8_t* out, size_t cap, size_t* bytes);
 

@@ -29,6 +29,7 @@ SOURCES = [
 HEADERS = [
     "api/api_internal.h",
     "gpu/dsp_math.cuh",
+    "gpu/md5.cuh",
     "gpu/engine_types.h",
     "gpu/engine.h",
     "host/parser.h",

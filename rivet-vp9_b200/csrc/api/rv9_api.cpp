@@ -430,6 +430,16 @@ void rv9_decoder_set_frame_sink(rv9_decoder* d, uint8_t* buf, size_t cap) {
   if (d) d->engine.set_sink(buf, buf ? cap : 0);
 }
 
+rv9_status rv9_decoder_set_frame_digests(rv9_decoder* d, size_t cap_frames) {
+  if (!d) return RV9_INVALID_INPUT;
+  return (rv9_status)d->engine.set_digests(cap_frames, &d->err);
+}
+
+size_t rv9_decoder_frame_digests(rv9_decoder* d, uint8_t* out, size_t cap) {
+  if (!d || (!out && cap)) return 0;
+  return d->engine.digests(out, cap);
+}
+
 void rv9_decoder_frame_sink_state(const rv9_decoder* d, uint64_t* frames, size_t* bytes, uint64_t* dropped) {
   if (frames) *frames = d ? d->engine.sink_frames() : 0;
   if (bytes) *bytes = d ? d->engine.sink_used() : 0;

@@ -65,6 +65,7 @@ Engine::~Engine() {
   if (stream_) cudaStreamDestroy(stream_);
   cudaFree(batch_d_);
   cudaFreeHost(batch_h_);
+  cudaFree(d_digest_);
 }
 
 bool Engine::init(int device, std::string* err) {
@@ -108,7 +109,7 @@ bool Engine::init(int device, std::string* err) {
   for (int a = 0; a < 4; ++a)
     for (int b = 0; b < 16; ++b)
       for (int c = 0; c < 8; ++c) f[a][b][c] = (int16_t)vp9t_subpel_filters[a][b][c];
-  if ((e = upload_filters(&f[0][0][0])) != cudaSuccess) {
+  if ((e = upload_filters(&f[0][0][0])) != cudaSuccess || (e = upload_md5_table()) != cudaSuccess) {
     *err = std::string("loading the kernels: ") + cudaGetErrorString(e);
     return false;
   }
@@ -676,8 +677,57 @@ rv9::Status Engine::download_async(DevFrame* f, uint8_t* dst, std::string* err) 
   return download_on(f, dst, stream_, err);
 }
 
-rv9::Status Engine::sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err) {
-  if (!sink_ || !shown || capturing_) return rv9::ST_OK;
+void Engine::digest_add(DevFrame* f, Md5Jobs* jobs, int* n) {
+  if (!d_digest_ || digest_n_ >= digest_cap_) return;
+  Md5Job& j = jobs->job[(*n)++];
+  const size_t bps = f->bps();
+  for (int p = 0; p < 3; ++p) {
+    j.plane[p] = (const uint8_t*)f->planes[p];
+    j.stride[p] = (int64_t)f->stride[p] * (int64_t)bps;
+    j.row_bytes[p] = (uint32_t)((p ? (f->width + f->ss_x) >> f->ss_x : f->width) * bps);
+    j.rows[p] = p ? (f->height + f->ss_y) >> f->ss_y : f->height;
+  }
+  j.out = d_digest_ + 16 * digest_n_++;
+}
+
+rv9::Status Engine::set_digests(size_t cap, std::string* err) {
+  if (d_digest_) {
+    CK(cudaDeviceSynchronize());
+    cudaFree(d_digest_);
+    d_digest_ = nullptr;
+  }
+  digest_cap_ = 0;
+  digest_n_ = 0;
+  if (cap) {
+    CK(cudaMalloc(&d_digest_, cap * 16));
+    digest_cap_ = cap;
+  }
+  return rv9::ST_OK;
+}
+
+size_t Engine::digests(uint8_t* out, size_t cap) const {
+  const size_t n = std::min(cap, digest_n_);
+  if (n && d_digest_ && cudaMemcpy(out, d_digest_, n * 16, cudaMemcpyDefault) != cudaSuccess) return 0;
+  return digest_n_;
+}
+
+rv9::Status Engine::sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err, Md5Jobs* jobs, int* n_jobs) {
+  if (!shown || capturing_) return rv9::ST_OK;
+  if (d_digest_) {
+    if (jobs) {
+      digest_add(shown, jobs, n_jobs);
+      if (*n_jobs == kMd5JobsPerLaunch) {
+        CK(launch_md5(*jobs, *n_jobs, stream));
+        *n_jobs = 0;
+      }
+    } else {
+      Md5Jobs one;
+      int n = 0;
+      digest_add(shown, &one, &n);
+      CK(launch_md5(one, n, stream));
+    }
+  }
+  if (!sink_) return rv9::ST_OK;
   const size_t nb = packed_bytes(shown);
   if (sink_used_ + nb > sink_cap_) {
     ++sink_dropped_;
@@ -1044,6 +1094,8 @@ rv9::Status Engine::launch_step(Engine* const* engines, const FrameWork* const* 
                                 uint8_t* d_tables, size_t* table_bytes, DevFrame** shown, int* launches,
                                 std::string* err) {
   *table_bytes = 0;
+  Md5Jobs jobs;
+  int n_jobs = 0;
   std::vector<KFrame> ks;
   std::vector<int> nb;
   std::vector<DevFrame*> curs;
@@ -1066,7 +1118,7 @@ rv9::Status Engine::launch_step(Engine* const* engines, const FrameWork* const* 
       if (st != rv9::ST_OK) return st;
       if (!cur) {
         e->commit_frame(fw, nullptr, &shown[q]);
-        st = e->sink_frame(shown[q], s, err);
+        st = e->sink_frame(shown[q], s, err, &jobs, &n_jobs);
         if (st != rv9::ST_OK) return st;
         continue;
       }
@@ -1088,10 +1140,11 @@ rv9::Status Engine::launch_step(Engine* const* engines, const FrameWork* const* 
       e->commit_frame(*fws[who[f]], curs[f], &shown[who[f]]);
       // The frame's error word, for sync() and error_word().
       CK(cudaMemcpyAsync(e->h_error_ + 1, e->d_counters_ + 2, 4, cudaMemcpyDeviceToHost, s));
-      rv9::Status st = e->sink_frame(shown[who[f]], s, err);
+      rv9::Status st = e->sink_frame(shown[who[f]], s, err, &jobs, &n_jobs);
       if (st != rv9::ST_OK) return st;
     }
   }
+  CK(launch_md5(jobs, n_jobs, s));
   return rv9::ST_OK;
 }
 

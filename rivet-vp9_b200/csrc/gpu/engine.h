@@ -42,6 +42,23 @@ cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm
                          void* hook_ctx, const TuneParams& tune = TuneParams(), const LaunchAux* aux = nullptr);
 cudaError_t upload_filters(const int16_t* f);
 
+// On-device MD5 of frames (k_md5_frames): one job per frame, its packed
+// planes read from the strided device planes, the 16-byte digest written to
+// `out` (device memory). At most kMd5JobsPerLaunch jobs per launch.
+struct Md5Job {
+  const uint8_t* plane[3];
+  int64_t stride[3];       // bytes
+  uint32_t row_bytes[3];   // packed row: width x bytes per sample
+  uint32_t rows[3];
+  uint8_t* out;
+};
+constexpr int kMd5JobsPerLaunch = 32;
+struct Md5Jobs {
+  Md5Job job[kMd5JobsPerLaunch];
+};
+cudaError_t upload_md5_table();
+cudaError_t launch_md5(const Md5Jobs& jobs, int n, cudaStream_t s);
+
 // Per-device kernel set-up: the shared-memory opt-ins of the wavefront
 // kernels and the batched launches' occupancy on that device. Once per
 // device (thread-safe), with `device` current; Engine::init calls it.
@@ -261,6 +278,12 @@ class Engine {
     sink_dropped_ = 0;
   }
   size_t sink_used() const { return sink_used_; }
+  // On-device digests: while on (cap > 0), the MD5 of every frame the
+  // engine shows (as the sink would copy it) is computed on the GPU into a
+  // device array of `cap` entries; digests() copies them out once the run
+  // that showed them has returned.
+  rv9::Status set_digests(size_t cap, std::string* err);
+  size_t digests(uint8_t* out, size_t cap) const;
   uint64_t sink_frames() const { return sink_frames_; }
   uint64_t sink_dropped() const { return sink_dropped_; }
 
@@ -287,8 +310,11 @@ class Engine {
   rv9::Status prepare_frame(const FrameWork& fw, const uint8_t* d_base, cudaStream_t stream, KFrame* k,
                             DevFrame** cur, std::string* err);
   void commit_frame(const FrameWork& fw, DevFrame* cur, DevFrame** shown);
-  // The shown frame's copy into the sink, if one is set (queued on `stream`).
-  rv9::Status sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err);
+  // The shown frame's copy into the sink and its digest, when they are on
+  // (queued on `stream`). With `jobs`, the digest joins those jobs (the
+  // caller launches them); without, it is launched at once.
+  rv9::Status sink_frame(DevFrame* shown, cudaStream_t stream, std::string* err, Md5Jobs* jobs = nullptr,
+                         int* n_jobs = nullptr);
   // Loop-filter records and progress words for every frame of `seq`, so
   // that no frame of a run reallocates them.
   rv9::Status reserve_scratch(const Sequence& seq, std::string* err);
@@ -331,6 +357,10 @@ class Engine {
   uint8_t* fixed_ = nullptr;  // the fixed scratch, during sequence_run_fixed
   uint8_t* sink_ = nullptr;
   size_t sink_cap_ = 0, sink_used_ = 0;
+  uint8_t* d_digest_ = nullptr;
+  size_t digest_cap_ = 0, digest_n_ = 0;
+  // Digest jobs of shown frames queued on a stream, launched together.
+  void digest_add(DevFrame* f, Md5Jobs* jobs, int* n);
   uint64_t sink_frames_ = 0, sink_dropped_ = 0;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   // run_batched's launch shapes and tables (pinned host, device), on the

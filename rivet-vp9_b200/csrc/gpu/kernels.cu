@@ -37,6 +37,7 @@
 #include <mutex>
 
 #include "dsp_math.cuh"
+#include "md5.cuh"
 #include "engine.h"
 #include "engine_types.h"
 
@@ -708,6 +709,17 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
 // ---------------------------------------------------------------------------
 // Loop filter wavefront.
 
+// The line filter the loop-filter kernels run: lf_line_select (the three
+// filters as independent chains, one result kept), or lf_line's branches
+// when built with RV9_LF_BRANCHES (kept for comparison).
+__device__ __forceinline__ void lf_line_kernel(int* s, int fs, int limit, int blimit, int thresh, int bd) {
+#ifdef RV9_LF_BRANCHES
+  lf_line(s, fs, limit, blimit, thresh, bd);
+#else
+  lf_line_select(s, fs, limit, blimit, thresh, bd);
+#endif
+}
+
 constexpr int kLfW = 80;   // tile row pitch (int16): 8 left + 64 + 8 of slack
 constexpr int kLfH = 72;   // 8 above + 64
 
@@ -801,13 +813,13 @@ __device__ __forceinline__ void lf_row_regs(int16_t* line, const LfEdge (*e)[16]
       if (f.fs >= 0) {
         int* sw = &v[4 * ed];
         if (4 * ed + 16 <= 72) {
-          lf_line(sw, f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line_kernel(sw, f.fs, f.limit, f.blimit, f.thresh, bd);
         } else {
           // The last edges' windows reach past the tile: only p3..q3 matter.
           int s[16];
 #pragma unroll
           for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < 72) ? v[4 * ed + q] : 0;
-          lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line_kernel(s, f.fs, f.limit, f.blimit, f.thresh, bd);
 #pragma unroll
           for (int q = 0; q < 16; ++q)
             if (4 * ed + q < 72) v[4 * ed + q] = s[q];
@@ -847,12 +859,12 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
       LfEdge f = e[ed][run];
       if (f.fs >= 0) {
         if (4 * ed + 16 <= 72) {
-          lf_line(&v[4 * ed], f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line_kernel(&v[4 * ed], f.fs, f.limit, f.blimit, f.thresh, bd);
         } else {
           int s[16];
 #pragma unroll
           for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < 72) ? v[4 * ed + q] : 0;
-          lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line_kernel(s, f.fs, f.limit, f.blimit, f.thresh, bd);
 #pragma unroll
           for (int q = 0; q < 16; ++q)
             if (4 * ed + q < 72) v[4 * ed + q] = s[q];
@@ -1604,6 +1616,88 @@ cudaError_t launch_frame(const KFrame& k, int n_blocks, cudaStream_t s, int n_sm
   if (k.bit_depth > 8)
     return launch_frame_t<uint16_t, L64>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune, aux);
   return launch_frame_t<uint8_t, L32>(k, n_blocks, s, n_sm, launches, hook, hook_ctx, tune, aux);
+}
+
+// ---------------------------------------------------------------------------
+// On-device MD5 of shown frames: the digest of the packed planes (the bytes
+// of the reference's Frame::packed()) computed from the frame's strided
+// device planes, one warp per frame. MD5 is a chain of 64-byte blocks, so a
+// frame's lanes gather the next 32 blocks of the byte stream (data, then the
+// RFC 1321 padding) into shared memory together, and lane 0 runs the
+// compression over them.
+
+__constant__ uint32_t c_md5_t[64];
+
+cudaError_t upload_md5_table() {
+  uint32_t t[64];
+  md5_sine_table(t);
+  return cudaMemcpyToSymbol(c_md5_t, t, sizeof t);
+}
+
+constexpr int kMd5Lanes = 32;
+
+__global__ void __launch_bounds__(kMd5Lanes) k_md5_frames(Md5Jobs jobs) {
+  __shared__ uint32_t words[kMd5Lanes * 16];
+  const Md5Job& j = jobs.job[blockIdx.x];
+  const int lane = threadIdx.x;
+  uint64_t plane_len[3], len = 0;
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    plane_len[p] = (uint64_t)j.row_bytes[p] * j.rows[p];
+    len += plane_len[p];
+  }
+  const uint64_t total = md5_padded_bytes(len);
+  Md5State h;
+  md5_init(&h);
+  for (uint64_t pos = 0; pos < total; pos += 64 * kMd5Lanes) {
+    const uint64_t k0 = pos + 64 * (uint64_t)lane;
+    if (k0 < total) {
+      // The byte stream's cursor at k0: plane, row, column.
+      int p = 0;
+      uint64_t r = k0;
+      while (p < 2 && r >= plane_len[p]) r -= plane_len[p++];
+      uint32_t row = 0, col = 0;
+      if (k0 < len) {
+        row = (uint32_t)(r / j.row_bytes[p]);
+        col = (uint32_t)(r - (uint64_t)row * j.row_bytes[p]);
+      }
+      for (int q = 0; q < 16; ++q) {
+        uint32_t w = 0;
+        for (int b = 0; b < 4; ++b) {
+          const uint64_t k = k0 + 4 * q + b;
+          uint32_t v;
+          if (k < len) {
+            v = __ldg(j.plane[p] + (uint64_t)row * j.stride[p] + col);
+            if (++col == j.row_bytes[p]) {
+              col = 0;
+              if (++row == j.rows[p] && p < 2) {
+                row = 0;
+                ++p;
+              }
+            }
+          } else {
+            v = md5_pad_byte(k, len);
+          }
+          w |= v << (8 * b);
+        }
+        words[lane * 16 + q] = w;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const uint64_t left = (total - pos) / 64;
+      const int nb = left < (uint64_t)kMd5Lanes ? (int)left : kMd5Lanes;
+      for (int b = 0; b < nb; ++b) md5_block(&h, &words[b * 16], c_md5_t);
+    }
+    __syncwarp();
+  }
+  if (lane == 0) md5_digest(h, j.out);
+}
+
+cudaError_t launch_md5(const Md5Jobs& jobs, int n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_md5_frames<<<n, kMd5Lanes, 0, s>>>(jobs);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

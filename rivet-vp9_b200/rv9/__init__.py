@@ -74,7 +74,8 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_sequence_record_bytes", "rv9_sequence_free", "rv9_sequence_clone", "rv9_decoder_download_slot", "rv9_kernel_stats",
            "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_sequences_run_batched", "rv9_sequences_autotune_batched", "rv9_decoder_autotune",
            "rv9_sequences_autotune", "rv9_decoder_set_event_mask", "rv9_decoder_threads", "rv9_decoder_set_wait_limit",
-           "rv9_decoder_set_test_fault", "rv9_decoder_set_frame_sink", "rv9_decoder_frame_sink_state")
+           "rv9_decoder_set_test_fault", "rv9_decoder_set_frame_sink", "rv9_decoder_frame_sink_state",
+           "rv9_decoder_set_frame_digests", "rv9_decoder_frame_digests")
 
 
 class CTuneResult(ctypes.Structure):
@@ -144,6 +145,9 @@ def load_library(path=None):
     lib.rv9_decoder_set_frame_sink.argtypes = [vp, vp, ctypes.c_size_t]
     lib.rv9_decoder_frame_sink_state.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_size_t),
                                                  ctypes.POINTER(ctypes.c_uint64)]
+    lib.rv9_decoder_set_frame_digests.argtypes = [vp, ctypes.c_size_t]
+    lib.rv9_decoder_frame_digests.restype = ctypes.c_size_t
+    lib.rv9_decoder_frame_digests.argtypes = [vp, vp, ctypes.c_size_t]
     lib.rv9_decoder_threads.restype = ctypes.c_uint32
     lib.rv9_decoder_threads.argtypes = [vp]
     lib.rv9_decoder_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
@@ -440,6 +444,19 @@ class Decoder:
         """Every frame shown from now on is copied, packed, to `cap` bytes at
         address `ptr` (host or device memory); ptr 0 turns the sink off."""
         self._lib.rv9_decoder_set_frame_sink(self._dec, ptr or None, cap if ptr else 0)
+
+    def set_frame_digests(self, cap_frames):
+        """On-device MD5 of every frame shown from now on (up to cap_frames;
+        0 turns it off)."""
+        st = self._lib.rv9_decoder_set_frame_digests(self._dec, cap_frames)
+        if st != RV9_OK:
+            _raise(self._lib, self._dec, st)
+
+    def frame_digests(self, cap=1 << 16):
+        """The hex MD5s computed on the device so far, in show order."""
+        buf = ctypes.create_string_buffer(16 * cap)
+        n = self._lib.rv9_decoder_frame_digests(self._dec, buf, cap)
+        return [buf.raw[16 * i:16 * i + 16].hex() for i in range(min(n, cap))]
 
     def frame_sink_state(self):
         """(frames, bytes, dropped) of the frame sink."""

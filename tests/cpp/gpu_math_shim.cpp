@@ -11,6 +11,7 @@
 #include "../../include/rv9_records.h"
 
 #include "../../rivet-vp9_b200/csrc/gpu/dsp_math.cuh"
+#include "../../rivet-vp9_b200/csrc/gpu/md5.cuh"
 
 using namespace rv9g;
 
@@ -95,6 +96,13 @@ void shim_lf(uint16_t* buf, int filter_size, int limit, int blimit, int thresh, 
   int s[16];
   for (int i = 0; i < 16; ++i) s[i] = buf[i];
   lf_line(s, filter_size, limit, blimit, thresh, bd);
+  for (int i = 0; i < 16; ++i) buf[i] = (uint16_t)s[i];
+}
+
+void shim_lf_select(uint16_t* buf, int filter_size, int limit, int blimit, int thresh, int bd) {
+  int s[16];
+  for (int i = 0; i < 16; ++i) s[i] = buf[i];
+  lf_line_select(s, filter_size, limit, blimit, thresh, bd);
   for (int i = 0; i < 16; ++i) buf[i] = (uint16_t)s[i];
 }
 
@@ -186,4 +194,27 @@ extern "C" void shim_lf_frame(const rv9_frame_desc* d, const rv9_block* blocks, 
             if (gy >= 0 && gx >= 0 && (r >= 8 || c >= 8)) planes[p][(size_t)gy * stride[p] + gx] = (uint16_t)px[p][r][c];
           }
     }
+}
+
+// The device MD5's steps on the host: data in 64-byte blocks, then the
+// padding, exactly as the frame digest kernel sequences them.
+extern "C" void shim_md5(const uint8_t* data, uint64_t len, uint8_t* out) {
+  uint32_t t[64];
+  md5_sine_table(t);
+  Md5State h;
+  md5_init(&h);
+  const uint64_t total = md5_padded_bytes(len);
+  for (uint64_t pos = 0; pos < total; pos += 64) {
+    uint32_t w[16];
+    for (int q = 0; q < 16; ++q) {
+      uint32_t v = 0;
+      for (int b = 0; b < 4; ++b) {
+        const uint64_t k = pos + 4 * q + b;
+        v |= (uint32_t)(k < len ? data[k] : md5_pad_byte(k, len)) << (8 * b);
+      }
+      w[q] = v;
+    }
+    md5_block(&h, w, t);
+  }
+  md5_digest(h, out);
 }

@@ -20,8 +20,9 @@ SHIM = os.path.join(REPO, "tests", "cpp", "_build", "libgpumath_shim.so")
 @pytest.fixture(scope="module")
 def libs(oracle_lib):
     os.makedirs(os.path.dirname(SHIM), exist_ok=True)
-    hdr = os.path.join(REPO, "rivet-vp9_b200", "csrc", "gpu", "dsp_math.cuh")
-    if not os.path.exists(SHIM) or max(os.path.getmtime(SHIM_SRC), os.path.getmtime(hdr)) > os.path.getmtime(SHIM):
+    hdrs = [os.path.join(REPO, "rivet-vp9_b200", "csrc", "gpu", h) for h in ("dsp_math.cuh", "md5.cuh")]
+    if not os.path.exists(SHIM) or max([os.path.getmtime(SHIM_SRC)] + [os.path.getmtime(h) for h in hdrs]) > \
+            os.path.getmtime(SHIM):
         subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", SHIM_SRC, "-o", SHIM], check=True)
     return oracle_lib.lib(), ctypes.CDLL(SHIM)
 
@@ -105,10 +106,12 @@ def test_loop_filter_lines(libs):
         if sharp:
             limit = min(limit, 9 - sharp)
         blimit, thresh = 2 * (lvl + 2) + limit, lvl >> 4
-        a, b = line.copy(), line.copy()
+        a, b, c = line.copy(), line.copy(), line.copy()
         o.rv9o_test_lf(P(a), fs, limit, blimit, thresh, bd)
         s.shim_lf(P(b), fs, limit, blimit, thresh, bd)
+        s.shim_lf_select(P(c), fs, limit, blimit, thresh, bd)
         assert np.array_equal(a, b), (fs, bd)
+        assert np.array_equal(a, c), ("select", fs, bd)
 
 
 def _lf_case(libs, rng, w, h, ss_x, ss_y, bd):
@@ -165,3 +168,17 @@ def test_loop_filter_frames(libs):
         bd = [8, 10, 12][i % 3]
         changed += _lf_case(libs, rng, w, h, ss[0], ss[1], bd)
     assert changed > 0
+
+
+def test_frame_digest_md5_matches_hashlib(libs):
+    # The on-device frame digest's MD5 steps (csrc/gpu/md5.cuh, RFC 1321)
+    # against Python's hashlib, at every padding boundary and on random data.
+    import hashlib
+    _, s = libs
+    rng = np.random.default_rng(5)
+    lengths = [0, 1, 3, 55, 56, 57, 63, 64, 65, 119, 120, 127, 128, 129, 1000, 4095, 4096, 4097, 100003]
+    for n in lengths:
+        data = rng.integers(0, 256, n, dtype=np.uint8)
+        out = np.zeros(16, np.uint8)
+        s.shim_md5(P(data), ctypes.c_uint64(n), P(out))
+        assert bytes(out).hex() == hashlib.md5(data.tobytes()).hexdigest(), n
