@@ -58,7 +58,7 @@ typedef struct rv9_frame_desc {
   uint8_t legacy_uv;              /* pre-final profile 1 stream rules */
   uint8_t frame_is_intra;
   uint8_t show_frame;
-  uint8_t reserved0;
+  uint8_t tile_cols_log2;         /* tile columns: 1 << tile_cols_log2 */
   int32_t base_q_idx;
   int32_t delta_q_y_dc, delta_q_uv_dc, delta_q_uv_ac;
   uint8_t lf_level, lf_sharpness, lf_delta_enabled, reserved1;

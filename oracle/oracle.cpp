@@ -29,6 +29,7 @@
 #include <chrono>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../include/rv9.h"
@@ -926,10 +927,22 @@ struct FrameRecon {
     *n_runs_out = n_runs;
   }
 
-  void filter_frame(const std::vector<MiLf>& mi) {
+  // The planes are filtered independently (each in the reference's order),
+  // on their own threads when `threads` > 1.
+  void filter_frame(const std::vector<MiLf>& mi, int threads = 1) {
     lf_setup();
+    if (threads > 1) {
+      std::thread t[3];
+      for (int plane = 0; plane < 3; ++plane) t[plane] = std::thread([&, plane] { filter_plane(mi, plane); });
+      for (auto& x : t) x.join();
+    } else {
+      for (int plane = 0; plane < 3; ++plane) filter_plane(mi, plane);
+    }
+  }
+
+  void filter_plane(const std::vector<MiLf>& mi, int plane) {
     Edges e;
-    for (int plane = 0; plane < 3; ++plane) {
+    {
       Plane& buf = cur.planes[plane];
       int stride = buf.stride;
       for (uint32_t row = 0; row < d.mi_rows; row += 8)
@@ -960,6 +973,53 @@ struct Decoder {
   std::shared_ptr<Picture> slots[8];
   std::string err;
   double recon_seconds = 0;
+  int threads = 1;  // tile columns reconstructed, and planes filtered, at once
+
+  // Replays the frame's blocks, each tile column on its own thread when
+  // threads > 1, as the reference decodes tile columns in parallel
+  // (src/decoder/block.rs:1768-1863): a column reads nothing of another.
+  bool replay_columns(const rv9::ParsedFrame& pf, Picture& pic) {
+    const rv9_frame_desc& d = pf.desc;
+    const uint32_t cols = 1u << d.tile_cols_log2;
+    auto make = [&](FrameRecon* fr) {
+      if (!d.frame_is_intra)
+        for (int i = 0; i < 3; ++i) fr->refs[i] = slots[pf.ref_slot[i]].get();
+    };
+    if (threads <= 1 || cols <= 1) {
+      FrameRecon fr(d, pic);
+      make(&fr);
+      return fr.replay(pf.blocks.data(), pf.blocks.size(), pf.toks.data(), pf.toks.size(), pf.coefs.data(), &err);
+    }
+    // Blocks of each column, in bitstream order. A column starts at
+    // get_tile_offset (spec 6.4.1): ((c * sb64_cols) >> log2) superblocks.
+    auto col_start = [&](uint32_t c) { return std::min<uint32_t>(((c * d.sb64_cols) >> d.tile_cols_log2) * 8, d.mi_cols); };
+    std::vector<std::vector<rv9_block>> by_col(cols);
+    for (const rv9_block& b : pf.blocks) {
+      uint32_t c = 0;
+      while (c + 1 < cols && b.mi_col >= col_start(c + 1)) ++c;
+      by_col[c].push_back(b);
+    }
+    std::vector<std::string> errs(cols);
+    std::vector<char> ok(cols, 1);
+    std::vector<std::thread> pool;
+    const uint32_t workers = std::min<uint32_t>(cols, (uint32_t)threads);
+    for (uint32_t w = 0; w < workers; ++w)
+      pool.emplace_back([&, w] {
+        for (uint32_t c = w; c < cols; c += workers) {
+          FrameRecon fr(d, pic);
+          make(&fr);
+          ok[c] = fr.replay(by_col[c].data(), by_col[c].size(), pf.toks.data(), pf.toks.size(), pf.coefs.data(),
+                            &errs[c]);
+        }
+      });
+    for (auto& t : pool) t.join();
+    for (uint32_t c = 0; c < cols; ++c)
+      if (!ok[c]) {
+        err = errs[c];
+        return false;
+      }
+    return true;
+  }
 
   rv9_status decode_frame(const uint8_t* data, size_t len, std::vector<std::shared_ptr<Picture>>* shown) {
     rv9::ParsedFrame pf;
@@ -988,11 +1048,8 @@ struct Decoder {
       pic->planes[p].stride = pw;
       pic->planes[p].height = ph;
     }
+    if (!replay_columns(pf, *pic)) return RV9_BITSTREAM;
     FrameRecon fr(d, *pic);
-    if (!d.frame_is_intra)
-      for (int i = 0; i < 3; ++i) fr.refs[i] = slots[pf.ref_slot[i]].get();
-    if (!fr.replay(pf.blocks.data(), pf.blocks.size(), pf.toks.data(), pf.toks.size(), pf.coefs.data(), &err))
-      return RV9_BITSTREAM;
     if (d.lf_level != 0) {
       std::vector<MiLf> mi((size_t)d.mi_rows * d.mi_cols);
       for (const rv9_block& b : pf.blocks) {
@@ -1002,7 +1059,7 @@ struct Decoder {
         for (uint32_t y = b.mi_row; y < std::min(b.mi_row + bh, d.mi_rows); ++y)
           for (uint32_t x = b.mi_col; x < std::min(b.mi_col + bw, d.mi_cols); ++x) mi[(size_t)y * d.mi_cols + x] = m;
       }
-      fr.filter_frame(mi);
+      fr.filter_frame(mi, threads);
     }
     recon_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int i = 0; i < 8; ++i)
@@ -1070,7 +1127,10 @@ struct rv9o_decoder {
 
 rv9o_decoder* rv9o_decoder_new(void) { return new rv9o_decoder; }
 void rv9o_decoder_free(rv9o_decoder* d) { delete d; }
-void rv9o_decoder_set_threads(rv9o_decoder* d, uint32_t t) { d->dec.parser.set_threads((int)t); }
+void rv9o_decoder_set_threads(rv9o_decoder* d, uint32_t t) {
+  d->dec.parser.set_threads((int)t);
+  d->dec.threads = t ? (int)t : (int)std::max(1u, std::thread::hardware_concurrency());
+}
 void rv9o_decoder_set_max_pixels(rv9o_decoder* d, uint64_t p) { d->dec.parser.set_max_pixels(p); }
 uint64_t rv9o_decoder_frames_decoded(const rv9o_decoder* d) { return d->dec.parser.frames_decoded(); }
 const char* rv9o_last_error(const rv9o_decoder* d) { return d->dec.err.c_str(); }

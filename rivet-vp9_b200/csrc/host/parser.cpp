@@ -590,6 +590,7 @@ static void fill_desc(const FrameHeader& h, const Persistent& st, const SlotInfo
   d->legacy_uv = h.legacy_uv;
   d->frame_is_intra = h.frame_is_intra;
   d->show_frame = h.show_frame;
+  d->tile_cols_log2 = (uint8_t)h.tile_cols_log2;
   d->base_q_idx = h.base_q_idx;
   d->delta_q_y_dc = h.delta_q_y_dc;
   d->delta_q_uv_dc = h.delta_q_uv_dc;

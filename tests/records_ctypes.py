@@ -13,7 +13,7 @@ class FrameDesc(ctypes.Structure):
                 ("mi_rows", ctypes.c_uint32), ("sb64_cols", ctypes.c_uint32), ("sb64_rows", ctypes.c_uint32),
                 ("ss_x", ctypes.c_uint8), ("ss_y", ctypes.c_uint8), ("bit_depth", ctypes.c_uint8),
                 ("lossless", ctypes.c_uint8), ("legacy_uv", ctypes.c_uint8), ("frame_is_intra", ctypes.c_uint8),
-                ("show_frame", ctypes.c_uint8), ("reserved0", ctypes.c_uint8), ("base_q_idx", ctypes.c_int32),
+                ("show_frame", ctypes.c_uint8), ("tile_cols_log2", ctypes.c_uint8), ("base_q_idx", ctypes.c_int32),
                 ("delta_q_y_dc", ctypes.c_int32), ("delta_q_uv_dc", ctypes.c_int32), ("delta_q_uv_ac", ctypes.c_int32),
                 ("lf_level", ctypes.c_uint8), ("lf_sharpness", ctypes.c_uint8), ("lf_delta_enabled", ctypes.c_uint8),
                 ("reserved1", ctypes.c_uint8), ("lf_ref_deltas", ctypes.c_int8 * 4), ("lf_mode_deltas", ctypes.c_int8 * 2),
