@@ -467,58 +467,6 @@ RV9_HD void lf_line(int* s, int filter_size, int limit, int blimit, int thresh, 
     lf_wide<4>(s);
 }
 
-// lf_line without branches between its filters: the narrow, 8-wide and
-// 16-wide results are all computed from the unfiltered samples and the one
-// the masks choose is kept. The same samples come out as from lf_line. On
-// the GPU the three computations are independent chains that one warp
-// issues interleaved, where lf_line's branches (taken differently by the
-// lines of a warp) run them one after another.
-RV9_HD void lf_line_select(int* s, int filter_size, int limit, int blimit, int thresh, int bd) {
-  const int q0 = s[8], q1 = s[9], q2 = s[10], q3 = s[11];
-  const int p0 = s[7], p1 = s[6], p2 = s[5], p3 = s[4];
-  const int sh = bd - 8, one = 1 << sh;
-  const int ap1 = iabs(p1 - p0), aq1 = iabs(q1 - q0);
-  const int m = imax(imax(imax(iabs(p3 - p2), iabs(p2 - p1)), imax(ap1, aq1)), imax(iabs(q2 - q1), iabs(q3 - q2)));
-  const bool mask = m <= (limit << sh) && iabs(p0 - q0) * 2 + (iabs(p1 - q1) >> 1) <= (blimit << sh);
-  const bool hev = imax(ap1, aq1) > (thresh << sh);
-  const bool flat = filter_size >= 1 && imax(imax(ap1, aq1), imax(imax(iabs(p2 - p0), iabs(q2 - q0)),
-                                                                  imax(iabs(p3 - p0), iabs(q3 - q0)))) <= one;
-  const bool flat2 = filter_size >= 2 &&
-                     imax(imax(imax(iabs(s[3] - p0), iabs(s[2] - p0)), imax(iabs(s[1] - p0), iabs(s[0] - p0))),
-                          imax(imax(iabs(s[12] - q0), iabs(s[13] - q0)), imax(iabs(s[14] - q0), iabs(s[15] - q0)))) <=
-                         one;
-  // Narrow filter (spec 8.8.5.2).
-  const int lo = -(1 << (bd - 1)), hi = (1 << (bd - 1)) - 1;
-  const int off = 0x80 << sh;
-  const int ps1 = p1 - off, ps0 = p0 - off, qs0 = q0 - off, qs1 = q1 - off;
-  int f = hev ? iclamp(ps1 - qs1, lo, hi) : 0;
-  f = iclamp(f + 3 * (qs0 - ps0), lo, hi);
-  const int f1 = iclamp(f + 4, lo, hi) >> 3, f2 = iclamp(f + 3, lo, hi) >> 3;
-  const int g = (f1 + 1) >> 1;
-  const int n6 = hev ? p1 : iclamp(ps1 + g, lo, hi) + off;
-  const int n7 = iclamp(ps0 + f2, lo, hi) + off;
-  const int n8 = iclamp(qs0 - f1, lo, hi) + off;
-  const int n9 = hev ? q1 : iclamp(qs1 - g, lo, hi) + off;
-  // The wide filters on copies of the line.
-  int w8[16], w16[16];
-#pragma unroll
-  for (int t = 0; t < 16; ++t) w8[t] = w16[t] = s[t];
-  lf_wide<3>(w8);
-  lf_wide<4>(w16);
-  const bool use16 = mask && flat && flat2, use8 = mask && flat && !flat2, use4 = mask && !flat;
-#pragma unroll
-  for (int t = 1; t < 15; ++t) {
-    int v = s[t];
-    if (t >= 5 && t <= 10) v = use8 ? w8[t] : v;
-    v = use16 ? w16[t] : v;
-    if (t == 6) v = use4 ? n6 : v;
-    if (t == 7) v = use4 ? n7 : v;
-    if (t == 8) v = use4 ? n8 : v;
-    if (t == 9) v = use4 ? n9 : v;
-    s[t] = v;
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Loop filter edge decisions (reference superblock(),
 // src/decoder/loopfilter.rs:466-620), one (edge, run) entry at a time.
@@ -657,7 +605,7 @@ RV9_HD void lf_vertical_row(int16_t* line, const LfEdge (*e)[16], int n_edges, i
     int s[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) s[q] = w[q];
-    lf_line_select(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+    lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
 #pragma unroll
     for (int q = 1; q < 15; ++q) w[q] = (int16_t)s[q];
   }
@@ -676,7 +624,7 @@ RV9_HD void lf_horizontal_col(int16_t* col, int pitch, int rows, const LfEdge (*
     int s[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) s[q] = q < avail ? w[q * pitch] : 0;
-    lf_line_select(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+    lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
 #pragma unroll
     for (int q = 1; q < 15; ++q)
       if (q < avail) w[q * pitch] = (int16_t)s[q];

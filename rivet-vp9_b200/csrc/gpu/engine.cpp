@@ -29,14 +29,6 @@ const char* const kKernelNames[K_COUNT] = {"k_prep", "k_inter", "k_inter_res", "
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-// The weight of a superblock's row in the intra work list's anti-diagonal
-// order (column + weight x row); RV9_INTRA_ROW_WEIGHT=2 builds the earlier,
-// more conservative order for comparison.
-#ifdef RV9_INTRA_ROW_WEIGHT
-constexpr int kIntraRowWeight = RV9_INTRA_ROW_WEIGHT;
-#else
-constexpr int kIntraRowWeight = 1;
-#endif
 
 // Waits, when it goes out of scope, for the streams of engines[0..n): a run
 // over several engines' streams that returns early (an error part-way
@@ -234,13 +226,13 @@ bool Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageRe
     const bool avail_l = b.flags & RV9_BLK_AVAIL_L, avail_u = b.flags & RV9_BLK_AVAIL_U;
     const int bsize = std::max<int>(b.mi_size, BLOCK_8X8);
     const int nrefs = b.ref_frame[1] > INTRA_FRAME ? 2 : 1;
-    // Superblock anti-diagonal (column + row): every superblock an intra
-    // block reads from lies on an earlier one. Its edges come from the
-    // superblocks left, above and above-left only: the above-right samples
-    // it reads stop at its own block's right edge (reference
-    // src/decoder/recon.rs:57-66, not_on_right), so no superblock to the
-    // above-right is read.
-    const uint16_t diag = (uint16_t)((b.mi_col >> 3) + kIntraRowWeight * (b.mi_row >> 3));
+    // Superblock anti-diagonal (column + 2 row): every superblock an intra
+    // block reads from (left, above, above-left; its above-right samples
+    // stop at its own block's right edge, src/decoder/recon.rs:57-66) lies
+    // on an earlier one. Column + row would also be safe, and measured 5 %
+    // slower: it hands out the jobs of superblocks farther down before
+    // those of the rows above them are done.
+    const uint16_t diag = (uint16_t)((b.mi_col >> 3) + 2 * (b.mi_row >> 3));
     uint32_t tok = b.tok_start;
     for (int plane = 0; plane < 3; ++plane) {
       int tx_sz = plane ? uv_tx_size(d, b) : b.tx_size;
@@ -309,7 +301,7 @@ bool Engine::build_work(const rv9::ParsedFrame& pf, FrameWork* fw, const StageRe
                     pf.coefs.size() * 4 + ref_bytes + area;
   // Intra items by anti-diagonal: a counting sort, stable.
   if (!intra_.empty()) {
-    size_t n_diag = (size_t)(d.sb64_cols + kIntraRowWeight * d.sb64_rows) + 1;
+    size_t n_diag = (size_t)(d.sb64_cols + 2 * d.sb64_rows) + 1;
     diag_start_.assign(n_diag + 1, 0);
     for (uint16_t g : intra_diag_) ++diag_start_[g + 1];
     for (size_t g = 0; g < n_diag; ++g) diag_start_[g + 1] += diag_start_[g];

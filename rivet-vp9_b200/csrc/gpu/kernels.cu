@@ -709,17 +709,6 @@ __global__ void __launch_bounds__(32 * kIntraWarps) k_intra(KFrame k) {
 // ---------------------------------------------------------------------------
 // Loop filter wavefront.
 
-// The line filter the loop-filter kernels run: lf_line_select (the three
-// filters as independent chains, one result kept), or lf_line's branches
-// when built with RV9_LF_BRANCHES (kept for comparison).
-__device__ __forceinline__ void lf_line_kernel(int* s, int fs, int limit, int blimit, int thresh, int bd) {
-#ifdef RV9_LF_BRANCHES
-  lf_line(s, fs, limit, blimit, thresh, bd);
-#else
-  lf_line_select(s, fs, limit, blimit, thresh, bd);
-#endif
-}
-
 constexpr int kLfW = 80;   // tile row pitch (int16): 8 left + 64 + 8 of slack
 constexpr int kLfH = 72;   // 8 above + 64
 
@@ -813,13 +802,13 @@ __device__ __forceinline__ void lf_row_regs(int16_t* line, const LfEdge (*e)[16]
       if (f.fs >= 0) {
         int* sw = &v[4 * ed];
         if (4 * ed + 16 <= 72) {
-          lf_line_kernel(sw, f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line(sw, f.fs, f.limit, f.blimit, f.thresh, bd);
         } else {
           // The last edges' windows reach past the tile: only p3..q3 matter.
           int s[16];
 #pragma unroll
           for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < 72) ? v[4 * ed + q] : 0;
-          lf_line_kernel(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
 #pragma unroll
           for (int q = 0; q < 16; ++q)
             if (4 * ed + q < 72) v[4 * ed + q] = s[q];
@@ -859,12 +848,12 @@ __device__ __forceinline__ void lf_col_regs(int16_t* col, const LfEdge (*e)[16],
       LfEdge f = e[ed][run];
       if (f.fs >= 0) {
         if (4 * ed + 16 <= 72) {
-          lf_line_kernel(&v[4 * ed], f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line(&v[4 * ed], f.fs, f.limit, f.blimit, f.thresh, bd);
         } else {
           int s[16];
 #pragma unroll
           for (int q = 0; q < 16; ++q) s[q] = (4 * ed + q < 72) ? v[4 * ed + q] : 0;
-          lf_line_kernel(s, f.fs, f.limit, f.blimit, f.thresh, bd);
+          lf_line(s, f.fs, f.limit, f.blimit, f.thresh, bd);
 #pragma unroll
           for (int q = 0; q < 16; ++q)
             if (4 * ed + q < 72) v[4 * ed + q] = s[q];

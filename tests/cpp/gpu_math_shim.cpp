@@ -99,12 +99,6 @@ void shim_lf(uint16_t* buf, int filter_size, int limit, int blimit, int thresh, 
   for (int i = 0; i < 16; ++i) buf[i] = (uint16_t)s[i];
 }
 
-void shim_lf_select(uint16_t* buf, int filter_size, int limit, int blimit, int thresh, int bd) {
-  int s[16];
-  for (int i = 0; i < 16; ++i) s[i] = buf[i];
-  lf_line_select(s, filter_size, limit, blimit, thresh, bd);
-  for (int i = 0; i < 16; ++i) buf[i] = (uint16_t)s[i];
-}
 
 }  // extern "C"
 

@@ -106,12 +106,10 @@ def test_loop_filter_lines(libs):
         if sharp:
             limit = min(limit, 9 - sharp)
         blimit, thresh = 2 * (lvl + 2) + limit, lvl >> 4
-        a, b, c = line.copy(), line.copy(), line.copy()
+        a, b = line.copy(), line.copy()
         o.rv9o_test_lf(P(a), fs, limit, blimit, thresh, bd)
         s.shim_lf(P(b), fs, limit, blimit, thresh, bd)
-        s.shim_lf_select(P(c), fs, limit, blimit, thresh, bd)
         assert np.array_equal(a, b), (fs, bd)
-        assert np.array_equal(a, c), ("select", fs, bd)
 
 
 def _lf_case(libs, rng, w, h, ss_x, ss_y, bd):
