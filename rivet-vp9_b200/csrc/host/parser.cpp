@@ -521,6 +521,7 @@ struct FrameState {
   SlotInfo slots[8];
   std::shared_ptr<std::vector<uint8_t>> prev_segment_ids = std::make_shared<std::vector<uint8_t>>();
   std::shared_ptr<std::vector<PrevMv>> prev_mvs = std::make_shared<std::vector<PrevMv>>();
+  bool prev_external = false;  // the last frame's vectors are held by an external tile parser
   bool have_last_size = false;
   uint32_t last_w = 0, last_h = 0;
   bool last_show_frame = false;
@@ -542,6 +543,9 @@ struct Parser::Job {
   bool ref_ok[3] = {true, true, true};
   std::shared_ptr<std::vector<uint8_t>> prev_seg;
   std::shared_ptr<std::vector<PrevMv>> prev_mvs;  // set when the frame uses them
+  bool use_prev = false;       // the frame reads the previous frame's vectors
+  bool prev_external = false;  // ... and an external tile parser holds them
+  bool external = false;       // the tiles were parsed outside (finish_external)
   const uint8_t* tiles = nullptr;
   size_t tiles_len = 0;
   bool non420 = false;
@@ -695,7 +699,9 @@ Parser::Job* Parser::begin(const uint8_t* data, size_t len, const AfterHeader& a
     parse_compressed(data + comp_start, h.header_size_in_bytes, h, job->probs);
     job->seg = S.st.seg;
     job->prev_seg = S.prev_segment_ids;
-    if (use_prev && S.prev_mvs->size() >= mi_len) job->prev_mvs = S.prev_mvs;
+    job->prev_external = S.prev_external;
+    job->use_prev = use_prev && (S.prev_external || S.prev_mvs->size() >= mi_len);
+    if (job->use_prev && !S.prev_external) job->prev_mvs = S.prev_mvs;
     job->tiles = data + comp_end;
     job->tiles_len = len - comp_end;
     job->non420 = !(h.ss_x == 1 && h.ss_y == 1);
@@ -733,6 +739,13 @@ Parser::Job* Parser::begin(const uint8_t* data, size_t len, const AfterHeader& a
 
 void Parser::run(Job* job) {
   if (job->st != ST_OK || job->show_existing) return;
+  if (job->use_prev && !job->prev_mvs) {
+    // The previous frame's vectors are held by an external parser and were
+    // not handed over (provide_prev_mvs).
+    job->tr.st = ST_INVALID_INPUT;
+    job->tr.err = "previous motion vectors held by the device parser were not provided";
+    return;
+  }
   auto t0 = std::chrono::steady_clock::now();
   const FrameHeader& h = job->h;
   TileWork& W = *job->work;
@@ -814,7 +827,6 @@ Status Parser::finish(Job* job, ParsedFrame* out, std::string* err) {
     return ST_OK;
   }
   const FrameHeader& h = job->h;
-  TileWork& W = *job->work;
   if (h.frame_is_intra) {
     // The layout the probe settled on carries to the inter frames that
     // follow, whether or not the tiles parsed.
@@ -827,12 +839,31 @@ Status Parser::finish(Job* job, ParsedFrame* out, std::string* err) {
     FrameState now = S;
     S = job->snap;
     S.prev_mvs = now.prev_mvs;
+    S.prev_external = now.prev_external;
     if (!h.frame_is_intra) S.legacy_uv = now.legacy_uv;
     *err = job->tr.err.empty() ? "bitstream error" : job->tr.err;
     return job->tr.st;
   }
   if (h.frame_is_intra) S.legacy_uv = job->h.legacy_uv;
   size_t mi_len = (size_t)h.mi_rows * h.mi_cols;
+  if (job->external) {
+    // Nothing of the frame adapts or segments (external_tiles); its motion
+    // vectors stay with the external parser.
+    S.prev_mvs = std::make_shared<std::vector<PrevMv>>();
+    S.prev_external = true;
+    out->show_existing = false;
+    out->show_frame = job->out.show_frame;
+    out->refresh_mask = job->out.refresh_mask;
+    for (int i = 0; i < 3; ++i) out->ref_slot[i] = job->out.ref_slot[i];
+    out->desc = job->out.desc;
+    out->blocks.clear();
+    out->toks.clear();
+    out->coefs.clear();
+    out->parse_seconds = 0;
+    ++frames_;
+    return ST_OK;
+  }
+  TileWork& W = *job->work;
   // Backward adaptation (refresh_probs, 6.1.2).
   if (job->late_ctx) {
     Counts counts;
@@ -866,6 +897,7 @@ Status Parser::finish(Job* job, ParsedFrame* out, std::string* err) {
     p.mv[1] = m.mv[1][3];
   }
   S.prev_mvs = mvs;
+  S.prev_external = false;
   out->show_existing = false;
   out->show_frame = job->out.show_frame;
   out->refresh_mask = job->out.refresh_mask;
@@ -880,6 +912,39 @@ Status Parser::finish(Job* job, ParsedFrame* out, std::string* err) {
 }
 
 void Parser::attach_work(Job* job) { job->work = impl_->take_work(); }
+
+bool Parser::external_tiles(const Job* job, ExternalTiles* out) const {
+  if (job->st != ST_OK || job->show_existing || job->late_ctx || job->seg.enabled) return false;
+  if (job->h.frame_is_intra && job->non420) return false;  // the legacy 4:4:4 probe
+  out->h = &job->h;
+  out->probs = &job->probs;
+  out->ref_ok = job->ref_ok;
+  out->tiles = job->tiles;
+  out->tiles_len = job->tiles_len;
+  out->use_prev = job->use_prev;
+  out->prev_host = job->use_prev && !job->prev_external ? job->prev_mvs->data() : nullptr;
+  return true;
+}
+
+Status Parser::finish_external(Job* job, Status tiles_st, const std::string& tiles_err, ParsedFrame* out,
+                               std::string* err) {
+  if (job->st == ST_OK && !job->show_existing) {
+    job->external = true;
+    job->tr.st = tiles_st;
+    job->tr.err = tiles_err;
+  }
+  return finish(job, out, err);
+}
+
+bool Parser::wants_external_prev(const Job* job) const {
+  return job->st == ST_OK && !job->show_existing && job->use_prev && job->prev_external && !job->prev_mvs;
+}
+
+void Parser::provide_prev_mvs(Job* job, const void* mvs, size_t n) {
+  auto v = std::make_shared<std::vector<PrevMv>>(n);
+  if (n) memcpy(v->data(), mvs, n * sizeof(PrevMv));
+  job->prev_mvs = v;
+}
 
 void Parser::release(Job* job) {
   if (!job) return;

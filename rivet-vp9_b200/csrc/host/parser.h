@@ -70,6 +70,7 @@ struct SlotInfo {
 
 namespace syn {
 struct FrameHeader;
+struct PrevMv;
 }
 
 class Parser {
@@ -97,6 +98,30 @@ class Parser {
   void run(Job* job);
   Status finish(Job* job, ParsedFrame* out, std::string* err);
   void release(Job* job);
+
+  // Frames whose tiles another parser takes (the device tile parser): after
+  // begin, external_tiles says whether the frame can be handed out (nothing
+  // of it adapts probabilities, reads or writes segment ids, or needs the
+  // legacy 4:4:4 probe) and what its tiles read; the other parser's outcome
+  // comes back through finish_external, in frame order (ST_OK, or the
+  // status and message of the first tile in bitstream order that failed).
+  // The frame's motion vectors then stay with that parser: a later frame
+  // parsed here that reads them (wants_external_prev) must be given them
+  // first (provide_prev_mvs, in syn::PrevMv layout, mi_rows x mi_cols).
+  struct ExternalTiles {
+    const syn::FrameHeader* h = nullptr;
+    const Probs* probs = nullptr;
+    const bool* ref_ok = nullptr;         // [3]
+    const uint8_t* tiles = nullptr;       // the frame's tile data
+    size_t tiles_len = 0;
+    bool use_prev = false;                // reads the previous frame's motion vectors
+    const syn::PrevMv* prev_host = nullptr;  // those vectors, when this parser holds them
+  };
+  bool external_tiles(const Job* job, ExternalTiles* out) const;
+  Status finish_external(Job* job, Status tiles_st, const std::string& tiles_err, ParsedFrame* out,
+                         std::string* err);
+  bool wants_external_prev(const Job* job) const;
+  void provide_prev_mvs(Job* job, const void* mvs, size_t n);
 
   struct Impl;
 
