@@ -383,23 +383,19 @@ def run_config3(local, dev):
     return out
 
 
-def run_batched(local, dev, n_streams=64, frames=60):
-    """64 independent streams of uneven sizes and depths, all resident,
-    reconstructed at once (one CUDA stream each; and one launch per stage)
-    against the plain path (the same sequences one at a time)."""
-    import random
-
+def run_batched(local, dev):
+    """Configuration 4: 64 independent seeded streams of uneven sizes and
+    depths (rv9.workloads.CONFIG4), all resident, reconstructed at once (one
+    CUDA stream each; and one launch per stage) against the plain path (the
+    same sequences one at a time)."""
     import torch
     import rv9
     from rv9 import workloads as W
-    rng = random.Random(64)
-    classes = W.BATCH_CLASSES
-    contents = [W.looped(W.packets(c), frames) for c in classes]
-    picks = [rng.randrange(len(classes)) for _ in range(n_streams)]
-    loader = rv9.Decoder(device=local)
-    base = [loader.load_sequence(pk) for pk in contents]
-    decs = [rv9.Decoder(device=local) for _ in range(n_streams)]
-    seqs = [d.clone_sequence(base[k]) for d, k in zip(decs, picks)]
+    specs = W.CONFIG4
+    W.ensure_cached(specs)
+    contents = [W.packets(s) for s in specs]
+    decs = [rv9.Decoder(device=local) for _ in specs]
+    seqs = [d.load_sequence(pk) for d, pk in zip(decs, contents)]
     pairs = list(zip(decs, seqs))
     luma = sum(sq.luma_samples for sq in seqs)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -430,9 +426,8 @@ def run_batched(local, dev, n_streams=64, frames=60):
     ms_g = min(rv9.run_batched(pairs, groups=g) for _ in range(2))
     # Every shown frame of one more stage-batched run, through device-memory
     # frame sinks, against the oracle's decode of each content.
-    want = oracle_frames_all([pk[:W.CLASS_FRAMES] for pk in contents], threads=2)
-    want = [W.looped(w, frames) for w in want]
-    sizes = [[sz for _, sz in want[k]] for k in picks]
+    want = oracle_frames_all(contents, threads=1)
+    sizes = [[sz for _, sz in w] for w in want]
     sinks = [torch.empty(sum(sz), dtype=torch.uint8, device=dev) for sz in sizes]
     for d, b in zip(decs, sinks):
         d.set_frame_sink(b.data_ptr(), b.numel())
@@ -442,7 +437,7 @@ def run_batched(local, dev, n_streams=64, frames=60):
         frames_j, used, dropped = d.frame_sink_state()
         d.set_frame_sink(0, 0)
         got = frame_md5s(b[:used].cpu().numpy(), sz) if not dropped else []
-        c = compare(got, [m for m, _ in want[picks[j]]])
+        c = compare(got, [m for m, _ in want[j]])
         checked += c["frames"]
         if not c["equal"] and ok:
             ok, first_bad = False, {"stream": j, **c}
@@ -451,8 +446,8 @@ def run_batched(local, dev, n_streams=64, frames=60):
               "speedup_vs_plain": round(ms_plain / ms_g, 2),
               "autotune": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in staged_tune.items()}}
     out = {
-        "workload": f"{n_streams} streams over 8 generated contents {{320x240, 640x360, 1280x720, 1920x1080}} x "
-                    f"{{8, 10}}-bit 4:2:0, q per content in [35, 85], {W.CLASS_FRAMES} frames looped to {frames}",
+        "workload": f"{len(specs)} independent streams, seeds 0..{len(specs) - 1}, sizes drawn from {{320x240, "
+                    "640x360, 1280x720, 1920x1080}, 8/10-bit 4:2:0 with p=0.5, 60 frames each, q drawn in [30, 90]",
         "frames": sum(sq.frames for sq in seqs),
         "value": round(luma / (ms_batched / 1e3) / 1e6, 2), "unit": "Mpixels/s",
         "plain_per_stream": round(luma / (ms_plain / 1e3) / 1e6, 2),
@@ -470,9 +465,9 @@ def run_batched(local, dev, n_streams=64, frames=60):
                                    "oracle's decode of the stream's content", "frames": checked, "equal": ok,
                             "first_mismatch": first_bad},
     }
-    for sq in seqs + base:
+    for sq in seqs:
         sq.free()
-    for d in decs + [loader]:
+    for d in decs:
         d.close()
     return out
 

@@ -13,7 +13,9 @@ The definitions follow the five benchmark configurations:
   CONFIG2  60 frames 1920x1080 8-bit 4:2:0, 4 tile columns, q40 and q80
   CONFIG3  60 frames 3840x2160 10-bit 4:2:0 and 30 frames 1280x720 12-bit
            4:4:4, q30, 4 tile columns, LAST and GOLDEN references
-  BATCH_CLASSES  the contents of the 64-stream batch (8 size / depth classes)
+  CONFIG4  64 independent streams, seeds 0..63, sizes 320x240 .. 1080p, 8/10-bit,
+           60 frames, q in [30, 90]
+  BATCH_CLASSES  eight size / depth classes (the batched tests' contents)
   SERVE_CLASSES  the contents of the 32-stream serving mix (720p / 1080p /
            2160p at 8 and 10 bits)
 """
@@ -42,6 +44,26 @@ CONFIG1 = [_spec("cif_q60", 352, 288, 30, 60, seed=0, tile_cols_log2=0, pan=(2, 
 CONFIG2 = [_spec("1080p_q40", 1920, 1080, 60, 40, seed=0), _spec("1080p_q80", 1920, 1080, 60, 80, seed=1)]
 CONFIG3 = [_spec("2160p_10bit_q30", 3840, 2160, 60, 30, seed=2, bit_depth=10, noise=24),
            _spec("720p_12bit_444_q30", 1280, 720, 30, 30, seed=3, bit_depth=12, chroma=(0, 0), noise=24)]
+
+
+def _config4():
+    """Configuration 4: 64 independent streams, seeds 0..63, each of a size
+    drawn uniformly from {320x240, 640x360, 1280x720, 1920x1080}, 8-bit or
+    10-bit with probability 0.5, 4:2:0, 60 frames, base q uniform in
+    [30, 90] (the draws from a generator seeded by the stream's seed)."""
+    import random
+    sizes = [(320, 240), (640, 360), (1280, 720), (1920, 1080)]
+    out = []
+    for seed in range(64):
+        rng = random.Random(7919 * seed + 4)
+        w, h = sizes[rng.randrange(4)]
+        bd = 10 if rng.random() < 0.5 else 8
+        q = rng.randint(30, 90)
+        out.append(_spec(f"c4_{seed:02d}_{w}x{h}_{bd}_q{q}", w, h, 60, q, seed=seed, bit_depth=bd))
+    return out
+
+
+CONFIG4 = _config4()
 CLASS_FRAMES = 30
 BATCH_CLASSES = [
     _spec("b240_8", 320, 240, CLASS_FRAMES, 35, seed=11),
@@ -103,17 +125,31 @@ def _generate(spec):
         os.replace(tmp, path)
 
 
-def ensure_cached(specs):
-    """Fills the cache for `specs` in a child process (the caller loads
-    neither the generator nor its library)."""
+def ensure_cached(specs, jobs=None):
+    """Fills the cache for `specs` in child processes (the caller loads
+    neither the generator nor its library): up to `jobs` of them at once
+    (default: the host's cores), the largest streams dealt out first so the
+    children finish together."""
     missing = [s for s in specs if not cached(s)]
     if not missing:
         return
     import subprocess
     import sys
+    jobs = max(1, min(len(missing), jobs or os.cpu_count() or 1))
+    work = sorted(missing, key=lambda s: -s["width"] * s["height"] * s["frames"])
+    shares = [[] for _ in range(jobs)]
+    load = [0] * jobs
+    for s in work:
+        k = load.index(min(load))
+        shares[k].append(s)
+        load[k] += s["width"] * s["height"] * s["frames"]
     code = ("import json, sys; sys.path.insert(0, sys.argv[1]); from rv9 import workloads; "
             "[workloads._generate(s) for s in json.loads(sys.argv[2])]")
-    subprocess.run([sys.executable, "-c", code, os.path.dirname(_HERE), json.dumps(missing)], check=True)
+    procs = [subprocess.Popen([sys.executable, "-c", code, os.path.dirname(_HERE), json.dumps(share)])
+             for share in shares]
+    codes = [p.wait() for p in procs]
+    if any(codes):
+        raise RuntimeError(f"stream generation failed (exit codes {codes})")
 
 
 def looped(pk, n):
