@@ -90,6 +90,24 @@ uint32_t rv9_decoder_threads(const rv9_decoder* dec);
 /* Frames of more than `pixels` luma samples are refused (RV9_UNSUPPORTED). */
 void rv9_decoder_set_max_pixels(rv9_decoder* dec, uint64_t pixels);
 
+/* Device parsing (no counterpart in the reference, which parses tiles on its
+ * host threads: src/decoder/block.rs:1776-1866). With `on`,
+ * rv9_decode_packets and rv9_sequence_load parse the tiles of every frame
+ * that allows it on the GPU, one thread per tile column and the columns of up
+ * to `window_frames` frames (0: 64) at once, and build the reconstruction's
+ * work lists there too; the host keeps the frame headers. A frame allows it
+ * when nothing of it adapts probabilities from its symbol counts, reads or
+ * writes segment ids, or needs the legacy 4:4:4 layout probe: key frames and
+ * error-resilient or frame-parallel frames of streams without segmentation
+ * (every frame of the generated streams but 4:2:2 / 4:4:4 key frames). The
+ * other frames parse on the host, in order. Results are identical to host
+ * parsing. rv9_sequence_load takes the device path only when every frame
+ * allows it. */
+rv9_status rv9_decoder_set_device_parse(rv9_decoder* dec, int on, uint32_t window_frames);
+/* Frames the device parser took, its boolean decodes, and the device time
+ * of its batches (tile parse and work lists, CUDA events on its stream). */
+void rv9_decoder_device_parse_stats(const rv9_decoder* dec, uint64_t* frames, uint64_t* bools, double* device_ms);
+
 /* Failure detection (no counterpart in the reference, whose waits are host
  * threads joining; its abort model is src/decoder/loopfilter.rs:300-338).
  * Every device-side wait of the intra and loop-filter wavefronts is bounded:

@@ -19,6 +19,8 @@ LIB = os.path.join(OUT, "librv9.so")
 
 SOURCES = [
     "gpu/kernels.cu",
+    "gpu/parse_kernels.cu",
+    "gpu/device_parse.cpp",
     "gpu/engine.cpp",
     "api/rv9_api.cpp",
     "serve/server.cpp",
@@ -32,6 +34,9 @@ HEADERS = [
     "gpu/md5.cuh",
     "gpu/engine_types.h",
     "gpu/engine.h",
+    "gpu/tile_parse.cuh",
+    "gpu/parse_plan.h",
+    "gpu/device_parse.h",
     "host/parser.h",
     "host/syntax.h",
     "host/probs.h",

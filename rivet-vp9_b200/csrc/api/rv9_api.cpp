@@ -6,11 +6,13 @@
 
 #include <algorithm>
 #include <chrono>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "../../../include/rv9.h"
+#include "../gpu/device_parse.h"
 #include "../gpu/engine.h"
 #include "api_internal.h"
 #include "../host/parser.h"
@@ -23,6 +25,20 @@ struct rv9_decoder {
   double parse_ms = 0;
   uint32_t parse_depth = 0;  // frames parsed at once; 0: one per two host threads
   uint32_t threads = 0;      // set_threads value; 0: one per core
+  // Device parsing (rv9_decoder_set_device_parse).
+  bool device_parse = false;
+  uint32_t dp_window = 64;
+  std::unique_ptr<rv9g::DeviceParser> dp;
+  cudaStream_t dp_stream = nullptr;
+  cudaEvent_t dp_ev[2] = {nullptr, nullptr};
+  uint64_t dp_frames = 0;
+  double dp_ms = 0;
+  ~rv9_decoder() {
+    dp.reset();
+    for (cudaEvent_t e : dp_ev)
+      if (e) cudaEventDestroy(e);
+    if (dp_stream) cudaStreamDestroy(dp_stream);
+  }
 };
 
 // Frames parsed at once by the multi-packet calls.
@@ -80,6 +96,35 @@ rv9_decoder* rv9_decoder_new(int device) {
 }
 
 void rv9_decoder_free(rv9_decoder* d) { delete d; }
+
+rv9_status rv9_decoder_set_device_parse(rv9_decoder* d, int on, uint32_t window_frames) {
+  if (!d) return RV9_INVALID_INPUT;
+  d->dp_window = window_frames ? window_frames : 64;
+  d->device_parse = on != 0;
+  if (!on || d->dp) return RV9_OK;
+  cudaError_t e = cudaSetDevice(d->engine.device());
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d->dp_stream, cudaStreamNonBlocking);
+  for (int i = 0; e == cudaSuccess && i < 2; ++i) e = cudaEventCreate(&d->dp_ev[i]);
+  if (e != cudaSuccess) {
+    d->err = std::string("device parser: ") + cudaGetErrorString(e);
+    d->device_parse = false;
+    return RV9_DEVICE;
+  }
+  std::unique_ptr<rv9g::DeviceParser> p(new rv9g::DeviceParser);
+  rv9::Status st = p->init(d->engine.device(), &d->err);
+  if (st != rv9::ST_OK) {
+    d->device_parse = false;
+    return (rv9_status)st;
+  }
+  d->dp = std::move(p);
+  return RV9_OK;
+}
+
+void rv9_decoder_device_parse_stats(const rv9_decoder* d, uint64_t* frames, uint64_t* bools, double* device_ms) {
+  if (frames) *frames = d ? d->dp_frames : 0;
+  if (bools) *bools = d && d->dp ? d->dp->bools() : 0;
+  if (device_ms) *device_ms = d ? d->dp_ms : 0;
+}
 void rv9_decoder_set_threads(rv9_decoder* d, uint32_t t) {
   d->threads = t;
   d->parser.set_threads((int)t);
@@ -158,11 +203,145 @@ void rv9_frame_release(rv9_frame* f) {
   f->size = 0;
 }
 
+// rv9_decode_packets with device parsing: frames in decode order; those
+// the device parser may take gather into a batch (up to the window), the
+// others parse on the host once the batch before them is reconstructed. A
+// batch parses and builds its work lists on the parser's stream while the
+// frames of the batch before it reconstruct on the engine's.
+static rv9_status decode_packets_device(rv9_decoder* d, const uint8_t* const* pkts, const size_t* lens, size_t n,
+                                        uint8_t* out, size_t cap, size_t* n_frames, size_t* bytes) {
+  rv9g::DeviceParser& P = *d->dp;
+  P.clear();
+  std::vector<rv9::Parser::Job*> pending;
+  // After an error in a launched batch: the jobs not finished are dropped,
+  // and the batch's stage buffer is handed back behind the reconstructions
+  // already queued from it.
+  auto release_pending = [&](size_t from) {
+    for (size_t i = from; i < pending.size(); ++i) d->parser.release(pending[i]);
+    pending.clear();
+    std::string ignored;
+    P.recon_queued(d->engine.stream(), &ignored);
+    P.clear();
+  };
+  auto show = [&](rv9g::DevFrame* shown) -> rv9_status {
+    if (!shown) return RV9_OK;
+    size_t nb = rv9g::Engine::packed_bytes(shown);
+    if (*bytes + nb > cap) {
+      d->err = "output buffer too small";
+      return RV9_INVALID_INPUT;
+    }
+    rv9::Status s2 = d->engine.download_async(shown, out + *bytes, &d->err);
+    if (s2 != rv9::ST_OK) return (rv9_status)s2;
+    *bytes += nb;
+    ++*n_frames;
+    return RV9_OK;
+  };
+  auto flush = [&]() -> rv9_status {
+    if (pending.empty()) return RV9_OK;
+    rv9::Status st;
+    cudaEventRecord(d->dp_ev[0], d->dp_stream);
+    if ((st = P.launch(d->dp_stream, &d->err)) != rv9::ST_OK || (st = P.collect(d->dp_stream, &d->err)) != rv9::ST_OK) {
+      release_pending(0);
+      return (rv9_status)st;
+    }
+    cudaEventRecord(d->dp_ev[1], d->dp_stream);
+    float ms = 0;
+    if (cudaEventSynchronize(d->dp_ev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, d->dp_ev[0], d->dp_ev[1]) == cudaSuccess)
+      d->dp_ms += ms;
+    for (size_t i = 0; i < pending.size(); ++i) {
+      std::string msg;
+      const rv9::Status ts = P.frame_status(i, &msg);
+      rv9::ParsedFrame meta;
+      st = d->parser.finish_external(pending[i], ts, msg, &meta, &d->err);
+      d->parser.release(pending[i]);
+      pending[i] = nullptr;
+      if (st != rv9::ST_OK) {
+        release_pending(i + 1);
+        return (rv9_status)st;
+      }
+      rv9g::FrameWork fw;
+      fw.desc = meta.desc;
+      fw.show_existing = false;
+      fw.show_frame = meta.show_frame;
+      fw.refresh_mask = meta.refresh_mask;
+      for (int k = 0; k < 3; ++k) fw.ref_slot[k] = meta.ref_slot[k];
+      P.frame_work(i, &fw);
+      rv9g::DevFrame* shown = nullptr;
+      st = d->engine.recon_resident(fw, P.frame_base(i), &shown, &d->err);
+      if (st != rv9::ST_OK) {
+        release_pending(i + 1);
+        return (rv9_status)st;
+      }
+      ++d->dp_frames;
+      rv9_status s3 = show(shown);
+      if (s3 != RV9_OK) {
+        release_pending(i + 1);
+        return s3;
+      }
+    }
+    pending.clear();
+    st = P.recon_queued(d->engine.stream(), &d->err);
+    P.clear();
+    return (rv9_status)st;
+  };
+  std::vector<std::pair<size_t, size_t>> frames;
+  for (size_t i = 0; i < n; ++i) {
+    rv9::superframe_split(pkts[i], lens[i], &frames);
+    for (auto& fr : frames) {
+      const uint8_t* data = pkts[i] + fr.first;
+      auto t0 = std::chrono::steady_clock::now();
+      rv9::Parser::Job* job = d->parser.begin(data, fr.second, nullptr);
+      rv9::Parser::ExternalTiles x;
+      const bool dev = d->parser.external_tiles(job, &x) && P.add(x, *x.desc);
+      d->parse_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      if (dev) {
+        pending.push_back(job);
+        // A batch ends at the window or at 4 GiB of device records.
+        if (pending.size() >= d->dp_window || P.stage_bytes() >= (4ull << 30)) {
+          rv9_status st = flush();
+          if (st != RV9_OK) return st;
+        }
+        continue;
+      }
+      // A frame for the host parser: what came before it first.
+      rv9_status st = flush();
+      if (st != RV9_OK) {
+        d->parser.release(job);
+        return st;
+      }
+      t0 = std::chrono::steady_clock::now();
+      if (d->parser.wants_external_prev(job) && P.have_last()) {
+        std::vector<rv9g::tp::PrevMv> prev;
+        rv9::Status s2 = P.last_prev(&prev, d->dp_stream, &d->err);
+        if (s2 != rv9::ST_OK) {
+          d->parser.release(job);
+          return (rv9_status)s2;
+        }
+        d->parser.provide_prev_mvs(job, prev.data(), prev.size());
+      }
+      d->parser.attach_work(job);
+      d->parser.run(job);
+      rv9::Status s2 = d->parser.finish(job, &d->pf, &d->err);
+      d->parser.release(job);
+      d->parse_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      if (s2 != rv9::ST_OK) return (rv9_status)s2;
+      rv9g::DevFrame* shown = nullptr;
+      s2 = d->engine.recon(d->pf, &shown, &d->err);
+      if (s2 != rv9::ST_OK) return (rv9_status)s2;
+      if ((st = show(shown)) != RV9_OK) return st;
+    }
+  }
+  rv9_status st = flush();
+  if (st != RV9_OK) return st;
+  return (rv9_status)d->engine.sync(&d->err);
+}
+
 rv9_status rv9_decode_packets(rv9_decoder* d, const uint8_t* const* pkts, const size_t* lens, size_t n,
                               uint8_t* out, size_t cap, size_t* n_frames, size_t* bytes) {
   *n_frames = 0;
   *bytes = 0;
   if (!d || (n && (!pkts || !lens))) return RV9_INVALID_INPUT;
+  if (d->device_parse && d->dp) return decode_packets_device(d, pkts, lens, n, out, cap, n_frames, bytes);
   // Frames parse `depth` at a time where the stream allows (FramePipeline);
   // each is reconstructed in order as its records come out.
   const int depth = parse_depth(d);
@@ -213,9 +392,102 @@ struct rv9_sequence {
   rv9g::Sequence seq;
 };
 
+// rv9_sequence_load with device parsing, when every frame allows it (a
+// fresh parser; *done false and nothing kept otherwise): one batch, whose
+// stage buffer becomes the sequence's device data.
+static rv9::Status sequence_load_device(rv9_decoder* d, const uint8_t* const* pkts, const size_t* lens, size_t n,
+                                        rv9g::Sequence* seq, bool* done) {
+  *done = false;
+  rv9::Parser parser;
+  parser.set_threads(0);
+  rv9g::DeviceParser& P = *d->dp;
+  P.clear();
+  std::vector<rv9::Parser::Job*> jobs;
+  auto drop = [&](size_t from) {
+    for (size_t i = from; i < jobs.size(); ++i) parser.release(jobs[i]);
+    jobs.clear();
+    P.clear();
+  };
+  std::vector<std::pair<size_t, size_t>> split;
+  for (size_t i = 0; i < n; ++i) {
+    rv9::superframe_split(pkts[i], lens[i], &split);
+    for (auto& fr : split) {
+      rv9::Parser::Job* job = parser.begin(pkts[i] + fr.first, fr.second, nullptr);
+      jobs.push_back(job);
+      rv9::Parser::ExternalTiles x;
+      if (!parser.external_tiles(job, &x) || !P.add(x, *x.desc)) {
+        drop(0);
+        return rv9::ST_OK;
+      }
+    }
+  }
+  *done = true;
+  rv9::Status st;
+  cudaEventRecord(d->dp_ev[0], d->dp_stream);
+  if ((st = P.launch(d->dp_stream, &d->err)) != rv9::ST_OK || (st = P.collect(d->dp_stream, &d->err)) != rv9::ST_OK) {
+    drop(0);
+    return st;
+  }
+  cudaEventRecord(d->dp_ev[1], d->dp_stream);
+  float ms = 0;
+  if (cudaEventSynchronize(d->dp_ev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, d->dp_ev[0], d->dp_ev[1]) == cudaSuccess)
+    d->dp_ms += ms;
+  seq->frames.resize(jobs.size());
+  seq->luma_samples = 0;
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    std::string msg;
+    const rv9::Status ts = P.frame_status(i, &msg);
+    rv9::ParsedFrame meta;
+    st = parser.finish_external(jobs[i], ts, msg, &meta, &d->err);
+    parser.release(jobs[i]);
+    jobs[i] = nullptr;
+    if (st != rv9::ST_OK) {
+      drop(i + 1);
+      return st;
+    }
+    rv9g::FrameWork& fw = seq->frames[i];
+    fw.desc = meta.desc;
+    fw.show_existing = false;
+    fw.show_frame = meta.show_frame;
+    fw.refresh_mask = meta.refresh_mask;
+    for (int k = 0; k < 3; ++k) fw.ref_slot[k] = meta.ref_slot[k];
+    P.frame_work(i, &fw);
+    const uint64_t off = P.frame_offset(i);
+    fw.o_blocks += off;
+    fw.o_toks += off;
+    fw.o_coefs += off;
+    fw.o_units += off;
+    fw.o_res += off;
+    fw.o_intra += off;
+    fw.o_intra_jobs += off;
+    if (meta.show_frame) seq->luma_samples += (uint64_t)meta.desc.width * meta.desc.height;
+    ++d->dp_frames;
+  }
+  jobs.clear();
+  seq->bytes = P.stage_bytes();
+  seq->d_data = P.release_stage();
+  P.clear();
+  return rv9::ST_OK;
+}
+
 rv9_status rv9_sequence_load(rv9_decoder* d, const uint8_t* const* pkts, const size_t* lens, size_t n,
                              rv9_sequence** out) {
   *out = nullptr;
+  if (d && d->device_parse && d->dp) {
+    rv9_sequence* s = new rv9_sequence;
+    bool done = false;
+    rv9::Status st = sequence_load_device(d, pkts, lens, n, &s->seq, &done);
+    if (st != rv9::ST_OK) {
+      d->engine.sequence_free(&s->seq);
+      delete s;
+      return (rv9_status)st;
+    }
+    if (done) {
+      *out = s;
+      return RV9_OK;
+    }
+    delete s;
+  }
   rv9::Parser parser;  // a fresh stream
   parser.set_threads(0);
   std::vector<rv9::ParsedFrame> frames;

@@ -161,6 +161,12 @@ class Engine {
   // (or null) stays valid until the next call. Work is queued; errors of the
   // device waits surface at the next sync().
   rv9::Status recon(const rv9::ParsedFrame& pf, DevFrame** shown, std::string* err);
+  // Reconstructs a frame whose records and work lists are already in device
+  // memory at d_base (the device parser's output, complete before this
+  // call), like recon().
+  rv9::Status recon_resident(const FrameWork& fw, const uint8_t* d_base, DevFrame** shown, std::string* err) {
+    return run_frame(fw, d_base, false, shown, err);
+  }
   // Copies the visible planes of `f`, packed (the reference Frame layout),
   // into host memory `dst` on the engine's stream (queued).
   rv9::Status download_async(DevFrame* f, uint8_t* dst, std::string* err);

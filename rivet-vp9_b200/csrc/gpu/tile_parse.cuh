@@ -325,57 +325,74 @@ struct TileParser {
     for (uint32_t r = mi_row_start; r < mi_row_end && !err; r += 8) {
       memset(left_nz, 0, sizeof left_nz);
       memset(left_part, 0, sizeof left_part);
-      for (uint32_t c = mi_col_start; c < mi_col_end && !err; c += 8) decode_partition(r, c, 12 /* BLOCK_64X64 */);
+      for (uint32_t c = mi_col_start; c < mi_col_end && !err; c += 8) decode_superblock(r, c);
     }
   }
 
-  TP_HD void decode_partition(uint32_t r, uint32_t c, uint8_t bsize) {
-    if (r >= mi_rows || c >= mi_cols || err) return;
-    const uint32_t num8x8 = T->n8w[bsize];
-    const uint32_t half = num8x8 >> 1;
-    const bool has_rows = (r + half) < mi_rows;
-    const bool has_cols = (c + half) < mi_cols;
-    const uint32_t bsl = T->mi_wl2[bsize];
-    const uint32_t boffset = T->mi_wl2[12] - bsl;
-    uint8_t above = 0, left = 0;
-    for (uint32_t i = 0; i < num8x8; ++i) {
-      above |= above_part[c + i];
-      left |= left_part[(r + i) & 7];
-    }
-    const bool a = (above & (1 << boffset)) != 0;
-    const bool l = (left & (1 << boffset)) != 0;
-    const int ctx = (int)(bsl * 4 + (l ? 2 : 0) + (a ? 1 : 0));
-    const uint8_t* probs = F->frame_is_intra ? T->kf_partition[ctx] : F->probs.partition[ctx];
-    int partition;
-    if (has_rows && has_cols)
-      partition = bd.tree(T->partition_tree, probs);
-    else if (has_cols)
-      partition = bd.read(probs[1]) ? 3 /* SPLIT */ : 1 /* HORZ */;
-    else if (has_rows)
-      partition = bd.read(probs[2]) ? 3 : 2 /* VERT */;
-    else
-      partition = 3;
-    const uint8_t subsize = T->subsize[partition][bsize];
-    if (subsize == 14 /* BLOCK_INVALID */) {
-      fail(TP_PARTITION);
-      return;
-    }
-    if (subsize < 3 /* BLOCK_8X8 */ || partition == 0) {
-      decode_block(r, c, subsize);
-    } else if (partition == 1) {
-      decode_block(r, c, subsize);
-      if (has_rows) decode_block(r + half, c, subsize);
-    } else if (partition == 2) {
-      decode_block(r, c, subsize);
-      if (has_cols) decode_block(r, c + half, subsize);
-    } else {
-      decode_partition(r, c, subsize);
-      decode_partition(r, c + half, subsize);
-      decode_partition(r + half, c, subsize);
-      decode_partition(r + half, c + half, subsize);
-    }
-    if (err) return;
-    if (bsize == 3 || partition != 3) {
+  // decode_partition (spec 6.4.3) from a superblock down, without recursion:
+  // a split pushes its four quarters (the first on top) and has nothing left
+  // to do after them, so an explicit stack visits the regions in the
+  // recursion's order.
+  TP_HD void decode_superblock(uint32_t r0, uint32_t c0) {
+    uint32_t st_r[16], st_c[16];
+    uint8_t st_b[16];
+    int top = 0;
+    st_r[0] = r0;
+    st_c[0] = c0;
+    st_b[0] = 12;  // BLOCK_64X64
+    top = 1;
+    while (top > 0 && !err) {
+      --top;
+      const uint32_t r = st_r[top], c = st_c[top];
+      const uint8_t bsize = st_b[top];
+      if (r >= mi_rows || c >= mi_cols) continue;
+      const uint32_t num8x8 = T->n8w[bsize];
+      const uint32_t half = num8x8 >> 1;
+      const bool has_rows = (r + half) < mi_rows;
+      const bool has_cols = (c + half) < mi_cols;
+      const uint32_t bsl = T->mi_wl2[bsize];
+      const uint32_t boffset = T->mi_wl2[12] - bsl;
+      uint8_t above = 0, left = 0;
+      for (uint32_t i = 0; i < num8x8; ++i) {
+        above |= above_part[c + i];
+        left |= left_part[(r + i) & 7];
+      }
+      const bool a = (above & (1 << boffset)) != 0;
+      const bool l = (left & (1 << boffset)) != 0;
+      const int ctx = (int)(bsl * 4 + (l ? 2 : 0) + (a ? 1 : 0));
+      const uint8_t* probs = F->frame_is_intra ? T->kf_partition[ctx] : F->probs.partition[ctx];
+      int partition;
+      if (has_rows && has_cols)
+        partition = bd.tree(T->partition_tree, probs);
+      else if (has_cols)
+        partition = bd.read(probs[1]) ? 3 /* SPLIT */ : 1 /* HORZ */;
+      else if (has_rows)
+        partition = bd.read(probs[2]) ? 3 : 2 /* VERT */;
+      else
+        partition = 3;
+      const uint8_t subsize = T->subsize[partition][bsize];
+      if (subsize == 14 /* BLOCK_INVALID */) {
+        fail(TP_PARTITION);
+        return;
+      }
+      if (subsize >= 3 /* BLOCK_8X8 */ && partition == 3) {
+        // The quarters, the first one on top.
+        st_r[top] = r + half; st_c[top] = c + half; st_b[top++] = subsize;
+        st_r[top] = r + half; st_c[top] = c;        st_b[top++] = subsize;
+        st_r[top] = r;        st_c[top] = c + half; st_b[top++] = subsize;
+        st_r[top] = r;        st_c[top] = c;        st_b[top++] = subsize;
+        continue;
+      }
+      if (subsize < 3 || partition == 0) {
+        decode_block(r, c, subsize);
+      } else if (partition == 1) {
+        decode_block(r, c, subsize);
+        if (has_rows) decode_block(r + half, c, subsize);
+      } else {
+        decode_block(r, c, subsize);
+        if (has_cols) decode_block(r, c + half, subsize);
+      }
+      if (err) return;
       const uint8_t av = (uint8_t)(15 >> T->b_wl2[subsize]);
       const uint8_t lv = (uint8_t)(15 >> T->b_hl2[subsize]);
       for (uint32_t i = 0; i < num8x8; ++i) {

@@ -923,6 +923,7 @@ bool Parser::external_tiles(const Job* job, ExternalTiles* out) const {
   out->tiles_len = job->tiles_len;
   out->use_prev = job->use_prev;
   out->prev_host = job->use_prev && !job->prev_external ? job->prev_mvs->data() : nullptr;
+  out->desc = &job->out.desc;
   return true;
 }
 

@@ -116,6 +116,7 @@ class Parser {
     size_t tiles_len = 0;
     bool use_prev = false;                // reads the previous frame's motion vectors
     const syn::PrevMv* prev_host = nullptr;  // those vectors, when this parser holds them
+    const rv9_frame_desc* desc = nullptr;    // the records' frame description
   };
   bool external_tiles(const Job* job, ExternalTiles* out) const;
   Status finish_external(Job* job, Status tiles_st, const std::string& tiles_err, ParsedFrame* out,

@@ -75,7 +75,8 @@ EXPORTS = ("rv9_decoder_new", "rv9_decoder_free", "rv9_decoder_set_threads", "rv
            "rv9_sequence_run_noalloc", "rv9_sequences_run", "rv9_sequences_run_batched", "rv9_sequences_autotune_batched", "rv9_decoder_autotune",
            "rv9_sequences_autotune", "rv9_decoder_set_event_mask", "rv9_decoder_threads", "rv9_decoder_set_wait_limit",
            "rv9_decoder_set_test_fault", "rv9_decoder_set_frame_sink", "rv9_decoder_frame_sink_state",
-           "rv9_decoder_set_frame_digests", "rv9_decoder_frame_digests")
+           "rv9_decoder_set_frame_digests", "rv9_decoder_frame_digests", "rv9_decoder_set_device_parse",
+           "rv9_decoder_device_parse_stats")
 
 
 class CTuneResult(ctypes.Structure):
@@ -106,6 +107,10 @@ def load_library(path=None):
     lib.rv9_decoder_set_threads.argtypes = [vp, ctypes.c_uint32]
     lib.rv9_decoder_set_parse_depth.argtypes = [vp, ctypes.c_uint32]
     lib.rv9_decoder_set_max_pixels.argtypes = [vp, ctypes.c_uint64]
+    lib.rv9_decoder_set_device_parse.restype = ctypes.c_int
+    lib.rv9_decoder_set_device_parse.argtypes = [vp, ctypes.c_int, ctypes.c_uint32]
+    lib.rv9_decoder_device_parse_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64),
+                                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double)]
     lib.rv9_decoder_frames_decoded.restype = ctypes.c_uint64
     lib.rv9_decoder_frames_decoded.argtypes = [vp]
     lib.rv9_last_error.restype = ctypes.c_char_p
@@ -343,6 +348,19 @@ class Decoder:
 
     def set_max_pixels(self, n):
         self._lib.rv9_decoder_set_max_pixels(self._dec, n)
+
+    def set_device_parse(self, on=True, window_frames=0):
+        """Parse tiles on the GPU where the frames allow it (rv9_decoder_set_device_parse):
+        decode_packets and load_sequence then take that path; results are identical."""
+        st = self._lib.rv9_decoder_set_device_parse(self._dec, 1 if on else 0, window_frames)
+        if st != 0:
+            _raise(self._lib, self._dec, st)
+
+    def device_parse_stats(self):
+        """(frames the device parser took, its boolean decodes, its device milliseconds)."""
+        f, b, ms = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_double(0)
+        self._lib.rv9_decoder_device_parse_stats(self._dec, ctypes.byref(f), ctypes.byref(b), ctypes.byref(ms))
+        return f.value, b.value, ms.value
 
     def set_wait_limit(self, polls):
         """Polls before a device-side wavefront wait gives up (0: default)."""
