@@ -42,6 +42,13 @@ typedef struct rv9_gen_config {
   uint32_t noise;            /* uniform noise amplitude at 8 bits */
   uint32_t threads;          /* encoder threads (tile columns); 0 = cores */
   uint32_t color_space;      /* coded colour space: 0 = BT.709 (2), else the VP9 code (1 BT.601 ...) */
+  /* 0: error-resilient frames (each parses on its own). 1: frames that are
+   * not error-resilient, so inter frames read the previous frame's motion
+   * vectors; they refresh no probability context, except that with
+   * adapt_interval N > 0 frames N, 2N and 3N adapt their probabilities into
+   * contexts 1, 2 and 3 (read by no other frame). */
+  uint32_t non_resilient;
+  uint32_t adapt_interval;
 } rv9_gen_config;
 
 /* Generates and encodes a stream: packets back to back into `out` (`cap`

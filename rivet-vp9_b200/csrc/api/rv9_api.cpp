@@ -310,6 +310,7 @@ static rv9_status decode_packets_device(rv9_decoder* d, const uint8_t* const* pk
         return st;
       }
       t0 = std::chrono::steady_clock::now();
+      d->parser.bind_prev(job);  // frames begun before it have finished now
       if (d->parser.wants_external_prev(job) && P.have_last()) {
         std::vector<rv9g::tp::PrevMv> prev;
         rv9::Status s2 = P.last_prev(&prev, d->dp_stream, &d->err);

@@ -603,6 +603,7 @@ struct Encoder {
   Picture16 refs[8];
   uint32_t frame_no = 0;
   Picture16 last_rec;
+  std::vector<rv9::syn::PrevMv> prev_mvs;  // the last frame's, when frames are not error-resilient
 
   std::vector<uint8_t> encode(const Picture16& src);
 };
@@ -622,6 +623,10 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
   uint32_t tcl = std::min(std::max(cfg.tile_cols_log2, min_log2), std::max(max_log2, min_log2));
   const int lf_level = std::min(63, q * 10 / 48);
   const uint8_t refresh = key ? 0xff : (uint8_t)(golden ? 0x03 : 0x01);
+  const bool nonres = cfg.non_resilient != 0;
+  const uint32_t ai = cfg.adapt_interval;
+  const bool adapt = nonres && !key && ai && frame_no % ai == 0 && frame_no / ai <= 3;
+  const uint32_t ctx_idx = adapt ? frame_no / ai : 0;
   // Uncompressed header (spec 6.2).
   BitWriter w;
   w.f(2, 2);
@@ -631,7 +636,7 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
   w.f(0, 1);  // show_existing_frame
   w.f(key ? 0 : 1, 1);
   w.f(1, 1);  // show_frame
-  w.f(1, 1);  // error_resilient_mode
+  w.f(nonres ? 0 : 1, 1);  // error_resilient_mode
   if (key) {
     w.f(0x49, 8);
     w.f(0x83, 8);
@@ -648,6 +653,7 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
     w.f(cfg.height - 1, 16);
     w.f(0, 1);  // render size = frame size
   } else {
+    if (nonres) w.f(0, 2);  // reset_frame_context
     w.f(refresh, 8);
     for (int i = 0; i < 3; ++i) {
       w.f((uint32_t)i, 3);  // LAST slot 0, GOLDEN slot 1, ALTREF slot 2
@@ -658,7 +664,11 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
     w.f(0, 1);  // allow_high_precision_mv
     w.f(1, 1);  // switchable interpolation filter
   }
-  w.f(0, 2);  // frame_context_idx
+  if (nonres) {
+    w.f(adapt ? 1 : 0, 1);  // refresh_frame_context
+    w.f(adapt ? 0 : 1, 1);  // frame_parallel_decoding_mode
+  }
+  w.f(ctx_idx, 2);  // frame_context_idx
   w.f((uint32_t)lf_level, 6);
   w.f(0, 3);  // sharpness
   w.f(1, 1);  // loop_filter_delta_enabled (the defaults)
@@ -706,8 +716,8 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
   h.bit_depth = cfg.bit_depth;
   h.interpolation_filter = SWITCHABLE;
   h.reference_mode = SINGLE_REFERENCE;
-  h.error_resilient_mode = true;
-  h.frame_parallel_decoding_mode = true;
+  h.error_resilient_mode = !nonres;
+  h.frame_parallel_decoding_mode = !adapt;
   h.tile_cols_log2 = tcl;
   h.tile_rows_log2 = 0;
   h.base_q_idx = q;
@@ -723,7 +733,7 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
   fc.probs = &probs;
   fc.prev_seg_ids = nullptr;
   fc.prev_seg_len = 0;
-  fc.prev_mvs = nullptr;
+  fc.prev_mvs = nonres && !key && prev_mvs.size() == (size_t)mi_rows * mi_cols ? prev_mvs.data() : nullptr;
   fc.mi = mi.data();
   for (int p = 0; p < 3; ++p) fc.above_nonzero[p] = an[p].data();
   fc.above_partition = ap.data();
@@ -819,6 +829,16 @@ std::vector<uint8_t> Encoder::encode(const Picture16& src) {
   for (int i = 0; i < 8; ++i)
     if ((refresh >> i) & 1) refs[i] = rec;
   last_rec = rec;
+  if (nonres) {
+    // PrevMvs / PrevRefFrames for the next frame (spec 8.10 step 2).
+    prev_mvs.resize(mi.size());
+    for (size_t i = 0; i < mi.size(); ++i) {
+      prev_mvs[i].ref_frame[0] = mi[i].ref_frame[0];
+      prev_mvs[i].ref_frame[1] = mi[i].ref_frame[1];
+      prev_mvs[i].mv[0] = mi[i].mv[0][3];
+      prev_mvs[i].mv[1] = mi[i].mv[1][3];
+    }
+  }
   ++frame_no;
   return out;
 }

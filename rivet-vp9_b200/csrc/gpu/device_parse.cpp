@@ -77,26 +77,36 @@ bool DeviceParser::add(const rv9::Parser::ExternalTiles& x, const rv9_frame_desc
   n_mi_ += mi_len;
   const uint64_t above_at = n_above_;
   n_above_ += align_up(tp::above_bytes(x.h->sb64_cols));
-  if (x.use_prev) {
+  // The previous frame is the batch's last one when the batch has frames (a
+  // frame parsed on the host ends a batch, and frames begun while a batch
+  // is open see the state from before it); else the state's: held by this
+  // parser from an earlier batch, or by the host parser, or none.
+  bool use_prev = x.use_prev;
+  if (use_prev) {
     info.prev_at = n_prev_;
     n_prev_ += mi_len;
-    if (x.prev_host) {
+    if (last_frame_ >= 0) {
+      info.prev_from = last_frame_;
+      info.wave = fi_[last_frame_].wave + 1;
+    } else if (x.prev_external) {
+      if (!have_last_ || last_mi_len_ != mi_len) {
+        n_prev_ -= mi_len;
+        n_mi_ -= mi_len;
+        n_above_ = above_at;
+        spans_.resize(s0);
+        chains_.resize(c0);
+        return false;
+      }
+      info.prev_from = -2;  // the last device-parsed frame of an earlier batch
+    } else if (x.prev_host) {
       info.prev_host = true;
       info.prev_host_at = prev_host_.size();
       const uint8_t* p = (const uint8_t*)x.prev_host;
       prev_host_.insert(prev_host_.end(), p, p + (size_t)mi_len * sizeof(tp::PrevMv));
-    } else if (last_frame_ >= 0) {
-      info.prev_from = last_frame_;
-      info.wave = fi_[last_frame_].wave + 1;
-    } else if (have_last_ && last_mi_len_ == mi_len) {
-      info.prev_from = -2;  // the last device-parsed frame of an earlier batch
     } else {
+      use_prev = false;  // the host parser's rule: no vectors of this size held
       n_prev_ -= mi_len;
-      n_mi_ -= mi_len;
-      n_above_ = above_at;
-      spans_.resize(s0);
-      chains_.resize(c0);
-      return false;
+      info.prev_at = 0;
     }
   }
   data_.insert(data_.end(), x.tiles, x.tiles + x.tiles_len);
@@ -144,6 +154,7 @@ bool DeviceParser::add(const rv9::Parser::ExternalTiles& x, const rv9_frame_desc
   scratch_used_ += (uint64_t)bf.cap_blocks * 8;
   tp::FrameIn f;
   tp::fill_frame_in(x, &f);
+  f.use_prev = use_prev;
   fin_.push_back(f);
   fi_.push_back(info);
   build_.push_back(bf);

@@ -41,7 +41,7 @@ cudaError_t parse_tables(int device, const tp::Tables** out) {
 // One tile column per CTA of one warp; its first thread parses (the syntax
 // is one serial chain of boolean decodes), with the token cache in shared
 // memory.
-__global__ void __launch_bounds__(32) k_parse_chains(const tp::Tables* __restrict__ T,
+__global__ void __launch_bounds__(32, 1) k_parse_chains(const tp::Tables* __restrict__ T,
                                                      const tp::FrameIn* __restrict__ frames,
                                                      const tp::Chain* __restrict__ chains, uint32_t first,
                                                      const tp::Span* __restrict__ spans,
@@ -49,10 +49,16 @@ __global__ void __launch_bounds__(32) k_parse_chains(const tp::Tables* __restric
                                                      const tp::PrevMv* prev, rv9_block* blocks, rv9_tok* toks,
                                                      uint32_t* coefs, tp::ChainOut* outs) {
   __shared__ uint8_t tc[1024];
-  if (threadIdx.x != 0) return;
+  __shared__ uint32_t pkw[sizeof(((tp::FrameIn*)0)->coef_pk) / 4];
   const uint32_t i = first + blockIdx.x;
   const tp::Chain ch = chains[i];
-  tp::parse_chain(T, frames, ch, spans, data, mi, above, prev, blocks, toks, coefs, tc, &outs[i]);
+  // The frame's coefficient probabilities into shared memory (the warp),
+  // then the first thread parses.
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(frames[ch.frame].coef_pk);
+  for (uint32_t k = threadIdx.x; k < sizeof(pkw) / 4; k += 32) pkw[k] = src[k];
+  __syncwarp();
+  if (threadIdx.x != 0) return;
+  tp::parse_chain(T, frames, ch, spans, data, mi, above, prev, blocks, toks, coefs, tc, pkw, &outs[i]);
 }
 
 cudaError_t launch_parse_chains(const tp::Tables* T, const tp::FrameIn* frames, const tp::Chain* chains,

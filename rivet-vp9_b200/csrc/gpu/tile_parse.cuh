@@ -31,13 +31,21 @@
 #if defined(__CUDACC__)
 #define TP_HD __host__ __device__
 #define TP_INL __host__ __device__ __forceinline__
+#define TP_NOINL __host__ __device__ __noinline__
 #else
 #define TP_HD
 #define TP_INL inline
+#define TP_NOINL __attribute__((noinline))
 #endif
 
 namespace rv9g {
 namespace tp {
+
+#if !defined(__CUDACC__)
+struct uint2 {
+  uint32_t x, y;
+};
+#endif
 
 enum Error : int32_t {
   TP_OK = 0,
@@ -92,7 +100,7 @@ struct PrevMv {
 // One scan index of a transform size and scan order: the coefficient's
 // position, the two positions whose token energies give its context (spec
 // 6.4.24's above and left; reference block.rs:1656-1699) and its band.
-struct ScanEnt {
+struct alignas(8) ScanEnt {
   uint16_t pos, nb0, nb1;
   uint8_t band, pad;
 };
@@ -195,51 +203,125 @@ TP_INL int clz32(uint32_t x) {
 #endif
 }
 
-// The boolean decoder (spec 9.2). `value` holds the decoder's current byte in
-// bits 31..24 followed by stream bits not yet consumed; `bits` counts the
-// valid bits from bit 31 down and stays at 16 or more between decodes. Bits
+// Device intrinsics with their host equivalents.
+// The top 32 bits of (hi:lo) << s, 0 <= s < 32.
+TP_INL uint32_t funnel_l(uint32_t lo, uint32_t hi, int s) {
+#if defined(__CUDA_ARCH__)
+  return __funnelshift_l(lo, hi, s);
+#else
+  return s ? (hi << s) | (lo >> (32 - s)) : hi;
+#endif
+}
+// Byte i of the result is byte (s >> 4i) & 7 of (y:x) (selector values 0-7).
+TP_INL uint32_t byte_perm(uint32_t x, uint32_t y, uint32_t s) {
+#if defined(__CUDA_ARCH__)
+  return __byte_perm(x, y, s);
+#else
+  const uint64_t v = ((uint64_t)y << 32) | x;
+  uint32_t r = 0;
+  for (int i = 0; i < 4; ++i) r |= (uint32_t)((v >> (8 * ((s >> (4 * i)) & 7))) & 0xff) << (8 * i);
+  return r;
+#endif
+}
+// Read-only loads through the non-coherent cache on the device.
+template <class T>
+TP_INL T ro(const T* p) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+// Four bytes at p, big-endian, when p + 4 <= the end of the data. On the
+// device, from the two aligned words around them (the buffer holding the
+// tile data has 16 bytes of padding past its end).
+TP_INL uint32_t load_be32(const uint8_t* p) {
+#if defined(__CUDA_ARCH__)
+  const uint32_t a = (uint32_t)((uintptr_t)p & 3);
+  const uint32_t* q = (const uint32_t*)(p - a);
+  return __byte_perm(__ldg(q), __ldg(q + 1), 0x0123u + a * 0x1111u);
+#else
+  return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3];
+#endif
+}
+
+// A scan entry in one 8-byte load.
+TP_INL ScanEnt ld_scan(const ScanEnt* p) {
+#if defined(__CUDA_ARCH__)
+  const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+  ScanEnt e;
+  e.pos = (uint16_t)(v.x & 0xffff);
+  e.nb0 = (uint16_t)(v.x >> 16);
+  e.nb1 = (uint16_t)(v.y & 0xffff);
+  e.band = (uint8_t)((v.y >> 16) & 0xff);
+  e.pad = 0;
+  return e;
+#else
+  return *p;
+#endif
+}
+
+// The boolean decoder (spec 9.2). The window hi:lo holds the decoder's
+// current byte in hi's bits 31..24 followed by stream bits not yet consumed;
+// `bits` counts its valid bits from the top (24 or more between decodes, so
+// that a decode, which shifts out at most 7, always compares 8 valid bits),
+// and bits below them are zero. Stream bits are appended 32 at a time; bits
 // past the end of the data read as zero.
 struct Bool {
-  uint32_t value, range;
+  uint32_t hi, lo, range;
   int bits;
   const uint8_t* p;
   const uint8_t* end;
   uint32_t count;
 
-  TP_INL void fill() {
-    while (bits <= 24) {
-      uint32_t byte = 0;
-      if (p < end) byte = *p++;
-      value |= byte << (24 - bits);
-      bits += 8;
+  // The last bytes of the data, then zeros: out of line, so that the
+  // decodes inlined everywhere stay small.
+  static TP_NOINL uint32_t tail_word(const uint8_t** pp, const uint8_t* end) {
+    const uint8_t* p = *pp;
+    uint32_t w = 0;
+    for (int k = 0; k < 4; ++k) {
+      w <<= 8;
+      if (p < end) w |= *p++;
     }
+    *pp = p;
+    return w;
+  }
+  // Appends 32 stream bits; bits <= 32.
+  TP_INL void refill() {
+    uint32_t w;
+    if (end - p >= 4) {
+      w = load_be32(p);
+      p += 4;
+    } else {
+      w = tail_word(&p, end);
+    }
+    if (bits < 32) hi |= w >> bits;
+    lo = bits ? w << (32 - bits) : 0;
+    bits += 32;
   }
   // init_bool(sz): false if the marker bit is 1.
   TP_INL bool init(const uint8_t* d, uint32_t n) {
     p = d;
     end = d + n;
-    value = 0;
+    hi = lo = 0;
     bits = 0;
     range = 255;
     count = 0;
-    fill();
+    refill();
     return !read(128);
   }
-  TP_INL bool read(int prob) {
-    const uint32_t split = 1 + (((range - 1) * (uint32_t)prob) >> 8);
+  TP_INL bool read(uint32_t prob) {
+    const uint32_t split = 1 + (((range - 1) * prob) >> 8);
     const uint32_t big = split << 24;
-    const bool bit = value >= big;
-    if (bit) {
-      range -= split;
-      value -= big;
-    } else {
-      range = split;
-    }
+    const bool bit = hi >= big;
+    range = bit ? range - split : split;
+    hi = bit ? hi - big : hi;
     const int shift = clz32(range) - 24;
     range <<= shift;
-    value <<= shift;
+    hi = funnel_l(lo, hi, shift);
+    lo <<= shift;
     bits -= shift;
-    if (bits < 16) fill();
+    if (bits < 24) refill();
     ++count;
     return bit;
   }
@@ -306,6 +388,11 @@ struct TileParser {
   uint32_t* coefs;
   uint32_t n_blocks, n_toks, n_coefs, cap_blocks, cap_toks, cap_coefs;
   uint8_t* tc;  // token cache, 1024 entries
+  // The frame's coefficient probabilities as 32-bit words, node k of band b
+  // of a (tx size, plane type, reference type) at 36 * index + 6 b + 2 k
+  // (low word: contexts 0-3, high word: 4-5); FrameIn::coef_pk, copied to
+  // shared memory on the device.
+  const uint32_t* pkw;
   uint8_t left_nz[3][16];
   uint8_t left_part[8];
   uint32_t mi_row_start, mi_row_end, mi_col_start, mi_col_end;
@@ -1084,62 +1171,68 @@ struct TileParser {
     }
     const int kind = ttype == 2 /* DCT_ADST */ ? 1 : ttype == 1 /* ADST_DCT */ ? 2 : 0;
     const ScanEnt* sc = T->scan[tx_sz][kind];
-    const uint64_t(*pk)[3] = F->coef_pk[tx_sz][ptype][ref_type];
+    const uint32_t* pk = pkw + 36 * ((tx_sz * 2 + ptype) * 2 + ref_type);
     const uint32_t bd_bits = F->bit_depth;
     const uint32_t coef0 = n_coefs;
     uint32_t* out = coefs + n_coefs;
     uint32_t n_out = 0;
     int c = 0;
-    // The context as a shift into the band's words `w`.
-    int sh = (above + left) * 8;
-    ScanEnt e = sc[0];
-    const uint64_t* w = pk[e.band];
+    // The current scan index's entry and band words, the next entry loaded
+    // ahead, and the context as a byte selector (bytes 6 and 7 of a band
+    // word are zero, so the selector 0x7770 | ctx yields the byte alone).
+    ScanEnt e = ld_scan(sc);
+    ScanEnt en = ld_scan(sc + 1);
+    const uint32_t* w = pk + 6 * e.band;
+    uint32_t ctx = above + left;
     Bool r = bd;
     while (true) {
       // more_coefs: read at the start and after every nonzero token.
-      if (!r.read((uint8_t)(w[0] >> sh))) break;
+      if (!r.read(byte_perm(w[0], w[1], 0x7770u | ctx))) break;
       // A run of zero tokens; after a zero token no more_coefs is read.
       bool done = false;
-      while (!r.read((uint8_t)(w[1] >> sh))) {
+      while (!r.read(byte_perm(w[2], w[3], 0x7770u | ctx))) {
         tc[e.pos] = 0;
         if (++c == seg_eob) {
           done = true;
           break;
         }
-        e = sc[c];
-        w = pk[e.band];
-        sh = ((1 + tc[e.nb0] + tc[e.nb1]) >> 1) * 8;
+        e = en;
+        en = ld_scan(sc + (c + 1 < seg_eob ? c + 1 : c));
+        w = pk + 6 * e.band;
+        ctx = (1 + tc[e.nb0] + tc[e.nb1]) >> 1;
       }
       if (done) break;
       int32_t coef;
-      const uint8_t p2 = (uint8_t)(w[2] >> sh);
+      const uint32_t p2 = byte_perm(w[4], w[5], 0x7770u | ctx);
       if (!r.read(p2)) {
         coef = 1;  // ONE_TOKEN
         tc[e.pos] = 1;
       } else {
         // The rest of the token tree, its probabilities from one pareto row.
-        const uint8_t* pp = T->pareto[p2];
+        const uint2 pp = ro(reinterpret_cast<const uint2*>(T->pareto[p2]));
         int n = 4;
         do {
-          n = T->token_tree[n + (int)r.read(pp[(n >> 1) - 2])];
+          const uint32_t pr = byte_perm(pp.x, pp.y, (uint32_t)((n >> 1) - 2)) & 0xffu;
+          n = ro(&T->token_tree[n + (int)r.read(pr)]);
         } while (n > 0);
         const int token = -n;
-        tc[e.pos] = T->energy[token];
-        coef = T->extra_bits[token][2];
-        const int num_extra = T->extra_bits[token][1];
+        tc[e.pos] = ro(&T->energy[token]);
+        coef = ro(&T->extra_bits[token][2]);
+        const int num_extra = ro(&T->extra_bits[token][1]);
         if (num_extra) {
           if (token == 10 /* DCT_VAL_CAT6 */)
             for (int k = 0; k < (int)bd_bits - 8; ++k) coef += (int32_t)r.read(255) << (5 + (int)bd_bits - k);
-          const uint8_t* cat = T->cat_probs[T->extra_bits[token][0]];
-          for (int k = 0; k < num_extra; ++k) coef += (int32_t)r.read(cat[k]) << (num_extra - 1 - k);
+          const uint8_t* cat = T->cat_probs[ro(&T->extra_bits[token][0])];
+          for (int k = 0; k < num_extra; ++k) coef += (int32_t)r.read(ro(&cat[k])) << (num_extra - 1 - k);
         }
       }
       const bool sign = r.read(128);
       out[n_out++] = RV9_COEF_PACK(e.pos, sign ? -coef : coef);
       if (++c == seg_eob) break;
-      e = sc[c];
-      w = pk[e.band];
-      sh = ((1 + tc[e.nb0] + tc[e.nb1]) >> 1) * 8;
+      e = en;
+      en = ld_scan(sc + (c + 1 < seg_eob ? c + 1 : c));
+      w = pk + 6 * e.band;
+      ctx = (1 + tc[e.nb0] + tc[e.nb1]) >> 1;
     }
     bd = r;
     n_coefs += n_out;
@@ -1160,14 +1253,17 @@ struct TileParser {
 };
 
 // Decodes one tile column (its tiles in bitstream order) into the chain's
-// outputs. `tc` is 1024 bytes of token cache; `data` the batch's packet bytes.
+// outputs. `tc` is 1024 bytes of token cache; `pkw` the frame's coef_pk as
+// 32-bit words; `data` the batch's packet bytes.
 // Record indices (tok_start, coef_start) are relative to the chain's own
 // arrays; the caller rebases them when it gathers a frame's columns.
 TP_HD inline void parse_chain(const Tables* T, const FrameIn* frames, const Chain& ch, const Span* spans,
                               const uint8_t* data, Mi* mi_base, uint8_t* above_base, const PrevMv* prev_base,
-                              rv9_block* blocks, rv9_tok* toks, uint32_t* coefs, uint8_t* tc, ChainOut* out) {
+                              rv9_block* blocks, rv9_tok* toks, uint32_t* coefs, uint8_t* tc, const uint32_t* pkw,
+                              ChainOut* out) {
   const FrameIn* F = &frames[ch.frame];
   TileParser P;
+  P.pkw = pkw;
   P.T = T;
   P.F = F;
   P.mi = mi_base + ch.mi_at;

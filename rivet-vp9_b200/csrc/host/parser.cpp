@@ -544,6 +544,7 @@ struct Parser::Job {
   std::shared_ptr<std::vector<uint8_t>> prev_seg;
   std::shared_ptr<std::vector<PrevMv>> prev_mvs;  // set when the frame uses them
   bool use_prev = false;       // the frame reads the previous frame's vectors
+  bool use_prev_hdr = false;   // ... as its header and the last frame's decide (before the vectors' size check)
   bool prev_external = false;  // ... and an external tile parser holds them
   bool external = false;       // the tiles were parsed outside (finish_external)
   const uint8_t* tiles = nullptr;
@@ -700,6 +701,7 @@ Parser::Job* Parser::begin(const uint8_t* data, size_t len, const AfterHeader& a
     job->seg = S.st.seg;
     job->prev_seg = S.prev_segment_ids;
     job->prev_external = S.prev_external;
+    job->use_prev_hdr = use_prev;
     job->use_prev = use_prev && (S.prev_external || S.prev_mvs->size() >= mi_len);
     if (job->use_prev && !S.prev_external) job->prev_mvs = S.prev_mvs;
     job->tiles = data + comp_end;
@@ -921,7 +923,8 @@ bool Parser::external_tiles(const Job* job, ExternalTiles* out) const {
   out->ref_ok = job->ref_ok;
   out->tiles = job->tiles;
   out->tiles_len = job->tiles_len;
-  out->use_prev = job->use_prev;
+  out->use_prev = job->use_prev_hdr;
+  out->prev_external = job->use_prev && job->prev_external;
   out->prev_host = job->use_prev && !job->prev_external ? job->prev_mvs->data() : nullptr;
   out->desc = &job->out.desc;
   return true;
@@ -935,6 +938,16 @@ Status Parser::finish_external(Job* job, Status tiles_st, const std::string& til
     job->tr.err = tiles_err;
   }
   return finish(job, out, err);
+}
+
+void Parser::bind_prev(Job* job) {
+  if (job->st != ST_OK || job->show_existing || !job->use_prev_hdr) return;
+  const FrameState& S = impl_->s;
+  // begin's rule, against the state as it is now: host-held vectors of
+  // another size are not used.
+  job->prev_external = S.prev_external;
+  job->use_prev = S.prev_external || S.prev_mvs->size() >= (size_t)job->h.mi_rows * job->h.mi_cols;
+  job->prev_mvs = job->use_prev && !S.prev_external ? S.prev_mvs : nullptr;
 }
 
 bool Parser::wants_external_prev(const Job* job) const {

@@ -108,19 +108,30 @@ class Parser {
   // The frame's motion vectors then stay with that parser: a later frame
   // parsed here that reads them (wants_external_prev) must be given them
   // first (provide_prev_mvs, in syn::PrevMv layout, mi_rows x mi_cols).
+  // begin takes the previous frame's vectors as the state holds them then;
+  // when frames were begun ahead of others that finish later, bind_prev
+  // (after those finish) takes them again from the state.
   struct ExternalTiles {
     const syn::FrameHeader* h = nullptr;
     const Probs* probs = nullptr;
     const bool* ref_ok = nullptr;         // [3]
     const uint8_t* tiles = nullptr;       // the frame's tile data
     size_t tiles_len = 0;
-    bool use_prev = false;                // reads the previous frame's motion vectors
-    const syn::PrevMv* prev_host = nullptr;  // those vectors, when this parser holds them
+    // Whether the frame reads the previous frame's motion vectors, as its
+    // header and the last frame decide. Where they come from, as the state
+    // was at begin (the right source when no frame begun before this one is
+    // still unfinished; else the previous frame is one of those):
+    // prev_external, held by the external parser; prev_host, held here; or
+    // neither, in which case the frame reads none.
+    bool use_prev = false;
+    bool prev_external = false;
+    const syn::PrevMv* prev_host = nullptr;
     const rv9_frame_desc* desc = nullptr;    // the records' frame description
   };
   bool external_tiles(const Job* job, ExternalTiles* out) const;
   Status finish_external(Job* job, Status tiles_st, const std::string& tiles_err, ParsedFrame* out,
                          std::string* err);
+  void bind_prev(Job* job);
   bool wants_external_prev(const Job* job) const;
   void provide_prev_mvs(Job* job, const void* mvs, size_t n);
 

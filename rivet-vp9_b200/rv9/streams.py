@@ -13,7 +13,8 @@ class GenConfig(ctypes.Structure):
                 ("base_q_idx", ctypes.c_int32), ("tile_cols_log2", ctypes.c_uint32),
                 ("golden_interval", ctypes.c_uint32), ("seed", ctypes.c_uint32), ("pan_x", ctypes.c_int32),
                 ("pan_y", ctypes.c_int32), ("rectangles", ctypes.c_uint32), ("noise", ctypes.c_uint32),
-                ("threads", ctypes.c_uint32), ("color_space", ctypes.c_uint32)]
+                ("threads", ctypes.c_uint32), ("color_space", ctypes.c_uint32),
+                ("non_resilient", ctypes.c_uint32), ("adapt_interval", ctypes.c_uint32)]
 
 
 _lib = None
@@ -41,7 +42,7 @@ def lib():
 
 
 def config(width, height, frames, q, bit_depth=8, chroma=(1, 1), tile_cols_log2=0, golden_interval=8, seed=0,
-           pan=(2, 1), rectangles=3, noise=8, threads=0, color_space=0):
+           pan=(2, 1), rectangles=3, noise=8, threads=0, color_space=0, non_resilient=0, adapt_interval=0):
     c = GenConfig()
     c.width, c.height, c.bit_depth = width, height, bit_depth
     c.ss_x, c.ss_y = chroma
@@ -50,6 +51,7 @@ def config(width, height, frames, q, bit_depth=8, chroma=(1, 1), tile_cols_log2=
     c.pan_x, c.pan_y = pan
     c.rectangles, c.noise, c.threads = rectangles, noise, threads
     c.color_space = color_space  # 0: BT.709
+    c.non_resilient, c.adapt_interval = non_resilient, adapt_interval
     return c
 
 

@@ -50,6 +50,12 @@ bool same_records(const rv9::ParsedFrame& a, const rv9::ParsedFrame& b, char* wh
   return true;
 }
 
+// How often each source of previous motion vectors served a frame, since
+// the library was loaded: [0] a batch's previous frame, [1] the host
+// parser's state, [2] the last device frame of an earlier batch, [3] a host
+// frame given device-held vectors.
+uint64_t g_prev_counts[4] = {0, 0, 0, 0};
+
 struct DeviceSide {
   Tables tables;
   std::vector<Mi> last_mi;  // the last device-parsed frame's mode info
@@ -58,11 +64,14 @@ struct DeviceSide {
 };
 
 // The device parser's path for one frame, on the CPU: returns the tiles'
-// status and fills `out` with the gathered records.
-rv9::Status device_frame(DeviceSide& D, const rv9::Parser::ExternalTiles& x, rv9::ParsedFrame* out,
+// status and fills `out` with the gathered records. prev_mode: where the
+// previous frame's vectors come from: 0 none, 1 the host parser
+// (x.prev_host), 2 the last device-parsed frame.
+rv9::Status device_frame(DeviceSide& D, const rv9::Parser::ExternalTiles& x, int prev_mode, rv9::ParsedFrame* out,
                          std::string* msg, bool* planned) {
   FrameIn fin;
   fill_frame_in(x, &fin);
+  fin.use_prev = prev_mode != 0;
   std::vector<Span> spans;
   std::vector<Chain> chains;
   const char* e = plan_frame(*x.h, x.tiles, x.tiles_len, 0, 0, &spans, &chains);
@@ -74,7 +83,7 @@ rv9::Status device_frame(DeviceSide& D, const rv9::Parser::ExternalTiles& x, rv9
   std::vector<PrevMv> prev;
   if (fin.use_prev) {
     prev.resize(mi_len);
-    if (x.prev_host) {
+    if (prev_mode == 1) {
       memcpy(prev.data(), x.prev_host, mi_len * sizeof(PrevMv));
     } else {
       for (size_t i = 0; i < mi_len; ++i) {
@@ -101,7 +110,8 @@ rv9::Status device_frame(DeviceSide& D, const rv9::Parser::ExternalTiles& x, rv9
   uint8_t tc[1024];
   for (size_t i = 0; i < chains.size(); ++i)
     parse_chain(&D.tables, &fin, chains[i], spans.data(), x.tiles, mi.data(), above.data(), prev.data(),
-                blocks.data(), toks.data(), coefs.data(), tc, &outs[i]);
+                blocks.data(), toks.data(), coefs.data(), tc, reinterpret_cast<const uint32_t*>(fin.coef_pk),
+                &outs[i]);
   int first = -1;
   for (size_t i = 0; i < chains.size(); ++i) {
     D.bools += outs[i].bools;
@@ -139,12 +149,22 @@ rv9::Status device_frame(DeviceSide& D, const rv9::Parser::ExternalTiles& x, rv9
 
 extern "C" {
 
-// Parses the packets (superframes split) frame by frame with the host parser
-// and with the device parser's split; returns the number of frames the device
-// parser took (>= 0), or -1 with a message. After an error both go on with
-// the next frame. bools_out: boolean decodes of the device-parsed tiles.
-int device_parse_check(const uint8_t* const* pkts, const size_t* lens, size_t n, char* msg, size_t msg_cap,
-                       uint64_t* bools_out) {
+// Parses the packets (superframes split) frame by frame with the host parser,
+// and as the decoder's device-parse mode does with a batch window of `window`
+// frames: frames the device parser may take are begun and gathered until the
+// window fills or a frame for the host parser comes; then the batch's frames
+// are parsed (here by the CPU build of the device parser, in order, each
+// taking the previous frame's vectors from the batch's previous frame, else
+// from the host parser's state, else from the last device-parsed frame) and
+// finished in order; a host frame then rebinds the previous vectors
+// (bind_prev) and takes device-held ones when it reads them. Every frame's
+// status, message and records must equal frame-by-frame parsing. After an
+// error the rest of the batch is dropped, as the decoder drops it, and both
+// go on with the frame after the failed one. Returns the number of frames the
+// device parser took (>= 0), or -1 with a message. bools_out: boolean decodes
+// of the device-parsed tiles.
+int device_parse_check(const uint8_t* const* pkts, const size_t* lens, size_t n, int window, char* msg,
+                       size_t msg_cap, uint64_t* bools_out) {
   std::vector<std::pair<const uint8_t*, size_t>> frames;
   std::vector<std::pair<size_t, size_t>> split;
   for (size_t i = 0; i < n; ++i) {
@@ -156,61 +176,139 @@ int device_parse_check(const uint8_t* const* pkts, const size_t* lens, size_t n,
   rv9::Parser ref, par;
   ref.set_threads(1);
   par.set_threads(1);
+  std::vector<rv9::Status> want_st(frames.size());
+  std::vector<rv9::ParsedFrame> want(frames.size());
+  std::vector<std::string> want_err(frames.size());
+  for (size_t i = 0; i < frames.size(); ++i)
+    want_st[i] = ref.parse_frame(frames[i].first, frames[i].second, &want[i], &want_err[i]);
   int taken = 0;
-  for (size_t i = 0; i < frames.size(); ++i) {
-    rv9::ParsedFrame want, got;
-    std::string want_err, err;
-    rv9::Status want_st = ref.parse_frame(frames[i].first, frames[i].second, &want, &want_err);
-    rv9::Parser::Job* job = par.begin(frames[i].first, frames[i].second, nullptr);
+  struct Pending {
+    rv9::Parser::Job* job;
+    size_t idx;
     rv9::Parser::ExternalTiles x;
-    rv9::Status st;
-    bool took = false;
-    if (par.external_tiles(job, &x)) {
-      std::string tmsg;
-      bool planned = false;
-      rv9::Status tst = device_frame(*D, x, &got, &tmsg, &planned);
-      if (planned) {
-        took = true;
-        ++taken;
-        rv9::ParsedFrame meta;
-        st = par.finish_external(job, tst, tmsg, &meta, &err);
-        if (st == rv9::ST_OK) {
-          meta.blocks.swap(got.blocks);
-          meta.toks.swap(got.toks);
-          meta.coefs.swap(got.coefs);
-          got = std::move(meta);
-        }
-      }
-    }
-    if (!took) {
-      if (par.wants_external_prev(job)) {
-        std::vector<rv9g::tp::PrevMv> prev(D->last_mi.size());
-        for (size_t k = 0; k < prev.size(); ++k) {
-          prev[k].ref_frame[0] = D->last_mi[k].ref_frame[0];
-          prev[k].ref_frame[1] = D->last_mi[k].ref_frame[1];
-          prev[k].mv[0] = D->last_mi[k].mv[0][3];
-          prev[k].mv[1] = D->last_mi[k].mv[1][3];
-        }
-        par.provide_prev_mvs(job, prev.data(), prev.size());
-      }
-      par.attach_work(job);
-      par.run(job);
-      st = par.finish(job, &got, &err);
-    }
-    par.release(job);
-    if (st != want_st || (st != rv9::ST_OK && err != want_err)) {
-      snprintf(msg, msg_cap, "frame %zu%s: status %d (%s), host %d (%s)", i, took ? " (device)" : "", (int)st,
-               err.c_str(), (int)want_st, want_err.c_str());
-      return -1;
+    bool prev_from_batch;
+  };
+  std::vector<Pending> pending;
+  auto check = [&](size_t i, rv9::Status st, const std::string& err, const rv9::ParsedFrame& got, bool dev) {
+    if (st != want_st[i] || (st != rv9::ST_OK && err != want_err[i])) {
+      snprintf(msg, msg_cap, "frame %zu%s: status %d (%s), host %d (%s)", i, dev ? " (device)" : "", (int)st,
+               err.c_str(), (int)want_st[i], want_err[i].c_str());
+      return false;
     }
     char why[160] = "";
-    if (st == rv9::ST_OK && !same_records(got, want, why, sizeof why)) {
-      snprintf(msg, msg_cap, "frame %zu%s: %s", i, took ? " (device)" : "", why);
+    if (st == rv9::ST_OK && !same_records(got, want[i], why, sizeof why)) {
+      snprintf(msg, msg_cap, "frame %zu%s: %s", i, dev ? " (device)" : "", why);
+      return false;
+    }
+    return true;
+  };
+  // Returns the index of the frame the next frame to begin follows: the
+  // failed frame's successor after an error, else `next`. -1: mismatch.
+  auto flush = [&](size_t next, long* resume) -> bool {
+    *resume = (long)next;
+    for (size_t k = 0; k < pending.size(); ++k) {
+      Pending& pe = pending[k];
+      rv9::ParsedFrame got;
+      std::string tmsg, err;
+      bool planned = false;
+      const rv9::Parser::ExternalTiles& x = pe.x;
+      // The source DeviceParser::add picks.
+      int prev_mode = 0;
+      if (x.use_prev) {
+        if (pe.prev_from_batch) {
+          prev_mode = 2;
+          ++g_prev_counts[0];
+        } else if (x.prev_external) {
+          prev_mode = 2;
+          ++g_prev_counts[2];
+        } else if (x.prev_host) {
+          prev_mode = 1;
+          ++g_prev_counts[1];
+        }
+      }
+      rv9::Status tst = device_frame(*D, x, prev_mode, &got, &tmsg, &planned);
+      rv9::ParsedFrame meta;
+      rv9::Status st = par.finish_external(pe.job, tst, tmsg, &meta, &err);
+      par.release(pe.job);
+      if (st == rv9::ST_OK) {
+        meta.blocks.swap(got.blocks);
+        meta.toks.swap(got.toks);
+        meta.coefs.swap(got.coefs);
+      }
+      ++taken;
+      if (!check(pe.idx, st, err, meta, true)) return false;
+      if (st != rv9::ST_OK) {
+        for (size_t j = k + 1; j < pending.size(); ++j) par.release(pending[j].job);
+        *resume = (long)pe.idx + 1;
+        pending.clear();
+        return true;
+      }
+    }
+    pending.clear();
+    return true;
+  };
+  size_t i = 0;
+  while (i < frames.size()) {
+    rv9::Parser::Job* job = par.begin(frames[i].first, frames[i].second, nullptr);
+    rv9::Parser::ExternalTiles x;
+    bool dev = par.external_tiles(job, &x);
+    if (dev) {
+      // The device parser refuses a frame whose tiles do not split.
+      std::vector<Span> sp;
+      std::vector<Chain> ch;
+      if (plan_frame(*x.h, x.tiles, x.tiles_len, 0, 0, &sp, &ch)) dev = false;
+      if (dev && x.use_prev && pending.empty() && x.prev_external && D->last_mi.empty()) dev = false;
+    }
+    if (dev) {
+      pending.push_back(Pending{job, i, x, !pending.empty()});
+      ++i;
+      if ((int)pending.size() >= window) {
+        long resume;
+        if (!flush(i, &resume)) return -1;
+        i = (size_t)resume;
+      }
+      continue;
+    }
+    long resume;
+    if (!flush(i, &resume)) {
+      par.release(job);
       return -1;
     }
+    if ((size_t)resume != i) {
+      // An error in the batch: this frame was begun after it; drop it.
+      par.release(job);
+      i = (size_t)resume;
+      continue;
+    }
+    par.bind_prev(job);
+    if (par.wants_external_prev(job) && !D->last_mi.empty()) {
+      std::vector<rv9g::tp::PrevMv> prev(D->last_mi.size());
+      for (size_t k = 0; k < prev.size(); ++k) {
+        prev[k].ref_frame[0] = D->last_mi[k].ref_frame[0];
+        prev[k].ref_frame[1] = D->last_mi[k].ref_frame[1];
+        prev[k].mv[0] = D->last_mi[k].mv[0][3];
+        prev[k].mv[1] = D->last_mi[k].mv[1][3];
+      }
+      par.provide_prev_mvs(job, prev.data(), prev.size());
+      ++g_prev_counts[3];
+    }
+    rv9::ParsedFrame got;
+    std::string err;
+    par.attach_work(job);
+    par.run(job);
+    rv9::Status st = par.finish(job, &got, &err);
+    par.release(job);
+    if (!check(i, st, err, got, false)) return -1;
+    ++i;
   }
+  long resume;
+  if (!flush(frames.size(), &resume)) return -1;
   if (bools_out) *bools_out = D->bools;
   return taken;
+}
+
+void device_parse_prev_counts(uint64_t* out) {
+  for (int k = 0; k < 4; ++k) out[k] = g_prev_counts[k];
 }
 
 }  // extern "C"

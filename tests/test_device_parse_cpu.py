@@ -19,7 +19,7 @@ import subprocess
 import pytest
 
 from conftest import REPO, read_packets, vector_paths
-from streams_cases import CASES, generate
+from streams_cases import CASES, LINKED, generate, generate_linked
 
 SRC = os.path.join(REPO, "tests", "cpp", "device_parse_shim.cpp")
 LIB = os.path.join(REPO, "tests", "cpp", "_build", "libdevice_parse_shim.so")
@@ -38,25 +38,26 @@ def shim():
     lib = ctypes.CDLL(LIB)
     lib.device_parse_check.restype = ctypes.c_int
     lib.device_parse_check.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t),
-                                       ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,
+                                       ctypes.c_size_t, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_uint64)]
     return lib
 
 
-def check(lib, packets):
+def check(lib, packets, window=4):
     n = len(packets)
     arr = (ctypes.c_char_p * n)(*packets)
     lens = (ctypes.c_size_t * n)(*[len(p) for p in packets])
     msg = ctypes.create_string_buffer(512)
     bools = ctypes.c_uint64(0)
-    r = lib.device_parse_check(arr, lens, n, msg, 512, ctypes.byref(bools))
+    r = lib.device_parse_check(arr, lens, n, window, msg, 512, ctypes.byref(bools))
     assert r >= 0, msg.value.decode()
     return r, bools.value
 
 
+@pytest.mark.parametrize("window", [1, 4])
 @pytest.mark.parametrize("path", vector_paths(), ids=os.path.basename)
-def test_vectors(shim, path):
-    check(shim, read_packets(path))
+def test_vectors(shim, path, window):
+    check(shim, read_packets(path), window)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -77,8 +78,35 @@ def test_benchmark_stream_frames(shim):
         if not W.cached(spec):
             pytest.skip("benchmark streams not generated here")
         pk = W.packets(spec, generate=False)[:6]
-        taken, _ = check(shim, pk)
+        taken, _ = check(shim, pk, window=3)
         assert taken == len(pk)
+
+
+@pytest.mark.parametrize("window", [1, 3, 8])
+@pytest.mark.parametrize("name", sorted(LINKED))
+def test_linked_streams(shim, name, window):
+    # Frames that read the previous frame's motion vectors, with frames that
+    # adapt probabilities (host-parsed) among them: every source of previous
+    # vectors the batched flow has is taken, and each frame's records equal
+    # host parsing.
+    before = (ctypes.c_uint64 * 4)()
+    shim.device_parse_prev_counts(before)
+    packets = generate_linked(name)
+    taken, _ = check(shim, packets, window)
+    after = (ctypes.c_uint64 * 4)()
+    shim.device_parse_prev_counts(after)
+    used = [after[k] - before[k] for k in range(4)]
+    adapt = LINKED[name][7]
+    chroma = LINKED[name][3]
+    host_frames = (len(packets) - 1) // adapt if adapt else 0
+    host_frames = min(host_frames, 3) + (chroma != (1, 1))
+    assert taken == len(packets) - host_frames, (taken, used)
+    if window > 1:
+        assert used[0] > 0, used            # from the batch's previous frame
+    if window == 1 or adapt:
+        assert used[1] + used[2] > 0, used  # from the state: host- or device-held
+    if adapt:
+        assert used[3] > 0, used            # device-held vectors given to the host parser
 
 
 def test_corrupted_packets(shim):
@@ -90,7 +118,9 @@ def test_corrupted_packets(shim):
     for i in range(len(flipped) // 2, len(flipped)):
         flipped[i] ^= 0xA5                           # corrupted tile data
     bad[6] = bytes(flipped)
-    check(shim, bad)
+    for window in (1, 3, 8):
+        check(shim, bad, window)
     vec = read_packets(os.path.join(REPO, "tests", "golden", "vectors", "vp90-2-05-resize.ivf"))
     vec[5] = bytes(b ^ 0x5A for b in vec[5])
-    check(shim, vec)
+    for window in (1, 4):
+        check(shim, vec, window)

@@ -9,9 +9,12 @@ oracle's:
     streams of every configuration shape, in small and large batch windows;
   * the benchmark's full-length streams (configurations 1-3);
   * rv9_sequence_load + rv9_sequence_run (the device-built records resident);
-  * the conformance vectors, whose frames mostly adapt probabilities and so
-    alternate between the host parser and the device parser, which hands the
-    host the motion vectors it holds;
+  * streams whose frames read the previous frame's motion vectors, with
+    probability-adapting frames (parsed on the host) among them, so that the
+    vectors pass between the device parser's batches and to and from the host
+    parser;
+  * the conformance vectors (whose frames all adapt probabilities, so they
+    stay with the host parser: the device-parse mode must leave them exact);
   * a stream with a corrupted frame: the same error as host parsing, and the
     frames before it decoded.
 """
@@ -20,7 +23,7 @@ import os
 import pytest
 
 from conftest import FrameSinks, expected_md5s, oracle_frames, read_packets, split_md5s, vector_paths
-from streams_cases import CASES, generate
+from streams_cases import CASES, LINKED, generate, generate_linked
 
 pytestmark = pytest.mark.gpu
 
@@ -47,6 +50,28 @@ def test_generated_streams(name, window, oracle_lib):
         assert split_md5s(buf, sizes) == [m for m, _ in want]
         frames, bools, ms = dec.device_parse_stats()
         assert frames == len(packets) - (CASES[name][3] != (1, 1)) and bools > 0 and ms > 0
+    finally:
+        dec.close()
+
+
+@pytest.mark.parametrize("window", [1, 3, 8])
+@pytest.mark.parametrize("name", sorted(LINKED))
+def test_linked_streams(name, window, oracle_lib):
+    # Frames that read the previous frame's motion vectors, some of them
+    # adapting probabilities (those parse on the host): the vectors pass
+    # between the batch's frames, from the host parser to the device and
+    # back, and between batches.
+    import rv9
+    packets = generate_linked(name)
+    want = oracle_frames(oracle_lib, packets)
+    sizes = [s for _, s in want]
+    dec = rv9.Decoder(0)
+    try:
+        dec.set_device_parse(True, window)
+        nf, nb, buf = _decode(dec, packets, sum(sizes))
+        assert (nf, nb) == (len(sizes), sum(sizes))
+        assert split_md5s(buf, sizes) == [m for m, _ in want]
+        assert dec.device_parse_stats()[0] > 0
     finally:
         dec.close()
 

@@ -10,7 +10,7 @@ import subprocess
 import pytest
 
 from conftest import REPO, read_packets, vector_paths
-from streams_cases import generate
+from streams_cases import LINKED, generate, generate_linked
 
 SRC = os.path.join(REPO, "tests", "cpp", "parse_pipeline_shim.cpp")
 LIB = os.path.join(REPO, "tests", "cpp", "_build", "libparse_pipeline_shim.so")
@@ -50,6 +50,14 @@ def test_vectors(shim, path):
 def test_error_resilient_streams(shim, name):
     packets, _ = generate(name)
     for depth in (1, 3, 8):
+        assert check(shim, packets, depth=depth) == len(packets)
+
+
+@pytest.mark.parametrize("name", sorted(LINKED))
+def test_linked_streams(shim, name):
+    # Frames that read the previous frame's motion vectors wait for it.
+    packets = generate_linked(name)
+    for depth in (1, 4):
         assert check(shim, packets, depth=depth) == len(packets)
 
 
