@@ -48,17 +48,17 @@ __global__ void __launch_bounds__(32, 1) k_parse_chains(const tp::Tables* __rest
                                                      const uint8_t* __restrict__ data, tp::Mi* mi, uint8_t* above,
                                                      const tp::PrevMv* prev, rv9_block* blocks, rv9_tok* toks,
                                                      uint32_t* coefs, tp::ChainOut* outs) {
-  __shared__ uint8_t tc[1024];
-  __shared__ uint32_t pkw[sizeof(((tp::FrameIn*)0)->coef_pk) / 4];
+  static_assert(sizeof(((tp::FrameIn*)0)->coef_pk) == sizeof(tp::tp_pkw_smem), "probability words");
   const uint32_t i = first + blockIdx.x;
   const tp::Chain ch = chains[i];
-  // The frame's coefficient probabilities into shared memory (the warp),
-  // then the first thread parses.
+  // The frame's coefficient probabilities into the parser's shared array
+  // (the warp), then the first thread parses.
   const uint32_t* src = reinterpret_cast<const uint32_t*>(frames[ch.frame].coef_pk);
-  for (uint32_t k = threadIdx.x; k < sizeof(pkw) / 4; k += 32) pkw[k] = src[k];
+  for (uint32_t k = threadIdx.x; k < sizeof(tp::tp_pkw_smem) / 4; k += 32) tp::tp_pkw_smem[k] = src[k];
   __syncwarp();
   if (threadIdx.x != 0) return;
-  tp::parse_chain(T, frames, ch, spans, data, mi, above, prev, blocks, toks, coefs, tc, pkw, &outs[i]);
+  tp::parse_chain(T, frames, ch, spans, data, mi, above, prev, blocks, toks, coefs, tp::tp_tc_smem, tp::tp_pkw_smem,
+                  &outs[i]);
 }
 
 cudaError_t launch_parse_chains(const tp::Tables* T, const tp::FrameIn* frames, const tp::Chain* chains,

@@ -12,8 +12,10 @@
 // parser's on every test stream.
 //
 // What differs from the host parser is the form, for one GPU thread:
-//   * a 32-bit arithmetic-decoder window, refilled byte by byte (the
-//     decoded values do not depend on the window's width);
+//   * a 64-bit arithmetic-decoder window (two 32-bit words), refilled 32
+//     bits at a time (the decoded values do not depend on the window's width);
+//   * the token cache and the coefficient probabilities in shared memory,
+//     the probabilities of the current band in registers;
 //   * the left contexts as 16-entry windows of the current superblock row
 //     (they are cleared at each superblock row and never read outside it);
 //   * tables in one device-resident struct (Tables), the scan position, the
@@ -245,6 +247,23 @@ TP_INL uint32_t load_be32(const uint8_t* p) {
 #endif
 }
 
+// The parse kernel's shared memory (one tile column per CTA): the token
+// cache and the frame's coefficient probabilities as 32-bit words. Declared
+// here so that the parser's accesses are shared-memory accesses, which the
+// compiler keeps apart from its global stores; the CPU build uses the
+// TileParser's own arrays.
+#if defined(__CUDACC__)
+__shared__ uint8_t tp_tc_smem[1024];
+__shared__ uint32_t tp_pkw_smem[576];
+#endif
+#if defined(__CUDA_ARCH__)
+#define TP_TC(i) tp_tc_smem[i]
+#define TP_PKW(i) tp_pkw_smem[i]
+#else
+#define TP_TC(i) tc[i]
+#define TP_PKW(i) pkw[i]
+#endif
+
 // A scan entry in one 8-byte load.
 TP_INL ScanEnt ld_scan(const ScanEnt* p) {
 #if defined(__CUDA_ARCH__)
@@ -274,16 +293,12 @@ struct Bool {
   const uint8_t* end;
   uint32_t count;
 
-  // The last bytes of the data, then zeros: out of line, so that the
-  // decodes inlined everywhere stay small.
-  static TP_NOINL uint32_t tail_word(const uint8_t** pp, const uint8_t* end) {
-    const uint8_t* p = *pp;
+  // The last bytes of the data (fewer than 4), then zeros: out of line, so
+  // that the decodes inlined everywhere stay small. Takes and returns values
+  // only, so that the window stays in registers.
+  static TP_NOINL uint32_t tail_word(const uint8_t* p, const uint8_t* end) {
     uint32_t w = 0;
-    for (int k = 0; k < 4; ++k) {
-      w <<= 8;
-      if (p < end) w |= *p++;
-    }
-    *pp = p;
+    for (int k = 0; k < 4; ++k) w = (w << 8) | (p + k < end ? p[k] : 0u);
     return w;
   }
   // Appends 32 stream bits; bits <= 32.
@@ -293,7 +308,8 @@ struct Bool {
       w = load_be32(p);
       p += 4;
     } else {
-      w = tail_word(&p, end);
+      w = tail_word(p, end);
+      p = end;
     }
     if (bits < 32) hi |= w >> bits;
     lo = bits ? w << (32 - bits) : 0;
@@ -387,11 +403,12 @@ struct TileParser {
   rv9_tok* toks;
   uint32_t* coefs;
   uint32_t n_blocks, n_toks, n_coefs, cap_blocks, cap_toks, cap_coefs;
-  uint8_t* tc;  // token cache, 1024 entries
-  // The frame's coefficient probabilities as 32-bit words, node k of band b
-  // of a (tx size, plane type, reference type) at 36 * index + 6 b + 2 k
-  // (low word: contexts 0-3, high word: 4-5); FrameIn::coef_pk, copied to
-  // shared memory on the device.
+  // Token cache (1024 entries) and the frame's coefficient probabilities as
+  // 32-bit words: node k of band b of a (tx size, plane type, reference
+  // type) at 36 * index + 6 b + 2 k (low word: contexts 0-3, high word: 4-5),
+  // FrameIn::coef_pk. On the device both are the kernel's shared arrays
+  // (TP_TC, TP_PKW).
+  uint8_t* tc;
   const uint32_t* pkw;
   uint8_t left_nz[3][16];
   uint8_t left_part[8];
@@ -489,7 +506,11 @@ struct TileParser {
     }
   }
 
-  TP_HD void decode_block(uint32_t r, uint32_t c, uint8_t subsize) {
+  // One block: its mode info with the decoder's state in registers (the
+  // mode-info functions are inlined here, and the block is decoded out of
+  // line once rather than inlined at each of its callers), then its
+  // residual and records.
+  TP_NOINL void decode_block(uint32_t r, uint32_t c, uint8_t subsize) {
     if (err) return;
     if (ss_x + ss_y > 0 && subsize >= 3 && T->ss_size[subsize][ss_x][ss_y] == 14) {
       fail(TP_CHROMA_BLOCK);
@@ -505,10 +526,14 @@ struct TileParser {
     b.left = b.avail_l ? &mi_at(r, c - 1) : nullptr;
     b.ref_frame[0] = 0;   // INTRA_FRAME
     b.ref_frame[1] = -1;  // NONE
-    if (F->frame_is_intra)
-      intra_frame_mode_info();
-    else
-      inter_frame_mode_info();
+    {
+      Bool rb = bd;
+      if (F->frame_is_intra)
+        intra_frame_mode_info(rb);
+      else
+        inter_frame_mode_info(rb);
+      bd = rb;
+    }
     eob_total = 0;
     if (n_blocks >= cap_blocks) {
       fail(TP_OVERFLOW);
@@ -563,16 +588,16 @@ struct TileParser {
 
   // ---- Mode info (spec 6.4.5 - 6.4.17) ----
 
-  TP_HD void intra_frame_mode_info() {
-    read_skip();
-    read_tx_size(true);
+  TP_INL void intra_frame_mode_info(Bool& r) {
+    read_skip(r);
+    read_tx_size(r, true);
     b.ref_frame[0] = 0;
     b.ref_frame[1] = -1;
     b.is_inter = false;
     if (b.mi_size >= 3) {
       const uint8_t am = b.above ? b.above->sub_modes[2] : 0;
       const uint8_t lm = b.left ? b.left->sub_modes[1] : 0;
-      const uint8_t mode = (uint8_t)bd.tree(T->intra_mode_tree, T->kf_y_mode[am][lm]);
+      const uint8_t mode = (uint8_t)r.tree(T->intra_mode_tree, T->kf_y_mode[am][lm]);
       b.y_mode = mode;
       for (int i = 0; i < 4; ++i) b.sub_modes[i] = mode;
     } else {
@@ -582,21 +607,21 @@ struct TileParser {
         for (int idx = 0; idx < 2; idx += n4w) {
           const uint8_t am = idy > 0 ? b.sub_modes[idx] : (b.above ? b.above->sub_modes[2 + idx] : 0);
           const uint8_t lm = idx > 0 ? b.sub_modes[idy * 2] : (b.left ? b.left->sub_modes[1 + idy * 2] : 0);
-          mode = (uint8_t)bd.tree(T->intra_mode_tree, T->kf_y_mode[am][lm]);
+          mode = (uint8_t)r.tree(T->intra_mode_tree, T->kf_y_mode[am][lm]);
           for (int y2 = 0; y2 < n4h; ++y2)
             for (int x2 = 0; x2 < n4w; ++x2) b.sub_modes[(idy + y2) * 2 + idx + x2] = mode;
         }
       b.y_mode = mode;
     }
-    b.uv_mode = (uint8_t)bd.tree(T->intra_mode_tree, T->kf_uv_mode[b.y_mode]);
+    b.uv_mode = (uint8_t)r.tree(T->intra_mode_tree, T->kf_uv_mode[b.y_mode]);
   }
 
-  TP_INL void read_skip() {
+  TP_INL void read_skip(Bool& r) {
     const int ctx = (b.above ? b.above->skip : 0) + (b.left ? b.left->skip : 0);
-    b.skip = bd.read(F->probs.skip[ctx]);
+    b.skip = r.read(F->probs.skip[ctx]);
   }
 
-  TP_HD void read_tx_size(bool allow_select) {
+  TP_INL void read_tx_size(Bool& r, bool allow_select) {
     const uint8_t max_tx = T->max_tx[b.mi_size];
     if (allow_select && F->tx_mode == 4 /* TX_MODE_SELECT */ && b.mi_size >= 3) {
       uint8_t above = max_tx, left = max_tx;
@@ -606,21 +631,21 @@ struct TileParser {
       if (!b.avail_u) above = left;
       const int ctx = (above + left) > max_tx ? 1 : 0;
       const int8_t* tree = max_tx == 3 ? T->tx32_tree : max_tx == 2 ? T->tx16_tree : T->tx8_tree;
-      b.tx_size = (uint8_t)bd.tree(tree, F->probs.tx[max_tx][ctx]);
+      b.tx_size = (uint8_t)r.tree(tree, F->probs.tx[max_tx][ctx]);
     } else {
       const uint8_t m = T->tx_mode_biggest[F->tx_mode];
       b.tx_size = max_tx < m ? max_tx : m;
     }
   }
 
-  TP_HD void inter_frame_mode_info() {
-    read_skip();
-    read_is_inter();
-    read_tx_size(!b.skip || !b.is_inter);
+  TP_INL void inter_frame_mode_info(Bool& r) {
+    read_skip(r);
+    read_is_inter(r);
+    read_tx_size(r, !b.skip || !b.is_inter);
     if (b.is_inter)
-      inter_block_mode_info();
+      inter_block_mode_info(r);
     else
-      intra_block_mode_info();
+      intra_block_mode_info(r);
   }
 
   TP_INL void left_ref(int8_t out[2]) const {
@@ -632,7 +657,7 @@ struct TileParser {
     out[1] = b.above ? b.above->ref_frame[1] : -1;
   }
 
-  TP_HD void read_is_inter() {
+  TP_INL void read_is_inter(Bool& r) {
     int8_t l[2], a[2];
     left_ref(l);
     above_ref(a);
@@ -645,14 +670,14 @@ struct TileParser {
       ctx = 2 * (au ? above_intra : left_intra);
     else
       ctx = 0;
-    b.is_inter = bd.read(F->probs.is_inter[ctx]);
+    b.is_inter = r.read(F->probs.is_inter[ctx]);
   }
 
-  TP_HD void intra_block_mode_info() {
+  TP_INL void intra_block_mode_info(Bool& r) {
     b.ref_frame[0] = 0;
     b.ref_frame[1] = -1;
     if (b.mi_size >= 3) {
-      const uint8_t mode = (uint8_t)bd.tree(T->intra_mode_tree, F->probs.y_mode[T->size_group[b.mi_size]]);
+      const uint8_t mode = (uint8_t)r.tree(T->intra_mode_tree, F->probs.y_mode[T->size_group[b.mi_size]]);
       b.y_mode = mode;
       for (int i = 0; i < 4; ++i) b.sub_modes[i] = mode;
     } else {
@@ -660,21 +685,21 @@ struct TileParser {
       uint8_t mode = 0;
       for (int idy = 0; idy < 2; idy += n4h)
         for (int idx = 0; idx < 2; idx += n4w) {
-          mode = (uint8_t)bd.tree(T->intra_mode_tree, F->probs.y_mode[0]);
+          mode = (uint8_t)r.tree(T->intra_mode_tree, F->probs.y_mode[0]);
           for (int y2 = 0; y2 < n4h; ++y2)
             for (int x2 = 0; x2 < n4w; ++x2) b.sub_modes[(idy + y2) * 2 + idx + x2] = mode;
         }
       b.y_mode = mode;
     }
-    b.uv_mode = (uint8_t)bd.tree(T->intra_mode_tree, F->probs.uv_mode[b.y_mode]);
+    b.uv_mode = (uint8_t)r.tree(T->intra_mode_tree, F->probs.uv_mode[b.y_mode]);
   }
 
-  TP_HD void inter_block_mode_info() {
-    read_ref_frames();
+  TP_INL void inter_block_mode_info(Bool& r) {
+    read_ref_frames(r);
     for (int j = 0; j < 2; ++j)
       if (b.ref_frame[j] > 0) find_best_ref_mvs(j);
     const bool is_compound = b.ref_frame[1] > 0;
-    if (b.mi_size >= 3) b.y_mode = (uint8_t)(10 /* NEARESTMV */ + read_inter_mode());
+    if (b.mi_size >= 3) b.y_mode = (uint8_t)(10 /* NEARESTMV */ + read_inter_mode(r));
     if (F->interp_filter == 4 /* SWITCHABLE */) {
       int8_t l[2], a[2];
       left_ref(l);
@@ -690,7 +715,7 @@ struct TileParser {
         ctx = left_interp;
       else
         ctx = 3;
-      b.interp_filter = (uint8_t)bd.tree(T->interp_tree, F->probs.interp_filter[ctx]);
+      b.interp_filter = (uint8_t)r.tree(T->interp_tree, F->probs.interp_filter[ctx]);
     } else {
       b.interp_filter = F->interp_filter;
     }
@@ -699,10 +724,10 @@ struct TileParser {
       const int n4w = T->n4w[b.mi_size], n4h = T->n4h[b.mi_size];
       for (int idy = 0; idy < 2; idy += n4h)
         for (int idx = 0; idx < 2; idx += n4w) {
-          b.y_mode = (uint8_t)(10 + read_inter_mode());
+          b.y_mode = (uint8_t)(10 + read_inter_mode(r));
           if (b.y_mode == 10 || b.y_mode == 11 /* NEARMV */)
             for (int j = 0; j < nrefs; ++j) append_sub8x8_mvs(idy * 2 + idx, j);
-          assign_mv(is_compound);
+          assign_mv(r, is_compound);
           for (int y2 = 0; y2 < n4h; ++y2)
             for (int x2 = 0; x2 < n4w; ++x2) {
               const int blk = (idy + y2) * 2 + idx + x2;
@@ -710,31 +735,31 @@ struct TileParser {
             }
         }
     } else {
-      assign_mv(is_compound);
+      assign_mv(r, is_compound);
       for (int rl = 0; rl < nrefs; ++rl)
         for (int k = 0; k < 4; ++k) b.block_mvs[rl][k] = b.mv[rl];
     }
   }
 
-  TP_INL int read_inter_mode() {
-    return bd.tree(T->inter_mode_tree, F->probs.inter_mode[b.mode_context[b.ref_frame[0]]]);
+  TP_INL int read_inter_mode(Bool& r) {
+    return r.tree(T->inter_mode_tree, F->probs.inter_mode[b.mode_context[b.ref_frame[0]]]);
   }
 
-  TP_HD void read_ref_frames() {
+  TP_INL void read_ref_frames(Bool& r) {
     int comp_mode;
     if (F->reference_mode == 2 /* REFERENCE_MODE_SELECT */)
-      comp_mode = bd.read(F->probs.comp_mode[comp_mode_ctx()]) ? 1 : 0;
+      comp_mode = r.read(F->probs.comp_mode[comp_mode_ctx()]) ? 1 : 0;
     else
       comp_mode = F->reference_mode;
     if (comp_mode == 1 /* COMPOUND_REFERENCE */) {
       const int idx = F->sign_bias[F->comp_fixed_ref] ? 1 : 0;
-      const bool v = bd.read(F->probs.comp_ref[comp_ref_ctx()]);
+      const bool v = r.read(F->probs.comp_ref[comp_ref_ctx()]);
       b.ref_frame[idx] = F->comp_fixed_ref;
       b.ref_frame[1 - idx] = F->comp_var_ref[v ? 1 : 0];
     } else {
-      const bool p1 = bd.read(F->probs.single_ref[single_ref_p1_ctx()][0]);
+      const bool p1 = r.read(F->probs.single_ref[single_ref_p1_ctx()][0]);
       if (p1) {
-        const bool p2 = bd.read(F->probs.single_ref[single_ref_p2_ctx()][1]);
+        const bool p2 = r.read(F->probs.single_ref[single_ref_p2_ctx()][1]);
         b.ref_frame[0] = p2 ? 3 : 2;
       } else {
         b.ref_frame[0] = 1;
@@ -888,11 +913,11 @@ struct TileParser {
     return 2;
   }
 
-  TP_HD void assign_mv(bool is_compound) {
+  TP_INL void assign_mv(Bool& r, bool is_compound) {
     b.mv[1] = Mv{0, 0};
     for (int i = 0; i < 1 + (is_compound ? 1 : 0); ++i) {
       switch (b.y_mode) {
-        case 13 /* NEWMV */: b.mv[i] = read_mv(i); break;
+        case 13 /* NEWMV */: b.mv[i] = read_mv(r, i); break;
         case 10: b.mv[i] = b.nearest_mv[i]; break;
         case 11: b.mv[i] = b.near_mv[i]; break;
         default: b.mv[i] = Mv{0, 0}; break;
@@ -900,32 +925,32 @@ struct TileParser {
     }
   }
 
-  TP_HD Mv read_mv(int r) {
-    const Mv best = b.best_mv[r];
+  TP_INL Mv read_mv(Bool& r, int rl) {
+    const Mv best = b.best_mv[rl];
     const bool use_hp = F->allow_hp && use_mv_hp(best);
     int32_t diff[2] = {0, 0};
-    const int joint = bd.tree(T->mv_joint_tree, F->probs.mv_joint);
-    if (joint == 2 /* HZVNZ */ || joint == 3 /* HNZVNZ */) diff[0] = read_mv_component(0, use_hp);
-    if (joint == 1 /* HNZVZ */ || joint == 3) diff[1] = read_mv_component(1, use_hp);
+    const int joint = r.tree(T->mv_joint_tree, F->probs.mv_joint);
+    if (joint == 2 /* HZVNZ */ || joint == 3 /* HNZVNZ */) diff[0] = read_mv_component(r, 0, use_hp);
+    if (joint == 1 /* HNZVZ */ || joint == 3) diff[1] = read_mv_component(r, 1, use_hp);
     return Mv{best.r + diff[0], best.c + diff[1]};
   }
 
-  TP_HD int32_t read_mv_component(int comp, bool use_hp) {
+  TP_INL int32_t read_mv_component(Bool& r, int comp, bool use_hp) {
     const rv9::Probs& pr = F->probs;
-    const bool sign = bd.read(pr.mv_sign[comp]);
-    const int cls = bd.tree(T->mv_class_tree, pr.mv_class[comp]);
+    const bool sign = r.read(pr.mv_sign[comp]);
+    const int cls = r.tree(T->mv_class_tree, pr.mv_class[comp]);
     int32_t mag;
     if (cls == 0) {
-      const int c0 = bd.read(pr.mv_class0_bit[comp]) ? 1 : 0;
-      const int fr = bd.tree(T->mv_fr_tree, pr.mv_class0_fr[comp][c0]);
-      const int hp = use_hp ? (bd.read(pr.mv_class0_hp[comp]) ? 1 : 0) : 1;
+      const int c0 = r.read(pr.mv_class0_bit[comp]) ? 1 : 0;
+      const int fr = r.tree(T->mv_fr_tree, pr.mv_class0_fr[comp][c0]);
+      const int hp = use_hp ? (r.read(pr.mv_class0_hp[comp]) ? 1 : 0) : 1;
       mag = ((c0 << 3) | (fr << 1) | hp) + 1;
     } else {
       int32_t dd = 0;
-      for (int i = 0; i < cls; ++i) dd |= (bd.read(pr.mv_bits[comp][i]) ? 1 : 0) << i;
+      for (int i = 0; i < cls; ++i) dd |= (r.read(pr.mv_bits[comp][i]) ? 1 : 0) << i;
       const int32_t m0 = 2 << (cls + 2);
-      const int fr = bd.tree(T->mv_fr_tree, pr.mv_fr[comp]);
-      const int hp = use_hp ? (bd.read(pr.mv_hp[comp]) ? 1 : 0) : 1;
+      const int fr = r.tree(T->mv_fr_tree, pr.mv_fr[comp]);
+      const int hp = use_hp ? (r.read(pr.mv_hp[comp]) ? 1 : 0) : 1;
       mag = m0 + ((dd << 3) | (fr << 1) | hp) + 1;
     }
     return sign ? -mag : mag;
@@ -937,46 +962,11 @@ struct TileParser {
     return r >= 0 && r < (int32_t)mi_rows && c >= (int32_t)mi_col_start && c < (int32_t)mi_col_end;
   }
 
-  TP_INL void get_block_mv(Search& s, int32_t r, int32_t c, int ref_list, bool use_prev) const {
-    if (use_prev) {
-      const PrevMv& p = prev[(size_t)r * mi_cols + c];
-      s.cand_mv[ref_list] = p.mv[ref_list];
-      s.cand_frame[ref_list] = p.ref_frame[ref_list];
-    } else {
-      const Mi& m = mi_at(r, c);
-      s.cand_mv[ref_list] = m.mv[ref_list][3];
-      s.cand_frame[ref_list] = m.ref_frame[ref_list];
-    }
-  }
-
-  TP_HD void if_same_ref_frame_add(Search& s, int32_t r, int32_t c, int8_t ref_frame, bool use_prev) const {
-    for (int j = 0; j < 2; ++j) {
-      get_block_mv(s, r, c, j, use_prev);
-      if (s.cand_frame[j] == ref_frame) {
-        s.add(j);
-        return;
-      }
-    }
-  }
-
   TP_INL void scale_mv(Search& s, int ref_list, int8_t ref_frame) const {
     const int8_t cand = s.cand_frame[ref_list];
     if (F->sign_bias[cand] != F->sign_bias[ref_frame]) {
       s.cand_mv[ref_list].r *= -1;
       s.cand_mv[ref_list].c *= -1;
-    }
-  }
-
-  TP_HD void if_diff_ref_frame_add(Search& s, int32_t r, int32_t c, int8_t ref_frame, bool use_prev) const {
-    for (int j = 0; j < 2; ++j) get_block_mv(s, r, c, j, use_prev);
-    const bool mvs_same = mv_eq(s.cand_mv[0], s.cand_mv[1]);
-    if (s.cand_frame[0] > 0 && s.cand_frame[0] != ref_frame) {
-      scale_mv(s, 0, ref_frame);
-      s.add(0);
-    }
-    if (s.cand_frame[1] > 0 && s.cand_frame[1] != ref_frame && !mvs_same) {
-      scale_mv(s, 1, ref_frame);
-      s.add(1);
     }
   }
 
@@ -998,42 +988,98 @@ struct TileParser {
     return v < lo ? lo : (v > hi ? hi : v);
   }
 
-  // find_mv_refs( refFrame, block ) (spec 6.5.1).
+  // The candidate searches of find_mv_refs on values already loaded: a
+  // candidate's two reference frames and the motion vectors it offers.
+  TP_INL static void same_add(Search& s, const int8_t rf[2], const Mv mv[2], int8_t ref_frame) {
+    for (int j = 0; j < 2; ++j) {
+      s.cand_mv[j] = mv[j];
+      s.cand_frame[j] = rf[j];
+      if (rf[j] == ref_frame) {
+        s.add(j);
+        return;
+      }
+    }
+  }
+  TP_INL void diff_add(Search& s, const int8_t rf[2], const Mv mv[2], int8_t ref_frame) const {
+    s.cand_mv[0] = mv[0];
+    s.cand_mv[1] = mv[1];
+    s.cand_frame[0] = rf[0];
+    s.cand_frame[1] = rf[1];
+    const bool mvs_same = mv_eq(s.cand_mv[0], s.cand_mv[1]);
+    if (s.cand_frame[0] > 0 && s.cand_frame[0] != ref_frame) {
+      scale_mv(s, 0, ref_frame);
+      s.add(0);
+    }
+    if (s.cand_frame[1] > 0 && s.cand_frame[1] != ref_frame && !mvs_same) {
+      scale_mv(s, 1, ref_frame);
+      s.add(1);
+    }
+  }
+
+  // find_mv_refs( refFrame, block ) (spec 6.5.1). The eight neighbours' mode
+  // info is loaded first, all loads at once (it sits in L2, written by this
+  // thread earlier), then searched in the specification's order.
   TP_HD void find_mv_refs(int8_t ref_frame, int block, Mv out[2]) {
     Search s;
     s.count = 0;
     s.list[0] = s.list[1] = Mv{0, 0};
     s.cand_mv[0] = s.cand_mv[1] = Mv{0, 0};
     s.cand_frame[0] = s.cand_frame[1] = 0;
-    int context_counter = 0;
     const int8_t(*search)[2] = T->mv_ref_blocks[b.mi_size];
     const int32_t mi_row = (int32_t)b.mi_row, mi_col = (int32_t)b.mi_col;
-    for (int i = 0; i < 2; ++i) {
+    bool in[8];
+    int8_t rf[8][2];
+    Mv mv3[8][2];    // the neighbour's vectors of its last 4x4 (sub-block 3)
+    Mv first[2][2];  // the first two neighbours' vectors of the sub-block next to `block`
+    uint8_t ym[2];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
       const int32_t r = mi_row + search[i][0], c = mi_col + search[i][1];
-      if (is_inside(r, c)) {
+      in[i] = is_inside(r, c);
+      rf[i][0] = rf[i][1] = 0;
+      mv3[i][0] = mv3[i][1] = Mv{0, 0};
+      if (in[i]) {
         const Mi& m = mi_at(r, c);
-        context_counter += T->mode_2_counter[m.y_mode];
-        for (int j = 0; j < 2; ++j) {
-          if (m.ref_frame[j] == ref_frame) {
-            const int idx = block >= 0 ? T->idx_n_col_to_sub[block][search[i][1] == 0 ? 1 : 0] : 3;
-            s.cand_mv[j] = m.mv[j][idx];
-            s.add(j);
-            break;
-          }
+        rf[i][0] = m.ref_frame[0];
+        rf[i][1] = m.ref_frame[1];
+        mv3[i][0] = m.mv[0][3];
+        mv3[i][1] = m.mv[1][3];
+        if (i < 2) {
+          ym[i] = m.y_mode;
+          const int idx = block >= 0 ? T->idx_n_col_to_sub[block][search[i][1] == 0 ? 1 : 0] : 3;
+          first[i][0] = m.mv[0][idx];
+          first[i][1] = m.mv[1][idx];
         }
       }
     }
-    for (int i = 2; i < 8; ++i) {
-      const int32_t r = mi_row + search[i][0], c = mi_col + search[i][1];
-      if (is_inside(r, c)) if_same_ref_frame_add(s, r, c, ref_frame, false);
+    int context_counter = 0;
+    for (int i = 0; i < 2; ++i) {
+      if (!in[i]) continue;
+      context_counter += T->mode_2_counter[ym[i]];
+      for (int j = 0; j < 2; ++j) {
+        if (rf[i][j] == ref_frame) {
+          s.cand_mv[j] = first[i][j];
+          s.add(j);
+          break;
+        }
+      }
     }
+    for (int i = 2; i < 8; ++i)
+      if (in[i]) same_add(s, rf[i], mv3[i], ref_frame);
     const bool use_prev = prev != nullptr;
-    if (use_prev) if_same_ref_frame_add(s, mi_row, mi_col, ref_frame, true);
-    for (int i = 0; i < 8; ++i) {
-      const int32_t r = mi_row + search[i][0], c = mi_col + search[i][1];
-      if (is_inside(r, c)) if_diff_ref_frame_add(s, r, c, ref_frame, false);
+    int8_t prf[2] = {0, 0};
+    Mv pmv[2] = {{0, 0}, {0, 0}};
+    if (use_prev) {
+      const PrevMv& pv = prev[(size_t)mi_row * mi_cols + mi_col];
+      prf[0] = pv.ref_frame[0];
+      prf[1] = pv.ref_frame[1];
+      pmv[0] = pv.mv[0];
+      pmv[1] = pv.mv[1];
+      same_add(s, prf, pmv, ref_frame);
     }
-    if (use_prev) if_diff_ref_frame_add(s, mi_row, mi_col, ref_frame, true);
+    for (int i = 0; i < 8; ++i)
+      if (in[i]) diff_add(s, rf[i], mv3[i], ref_frame);
+    if (use_prev) diff_add(s, prf, pmv, ref_frame);
     b.mode_context[ref_frame] = T->counter_to_ctx[context_counter];
     for (int i = 0; i < 2; ++i) {
       s.list[i].r = clamp_mv_row(s.list[i].r, 128 /* MV_BORDER */);
@@ -1171,19 +1217,43 @@ struct TileParser {
     }
     const int kind = ttype == 2 /* DCT_ADST */ ? 1 : ttype == 1 /* ADST_DCT */ ? 2 : 0;
     const ScanEnt* sc = T->scan[tx_sz][kind];
-    const uint32_t* pk = pkw + 36 * ((tx_sz * 2 + ptype) * 2 + ref_type);
+    const uint32_t pkb = 36 * ((tx_sz * 2 + ptype) * 2 + ref_type);
     const uint32_t bd_bits = F->bit_depth;
     const uint32_t coef0 = n_coefs;
     uint32_t* out = coefs + n_coefs;
     uint32_t n_out = 0;
     int c = 0;
-    // The current scan index's entry and band words, the next entry loaded
-    // ahead, and the context as a byte selector (bytes 6 and 7 of a band
-    // word are zero, so the selector 0x7770 | ctx yields the byte alone).
+    // The loop keeps the current scan index's entry `e`, its band's six
+    // probability words `w` (in registers) and its context; and, loaded a
+    // step ahead so that no load waits on the decode, the next entry `en`,
+    // its band's words `wn` and the token energies of its two context
+    // neighbours (t0, t1). A neighbour of `en` may be the current position,
+    // whose energy is only known once its token is decoded: advance()
+    // substitutes it. Bytes 6 and 7 of a band word are zero, so the selector
+    // 0x7770 | ctx yields the context's probability byte alone.
     ScanEnt e = ld_scan(sc);
     ScanEnt en = ld_scan(sc + 1);
-    const uint32_t* w = pk + 6 * e.band;
+    uint32_t w[6], wn[6];
+    auto band = [&](uint32_t* dst, uint32_t b) {
+      const uint32_t o = pkb + 6 * b;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dst[k] = TP_PKW(o + k);
+    };
+    band(w, e.band);
+    band(wn, en.band);
+    uint32_t t0 = TP_TC(en.nb0), t1 = TP_TC(en.nb1);
     uint32_t ctx = above + left;
+    // After the token at e.pos (energy `cur`, already stored) and ++c.
+    auto advance = [&](uint32_t cur) {
+      ctx = (1 + (en.nb0 == e.pos ? cur : t0) + (en.nb1 == e.pos ? cur : t1)) >> 1;
+      e = en;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) w[k] = wn[k];
+      en = ld_scan(sc + (c + 1 < seg_eob ? c + 1 : c));
+      band(wn, en.band);
+      t0 = TP_TC(en.nb0);
+      t1 = TP_TC(en.nb1);
+    };
     Bool r = bd;
     while (true) {
       // more_coefs: read at the start and after every nonzero token.
@@ -1191,22 +1261,20 @@ struct TileParser {
       // A run of zero tokens; after a zero token no more_coefs is read.
       bool done = false;
       while (!r.read(byte_perm(w[2], w[3], 0x7770u | ctx))) {
-        tc[e.pos] = 0;
+        TP_TC(e.pos) = 0;
         if (++c == seg_eob) {
           done = true;
           break;
         }
-        e = en;
-        en = ld_scan(sc + (c + 1 < seg_eob ? c + 1 : c));
-        w = pk + 6 * e.band;
-        ctx = (1 + tc[e.nb0] + tc[e.nb1]) >> 1;
+        advance(0);
       }
       if (done) break;
       int32_t coef;
+      uint32_t energy;
       const uint32_t p2 = byte_perm(w[4], w[5], 0x7770u | ctx);
       if (!r.read(p2)) {
         coef = 1;  // ONE_TOKEN
-        tc[e.pos] = 1;
+        energy = 1;
       } else {
         // The rest of the token tree, its probabilities from one pareto row.
         const uint2 pp = ro(reinterpret_cast<const uint2*>(T->pareto[p2]));
@@ -1216,7 +1284,7 @@ struct TileParser {
           n = ro(&T->token_tree[n + (int)r.read(pr)]);
         } while (n > 0);
         const int token = -n;
-        tc[e.pos] = ro(&T->energy[token]);
+        energy = ro(&T->energy[token]);
         coef = ro(&T->extra_bits[token][2]);
         const int num_extra = ro(&T->extra_bits[token][1]);
         if (num_extra) {
@@ -1226,13 +1294,11 @@ struct TileParser {
           for (int k = 0; k < num_extra; ++k) coef += (int32_t)r.read(ro(&cat[k])) << (num_extra - 1 - k);
         }
       }
+      TP_TC(e.pos) = (uint8_t)energy;
       const bool sign = r.read(128);
       out[n_out++] = RV9_COEF_PACK(e.pos, sign ? -coef : coef);
       if (++c == seg_eob) break;
-      e = en;
-      en = ld_scan(sc + (c + 1 < seg_eob ? c + 1 : c));
-      w = pk + 6 * e.band;
-      ctx = (1 + tc[e.nb0] + tc[e.nb1]) >> 1;
+      advance(energy);
     }
     bd = r;
     n_coefs += n_out;
