@@ -467,6 +467,27 @@ def run_batched(local, dev):
     }
     for sq in seqs:
         sq.free()
+    # End to end from host packets: each stream on its own decoder and host
+    # thread through rv9_decode_packets, its frames back to pinned host
+    # memory; host parsing, then device parsing (16-frame batches per stream,
+    # all streams' batches on the GPU at once). The first pass of each grows
+    # the decoders' buffers; the second is timed. Every frame is checked.
+    outs = [torch.empty(sum(sz) + (1 << 20), dtype=torch.uint8, pin_memory=True) for sz in sizes]
+    e2e = {}
+    for mode, window in (("host_parse", 0), ("device_parse", 16)):
+        for d in decs:
+            d.set_device_parse(window > 0, window)
+        dt, results = None, None
+        for _ in range(2):
+            dt, results = e2e_pass(decs, contents, outs)
+        md5s = [frame_md5s(o[:nb].numpy(), sz) for o, (_, nb), sz in zip(outs, results, sizes)]
+        e2e[mode] = {"value": round(luma / dt / 1e6, 2), "unit": "Mpixels/s", "seconds": round(dt, 3),
+                     "bit_exact": all(m == [x for x, _ in w] for m, w in zip(md5s, want))}
+    e2e["how"] = ("64 decoders, each stream's 60 packets through rv9_decode_packets on its own host thread "
+                  f"({os.cpu_count()} host cores), frames copied back to pinned host memory; device_parse: "
+                  "rv9_decoder_set_device_parse(1, 16)")
+    out["e2e"] = e2e
+    del outs
     for d in decs:
         d.close()
     return out
@@ -741,15 +762,50 @@ def run_gpu(args, world, rank, local):
     e2e_secs = dist_max(e2e_secs, world, dev)
     e2e_value = luma_per_step * e2e_steps * world / e2e_secs / 1e6
     e2e_md5s = [frame_md5s(o[:nb].numpy(), sz) for o, (_, nb), sz in zip(host_outs, results, sizes)]
+    # The same end-to-end passes with device parsing (rv9_decoder_set_device_parse):
+    # every frame's tile columns parsed on the GPU and its work lists built
+    # there; the host keeps the frame headers.
+    for d in decs:
+        d.set_device_parse(True, 64)
+    dp_secs, dp_each, dp_results = 0.0, [], None
+    dp0 = [d.device_parse_stats() for d in decs]
+    for i in range(e2e_steps + 1):
+        dist_barrier(world)
+        dt, dp_results = e2e_pass(decs, packets, host_outs)
+        if i == 0:
+            dp0 = [d.device_parse_stats() for d in decs]
+        else:
+            dp_secs += dt
+            dp_each.append(round(dt * 1e3, 1))
+    dp1 = [d.device_parse_stats() for d in decs]
+    for d in decs:
+        d.set_device_parse(False)
+    dp_secs = dist_max(dp_secs, world, dev)
+    dp_md5s = [frame_md5s(o[:nb].numpy(), sz) for o, (_, nb), sz in zip(host_outs, dp_results, sizes)]
+    dp_bools = sum(b[1] - a[1] for a, b in zip(dp0, dp1)) / e2e_steps
+    dp_ms = [(b[2] - a[2]) / e2e_steps for a, b in zip(dp0, dp1)]
+    e2e_device_parse = {
+        "value": round(luma_per_step * e2e_steps * world / dp_secs / 1e6, 2), "unit": "Mpixels/s",
+        "steps": e2e_steps, "ms_each_step": dp_each,
+        "frames_device_parsed_per_step": int(sum(b[0] - a[0] for a, b in zip(dp0, dp1)) / e2e_steps),
+        "bools_per_step": int(dp_bools),
+        "parse_device_ms_per_stream": [round(m, 1) for m in dp_ms],
+        "how": "rv9_decode_packets with rv9_decoder_set_device_parse(1, 64): each stream's 60 frames go to the "
+               "GPU as one batch (one thread per tile column, 240 columns per stream; then one CTA per frame "
+               "builds its work lists), reconstructed in order as usual; parse_device_ms is the batch's CUDA-event "
+               "time on its stream (the two streams' batches overlap)",
+    }
     del host_outs
     check = {"how": "per-frame MD5 of every shown frame of both streams, from an untimed replay (frame sinks) "
                     "and from the last end-to-end pass, against the oracle's decode of the same packets"}
     if want:
-        for s, w, r, e in zip(W.CONFIG2, want, replay_md5s, e2e_md5s):
+        for s, w, r, e, dp in zip(W.CONFIG2, want, replay_md5s, e2e_md5s, dp_md5s):
             check[f"replay_{s['name']}"] = compare(r, [m for m, _ in w])
             check[f"e2e_{s['name']}"] = compare(e, [m for m, _ in w])
+            check[f"e2e_device_parse_{s['name']}"] = compare(dp, [m for m, _ in w])
     else:
         check["e2e_equals_replay"] = e2e_md5s == replay_md5s
+        check["e2e_device_parse_equals_replay"] = dp_md5s == replay_md5s
     extra = {}
     sections = args.sections.split(",") if world == 1 else []
     if "config3" in sections:
@@ -773,6 +829,7 @@ def run_gpu(args, world, rank, local):
                     "note": "the generator writes error-resilient, single-reference inter frames (no compound "
                             "prediction, no backward adaptation), as the reference's own encoder does; the 15 "
                             "conformance vectors cover the rest for parity"},
+            "e2e_device_parse": e2e_device_parse,
             "roofline": roofline,
             "autotune": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in tuned.items()},
             "graph_replay": {"value": round(whole_job_value(luma_per_step, world, ms_graph), 2),
