@@ -1276,22 +1276,38 @@ struct TileParser {
         coef = 1;  // ONE_TOKEN
         energy = 1;
       } else {
-        // The rest of the token tree, its probabilities from one pareto row.
+        // The rest of the token tree (TOKEN_TREE from node 4), its node
+        // probabilities from one pareto row, walked as its fixed branches:
+        // no table load waits between two decodes.
         const uint2 pp = ro(reinterpret_cast<const uint2*>(T->pareto[p2]));
-        int n = 4;
-        do {
-          const uint32_t pr = byte_perm(pp.x, pp.y, (uint32_t)((n >> 1) - 2)) & 0xffu;
-          n = ro(&T->token_tree[n + (int)r.read(pr)]);
-        } while (n > 0);
-        const int token = -n;
-        energy = ro(&T->energy[token]);
-        coef = ro(&T->extra_bits[token][2]);
-        const int num_extra = ro(&T->extra_bits[token][1]);
-        if (num_extra) {
-          if (token == 10 /* DCT_VAL_CAT6 */)
+        auto pr = [&](uint32_t k) { return byte_perm(pp.x, pp.y, k) & 0xffu; };
+        int cat = 0;  // DCT_VAL_CATEGORY1..6 as 1..6; 0: TWO, THREE or FOUR
+        if (!r.read(pr(0))) {
+          if (!r.read(pr(1))) {
+            coef = 2;  // TWO_TOKEN
+            energy = 2;
+          } else {
+            coef = r.read(pr(2)) ? 4 : 3;  // FOUR_TOKEN : THREE_TOKEN
+            energy = 3;
+          }
+        } else if (!r.read(pr(3))) {
+          cat = r.read(pr(4)) ? 2 : 1;
+          energy = 4;
+        } else if (!r.read(pr(5))) {
+          cat = r.read(pr(6)) ? 4 : 3;
+          energy = 5;
+        } else {
+          cat = r.read(pr(7)) ? 6 : 5;
+          energy = 5;
+        }
+        if (cat) {
+          // The category's base value and extra bits (spec 9.3: extra_bits).
+          const int num_extra = cat == 6 ? 14 : cat;
+          coef = cat == 6 ? 67 : cat == 5 ? 35 : cat == 4 ? 19 : cat == 3 ? 11 : cat == 2 ? 7 : 5;
+          if (cat == 6)
             for (int k = 0; k < (int)bd_bits - 8; ++k) coef += (int32_t)r.read(255) << (5 + (int)bd_bits - k);
-          const uint8_t* cat = T->cat_probs[ro(&T->extra_bits[token][0])];
-          for (int k = 0; k < num_extra; ++k) coef += (int32_t)r.read(ro(&cat[k])) << (num_extra - 1 - k);
+          const uint8_t* probs = T->cat_probs[cat];
+          for (int k = 0; k < num_extra; ++k) coef += (int32_t)r.read(ro(&probs[k])) << (num_extra - 1 - k);
         }
       }
       TP_TC(e.pos) = (uint8_t)energy;
