@@ -469,12 +469,14 @@ def run_batched(local, dev):
         sq.free()
     # End to end from host packets: each stream on its own decoder and host
     # thread through rv9_decode_packets, its frames back to pinned host
-    # memory; host parsing, then device parsing (16-frame batches per stream,
+    # memory; host parsing, then device parsing (32-frame batches per stream,
     # all streams' batches on the GPU at once). The first pass of each grows
-    # the decoders' buffers; the second is timed. Every frame is checked.
+    # the decoders' buffers (both of a device parser's alternating stage
+    # buffers: two batches per stream); the second is timed. Every frame is
+    # checked.
     outs = [torch.empty(sum(sz) + (1 << 20), dtype=torch.uint8, pin_memory=True) for sz in sizes]
     e2e = {}
-    for mode, window in (("host_parse", 0), ("device_parse", 16)):
+    for mode, window in (("host_parse", 0), ("device_parse", 32)):
         for d in decs:
             d.set_device_parse(window > 0, window)
         dt, results = None, None
@@ -485,7 +487,7 @@ def run_batched(local, dev):
                      "bit_exact": all(m == [x for x, _ in w] for m, w in zip(md5s, want))}
     e2e["how"] = ("64 decoders, each stream's 60 packets through rv9_decode_packets on its own host thread "
                   f"({os.cpu_count()} host cores), frames copied back to pinned host memory; device_parse: "
-                  "rv9_decoder_set_device_parse(1, 16)")
+                  "rv9_decoder_set_device_parse(1, 32)")
     out["e2e"] = e2e
     del outs
     for d in decs:
@@ -769,10 +771,12 @@ def run_gpu(args, world, rank, local):
         d.set_device_parse(True, 64)
     dp_secs, dp_each, dp_results = 0.0, [], None
     dp0 = [d.device_parse_stats() for d in decs]
-    for i in range(e2e_steps + 1):
+    # Two untimed passes: a call is one batch per stream, and batches
+    # alternate between two stage buffers, each allocated on first use.
+    for i in range(e2e_steps + 2):
         dist_barrier(world)
         dt, dp_results = e2e_pass(decs, packets, host_outs)
-        if i == 0:
+        if i <= 1:
             dp0 = [d.device_parse_stats() for d in decs]
         else:
             dp_secs += dt
