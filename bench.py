@@ -495,8 +495,12 @@ def run_batched(local, dev):
     return out
 
 
+SERVED_FORMS = (("per_stream", {}), ("batched", {"groups": 2}),
+                ("per_stream_device_parse", {"device_parse": True, "window": 8}))
+
+
 def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4000, 120)), n_streams=32, frames=120,
-               seed=5):
+               seed=5, forms_run=SERVED_FORMS):
     """The serving loop: 32 live streams (40% 720p, 40% 1080p, 20% 2160p;
     8/10-bit), requests arriving as a Poisson process at each total rate;
     throughput and per-request latency (submit -> frames in host memory).
@@ -559,11 +563,12 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
     hashes = []
     checked, mismatches = 0, []
     forms = {}
-    for form, groups in (("per_stream", 0), ("batched", 2)):
+    dp_stats = {}
+    for form, opts in forms_run:
         results = []
         for rate, nfr in rates:
             every = 1 if rate == rates[0][0] else 8
-            eng = server.Engine(local, hbm_budget=120 << 30, groups=groups)
+            eng = server.Engine(local, hbm_budget=120 << 30, **opts)
             sids = [eng.open_stream(spec[n]["width"], spec[n]["height"], spec[n]["bit_depth"]) for n in mix]
             # Set-up, untimed: every stream admitted (its reservation allocated)
             # and its first frame (a keyframe) decoded.
@@ -605,6 +610,9 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
                 done += got
             wall = time.perf_counter() - t0
             feeder.join()
+            if opts.get("device_parse"):
+                st = eng.stats()
+                dp_stats[f"{form}@{rate}"] = {"batches": st["device_parse_batches"], "frames": st["device_parsed_frames"]}
             for sid in sids:
                 eng.close_stream(sid)
             eng.close()
@@ -625,12 +633,19 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
         forms[form] = results
     pool.shutdown()
     best = max(r["mpixels_s"] for rs in forms.values() for r in rs)
-    return {"workload": f"{n_streams} streams: 13 x 720p, 13 x 1080p, 6 x 2160p, 8/10-bit 4:2:0, q60, "
+    others = {"rates_" + f: rs for f, rs in forms.items()
+              if f not in ("batched", "per_stream", "per_stream_device_parse")}
+    return {**others, "workload": f"{n_streams} streams: 13 x 720p, 13 x 1080p, 6 x 2160p, 8/10-bit 4:2:0, q60, "
                         f"{W.CLASS_FRAMES} frames looped to {frames}; Poisson arrivals; HBM budget 120 GB",
-            "rates": forms["batched"], "rates_per_stream": forms["per_stream"],
+            "rates": forms.get("batched"), "rates_per_stream": forms.get("per_stream"),
+            "rates_device_parse": forms.get("per_stream_device_parse"),
+            "device_parse_batches": dp_stats or None,
             "forms": {"batched": "rv9_engine_create_batched, 2 launch groups: the next parsed frame of every stream "
                                  "of a group reconstructed together, one launch per stage per step",
-                      "per_stream": "rv9_engine_create: each stream's frames on its own CUDA stream"},
+                      "per_stream": "rv9_engine_create: each stream's frames on its own CUDA stream",
+                      "per_stream_device_parse": "rv9_engine_create + rv9_engine_set_device_parse (window 8): a "
+                                                 "stream's queued requests parsed on the GPU as one batch, lone "
+                                                 "requests on the host"},
             "plain_single_stream_e2e_mpixels_s": round(plain, 1),
             "best_vs_plain": round(best / plain, 2),
             "plain_decode_all_mpixels_s": round(plain_da, 1), "best_vs_decode_all": round(best / plain_da, 2),
@@ -641,7 +656,7 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
                        "their first frame decoded before the timed arrivals",
             "bit_exact_check": {"how": "MD5 of each checked request's frames (copied out as it is polled, hashed on "
                                        "other threads) against the oracle's decode of the stream's content: every "
-                                       "request at the lowest rate, every eighth at the others, both forms",
+                                       "request at the lowest rate, every eighth at the others, every form",
                                 "requests": checked, "equal": checked > 0 and not mismatches,
                                 "mismatches": mismatches[:5]},
             "host_cores": os.cpu_count()}

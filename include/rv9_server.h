@@ -46,6 +46,21 @@ rv9_engine* rv9_engine_create_batched(int device, uint64_t hbm_budget_bytes, uin
 /* Closes every stream, waits for their submitted requests, then frees the
  * engine, with any completions not yet released. */
 void rv9_engine_free(rv9_engine* eng);
+/* Device parsing for the streams opened after this call (plain form only;
+ * RV9_UNSUPPORTED for a batched engine). A worker that takes a stream with
+ * two or more queued requests takes up to `window` of them (0: 8, at most
+ * 64) and parses their frames on the GPU as one batch, as
+ * rv9_decoder_set_device_parse does; a lone request is parsed on the host as
+ * before, and so is any frame the device parser does not take. At most
+ * `max_batches` batches are on the device at once (0: one per host worker);
+ * the engine adds that many workers, which sleep while their batch parses,
+ * so the host keeps parsing other streams meanwhile. Each such stream keeps
+ * `window` output buffers and reserves room for a batch's device records
+ * (rv9_stream_reservation plus the device parser's buffers). A frame that
+ * fails fails its request and the requests of the same batch after it.
+ * `on` = 0 turns it off for streams opened later. Results are bit-identical
+ * to host parsing. */
+rv9_status rv9_engine_set_device_parse(rv9_engine* eng, int on, uint32_t window, uint32_t max_batches);
 
 /* The largest frame a stream will carry, which sizes its reservation. */
 typedef struct rv9_stream_spec {
@@ -58,6 +73,10 @@ typedef struct rv9_stream_spec {
  * frames (eight slots and two in flight), record staging and scratch. Needs
  * no device. */
 uint64_t rv9_stream_reservation(const rv9_stream_spec* spec);
+/* The bytes a stream of this spec reserves in `eng`: rv9_stream_reservation
+ * plus, when the engine parses on the device, the device parser's buffers
+ * for a batch (rv9_engine_set_device_parse). */
+uint64_t rv9_engine_stream_reservation(rv9_engine* eng, const rv9_stream_spec* spec);
 
 /* Opens a stream; *id receives its handle. The stream is admitted at once
  * when the budget allows, else it is pending and its requests wait until
@@ -97,6 +116,11 @@ typedef struct rv9_engine_stats {
   uint64_t frames_decoded;
   uint64_t reserved_bytes, budget_bytes;
   uint64_t batched_steps, batched_frames; /* batched form: steps launched and frames in them */
+  /* rv9_engine_set_device_parse: batches, the frames parsed on the device,
+   * the workers' time waiting for their batches' parse on the device, and
+   * their time on the batches in all (microseconds, summed over workers) */
+  uint64_t device_parse_batches, device_parsed_frames;
+  uint64_t device_parse_wait_us, device_parse_batch_us;
 } rv9_engine_stats;
 void rv9_engine_get_stats(rv9_engine* eng, rv9_engine_stats* out);
 
@@ -116,6 +140,9 @@ typedef struct rv9_cluster rv9_cluster;
 rv9_cluster* rv9_cluster_create(const int* devices, size_t n, uint64_t hbm_budget_per_device,
                                 uint32_t workers_per_device);
 void rv9_cluster_free(rv9_cluster* c);
+/* rv9_engine_set_device_parse on every device's engine (streams are then
+ * placed by rv9_engine_stream_reservation). */
+rv9_status rv9_cluster_set_device_parse(rv9_cluster* c, int on, uint32_t window, uint32_t max_batches);
 /* Opens a stream on the device the placement rule picks; *device receives
  * that device's ordinal (may be NULL). RV9_UNSUPPORTED when no device's
  * budget could ever hold the stream. */

@@ -33,6 +33,7 @@ DeviceParser::~DeviceParser() {
     if (p) cudaFree(p);
   for (cudaEvent_t e : stage_free_)
     if (e) cudaEventDestroy(e);
+  if (collected_) cudaEventDestroy(collected_);
   if (h_pinned_) cudaFreeHost(h_pinned_);
 }
 
@@ -41,6 +42,7 @@ rv9::Status DeviceParser::init(int device, std::string* err) {
   DP_CK(parse_tables(device, &T_));
   for (cudaEvent_t& e : stage_free_)
     if (!e) DP_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!collected_) DP_CK(cudaEventCreateWithFlags(&collected_, cudaEventDisableTiming | cudaEventBlockingSync));
   return rv9::ST_OK;
 }
 
@@ -163,6 +165,92 @@ bool DeviceParser::add(const rv9::Parser::ExternalTiles& x, const rv9_frame_desc
   return true;
 }
 
+namespace {
+
+// A frame's worst-case sizes in the batch arrays (what add() reserves for
+// it), with the most tile columns the frame's width allows (each rounds its
+// width up to whole superblocks).
+struct FrameCaps {
+  uint64_t mi, above, blocks, toks, coefs, stage, chains, spans, data;
+};
+
+FrameCaps frame_caps(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y) {
+  FrameCaps c;
+  const uint32_t mi_cols = (width + 7) >> 3, mi_rows = (height + 7) >> 3;
+  const uint32_t sb_cols = (mi_cols + 7) >> 3;
+  uint32_t log2 = 0;
+  while ((sb_cols >> (log2 + 1)) >= 4) ++log2;  // tile columns at least 4 superblocks wide
+  const uint32_t cols = 1u << log2;
+  uint32_t blocks, toks, coefs;
+  tp::chain_caps(mi_cols + 8 * cols, mi_rows, ss_x, ss_y, &blocks, &toks, &coefs);
+  c.mi = (uint64_t)mi_cols * mi_rows;
+  c.above = align_up(tp::above_bytes(sb_cols));
+  c.blocks = blocks;
+  c.toks = toks;
+  c.coefs = coefs;
+  c.stage = align_up((uint64_t)blocks * sizeof(rv9_block)) + align_up((uint64_t)toks * sizeof(rv9_tok)) +
+            align_up((uint64_t)coefs * 4) + align_up((uint64_t)toks * sizeof(InterUnit)) +
+            align_up((uint64_t)toks * sizeof(ResItem)) + align_up((uint64_t)toks * sizeof(IntraItem)) +
+            align_up(((uint64_t)toks + 1) * 4);
+  c.chains = cols;
+  c.spans = 4ull * cols;  // up to four tile rows
+  c.data = (uint64_t)width * height / 2 + (64 << 10);
+  return c;
+}
+
+}  // namespace
+
+uint64_t DeviceParser::footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames) {
+  const FrameCaps c = frame_caps(width, height, ss_x, ss_y);
+  const uint64_t records = c.blocks * sizeof(rv9_block) + c.toks * sizeof(rv9_tok) + c.coefs * 4;
+  const uint64_t per_frame = 2 * c.stage + records + c.mi * (sizeof(tp::Mi) + sizeof(tp::PrevMv)) + c.above +
+                             c.blocks * 32 + c.data;
+  return per_frame * frames + c.mi * sizeof(tp::PrevMv);
+}
+
+rv9::Status DeviceParser::reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames,
+                                  std::string* err) {
+  const FrameCaps c = frame_caps(width, height, ss_x, ss_y);
+  const uint64_t n = frames;
+  rv9::Status st;
+#define DP_RESERVE(p, cap, need) \
+  if ((st = grow(&p, &cap, (size_t)(need), err)) != rv9::ST_OK) return st
+  DP_RESERVE(d_data_, data_cap_, n * c.data + 16);
+  DP_RESERVE(d_fin_, fin_cap_, n);
+  DP_RESERVE(d_chains_, chains_cap_, n * c.chains);
+  DP_RESERVE(d_spans_, spans_cap_, n * c.spans);
+  DP_RESERVE(d_outs_, outs_cap_, n * c.chains);
+  DP_RESERVE(d_mi_, mi_cap_, n * c.mi);
+  DP_RESERVE(d_above_, above_cap_, n * c.above);
+  DP_RESERVE(d_prev_, prev_cap_, n * c.mi);
+  DP_RESERVE(d_blocks_, blocks_cap_, n * c.blocks);
+  DP_RESERVE(d_toks_, toks_cap_, n * c.toks);
+  DP_RESERVE(d_coefs_, coefs_cap_, n * c.coefs);
+  for (int b = 0; b < 2; ++b) {
+    if (stage_pending_[b] && n * c.stage > stage_cap_[b]) {
+      DP_CK(cudaEventSynchronize(stage_free_[b]));
+      stage_pending_[b] = false;
+    }
+    DP_RESERVE(d_stage_[b], stage_cap_[b], n * c.stage);
+  }
+  DP_RESERVE(d_scratch_, scratch_cap_, n * c.blocks * 8);
+  DP_RESERVE(d_build_, build_cap_, n);
+  DP_RESERVE(d_results_, results_cap_, n);
+  DP_RESERVE(d_last_prev_, last_prev_cap_, c.mi);
+#undef DP_RESERVE
+  const size_t pinned = align_up(n * sizeof(tp::FrameIn)) + align_up(n * c.chains * sizeof(tp::Chain)) +
+                        align_up(n * c.spans * sizeof(tp::Span)) + align_up(n * sizeof(BuildFrame)) +
+                        align_up(c.mi * sizeof(tp::PrevMv)) + n * c.data;
+  if (pinned > pinned_cap_) {
+    if (h_pinned_) cudaFreeHost(h_pinned_);
+    h_pinned_ = nullptr;
+    pinned_cap_ = 0;
+    DP_CK(cudaMallocHost(&h_pinned_, pinned));
+    pinned_cap_ = pinned;
+  }
+  return rv9::ST_OK;
+}
+
 template <class T>
 rv9::Status DeviceParser::grow(T** p, size_t* cap, size_t need, std::string* err) {
   if (need <= *cap) return rv9::ST_OK;
@@ -272,7 +360,8 @@ rv9::Status DeviceParser::collect(cudaStream_t s, std::string* err) {
   outs_.assign(nf, BuildOut());
   if (nf == 0) return rv9::ST_OK;
   DP_CK(cudaMemcpyAsync(outs_.data(), d_results_, nf * sizeof(BuildOut), cudaMemcpyDeviceToHost, s));
-  DP_CK(cudaStreamSynchronize(s));
+  DP_CK(cudaEventRecord(collected_, s));
+  DP_CK(cudaEventSynchronize(collected_));
   // The motion vectors a later batch (or the host parser) may read: those of
   // the last frame before the first that failed.
   int last_ok = -1;

@@ -92,6 +92,17 @@ class DeviceParser {
   rv9::Status last_prev(std::vector<tp::PrevMv>* out, cudaStream_t s, std::string* err);
   bool have_last() const { return have_last_; }
   uint64_t bools() const { return bools_; }
+  // Device bytes a parser holds for batches of `frames` frames of this size
+  // at most: both stage buffers, the parse records, the frames' mode info
+  // and motion vectors, and the build scratch, at the worst-case capacities
+  // add() reserves (the compressed data and per-frame tables, which are
+  // small beside them, excluded).
+  static uint64_t footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames);
+  // Allocates every buffer for batches of `frames` frames of this size at
+  // the capacities footprint counts, so that such batches allocate nothing
+  // (a device allocation or free waits for the whole device).
+  rv9::Status reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames,
+                      std::string* err);
   // Lets go of the current stage buffer: the caller owns it (cudaFree) and
   // a new one is allocated for the next batch that uses this slot.
   uint8_t* release_stage();
@@ -151,6 +162,7 @@ class DeviceParser {
   uint8_t* d_stage_[2] = {nullptr, nullptr};
   size_t stage_cap_[2] = {0, 0};
   cudaEvent_t stage_free_[2] = {nullptr, nullptr};
+  cudaEvent_t collected_ = nullptr;  // collect's wait (blocking: the waiting thread sleeps)
   bool stage_pending_[2] = {false, false};  // stage_free_ recorded, not yet waited for
   int cur_ = 0;
   uint32_t* d_scratch_ = nullptr;

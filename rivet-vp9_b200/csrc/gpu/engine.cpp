@@ -69,7 +69,7 @@ Engine::~Engine() {
   cudaFree(d_digest_);
 }
 
-bool Engine::init(int device, std::string* err) {
+bool Engine::init(int device, std::string* err, bool side_stream) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) {
@@ -98,7 +98,7 @@ bool Engine::init(int device, std::string* err) {
       (e = cudaEventCreate(&ev0_)) != cudaSuccess || (e = cudaEventCreate(&ev1_)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&stage_ev_[0], cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&stage_ev_[1], cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaStreamCreateWithFlags(&aux_.side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (side_stream && (e = cudaStreamCreateWithFlags(&aux_.side, cudaStreamNonBlocking)) != cudaSuccess) ||
       (e = cudaEventCreateWithFlags(&aux_.fork, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&aux_.join, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaMalloc(&d_counters_, 64)) != cudaSuccess || (e = cudaMallocHost(&h_error_, 64)) != cudaSuccess) {

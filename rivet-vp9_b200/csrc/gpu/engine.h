@@ -156,7 +156,13 @@ class Engine {
  public:
   Engine() = default;
   ~Engine();
-  bool init(int device, std::string* err);
+  // side_stream: a second CUDA stream that the large inter units of a frame
+  // run on beside its small ones. Without it every launch of the engine is
+  // on its one CUDA stream, which is what many engines on one device want:
+  // the device has a fixed number of hardware queues, and CUDA streams
+  // beyond them share queues, where one stream's long kernel holds up the
+  // other's work.
+  bool init(int device, std::string* err, bool side_stream = true);
   // Reconstructs a parsed frame (or handles show_existing); the frame to show
   // (or null) stays valid until the next call. Work is queued; errors of the
   // device waits surface at the next sync().

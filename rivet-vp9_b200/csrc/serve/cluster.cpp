@@ -76,6 +76,16 @@ rv9_cluster* rv9_cluster_create(const int* devices, size_t n, uint64_t hbm_budge
   return c;
 }
 
+rv9_status rv9_cluster_set_device_parse(rv9_cluster* c, int on, uint32_t window, uint32_t max_batches) {
+  if (!c) return RV9_INVALID_INPUT;
+  std::lock_guard<std::mutex> lock(c->mu);
+  for (rv9_engine* e : c->engines) {
+    rv9_status st = rv9_engine_set_device_parse(e, on, window, max_batches);
+    if (st != RV9_OK) return st;
+  }
+  return RV9_OK;
+}
+
 void rv9_cluster_free(rv9_cluster* c) {
   if (!c) return;
   for (rv9_engine* e : c->engines) rv9_engine_free(e);
@@ -85,8 +95,9 @@ void rv9_cluster_free(rv9_cluster* c) {
 rv9_status rv9_cluster_stream_open(rv9_cluster* c, const rv9_stream_spec* spec, int64_t* id, int* device) {
   if (!c || !spec || !id) return RV9_INVALID_INPUT;
   *id = 0;
-  const uint64_t need = rv9_stream_reservation(spec);
   std::lock_guard<std::mutex> lock(c->mu);
+  // The engines share their settings: the first one's reservation holds.
+  const uint64_t need = rv9_engine_stream_reservation(c->engines[0], spec);
   std::vector<uint64_t> budgets(c->engines.size(), c->budget);
   const int d = rv9_place_least_loaded(c->load.data(), budgets.data(), c->engines.size(), need);
   if (d < 0) return RV9_UNSUPPORTED;

@@ -21,6 +21,14 @@
 // step. Requests of a stream still complete in order (one CUDA stream per
 // group), and requests arriving while others are on the GPU join the next
 // step: continuous batching on the device.
+//
+// With device parsing (rv9_engine_set_device_parse, plain form), a worker
+// that takes a stream with several queued requests takes a window of them
+// and parses their frames on the GPU as one batch (one thread per tile
+// column of every frame, rv9g::DeviceParser), then reconstructs them on the
+// stream's CUDA stream as above. While a batch parses, the worker sleeps
+// and the other workers parse other streams' requests on the host, so the
+// device parser adds to the host's parsing rate rather than replacing it.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -38,6 +46,7 @@
 
 #include "../../../include/rv9_server.h"
 #include "../api/api_internal.h"
+#include "../gpu/device_parse.h"
 #include "../gpu/engine.h"
 #include "../host/parser.h"
 
@@ -107,6 +116,15 @@ struct Stream {
   std::unique_ptr<rv9g::Engine> engine;
   std::vector<OutBuf> outs;
   std::vector<int> free_outs;
+  // Device parsing: requests per batch (0: off for this stream) and the
+  // stream's device parser, its buffers allocated at admission. Batches
+  // parse on the engine's CUDA stream, ahead of their reconstruction, and
+  // the engine runs without its side stream: one CUDA stream per stream
+  // keeps the device's hardware queues (32 at most) from being shared
+  // between streams, where one stream's parse, hundreds of milliseconds
+  // long, would hold up the other's reconstruction.
+  uint32_t dp_window = 0;
+  std::unique_ptr<rv9g::DeviceParser> dp;
   ~Stream() {
     for (OutBuf& b : outs) cudaFreeHost(b.data);
   }
@@ -119,6 +137,14 @@ size_t stage_bytes_of(const rv9_stream_spec& s) {
 uint64_t reservation_of(const rv9_stream_spec& s) {
   return rv9g::Engine::footprint(s.max_width, s.max_height, s.ss_x, s.ss_y, s.bit_depth, kReservedFrames,
                                  stage_bytes_of(s));
+}
+
+// A stream's reservation when its requests may parse on the device in
+// batches of `window` frames: the device parser's buffers are added.
+uint64_t reservation_of(const rv9_stream_spec& s, uint32_t window) {
+  uint64_t r = reservation_of(s);
+  if (window) r += rv9g::DeviceParser::footprint(s.max_width, s.max_height, s.ss_x, s.ss_y, window);
+  return r;
 }
 
 size_t packed_cap(const rv9_stream_spec& s) {
@@ -194,6 +220,13 @@ struct rv9_engine {
   std::vector<std::thread> workers;
   size_t cursor = 0;
   uint64_t n_submitted = 0, n_completed = 0, n_frames = 0;
+  // Device parsing (plain form): requests per batch (0: off), batches on the
+  // device at once, and statistics.
+  uint32_t dp_window = 0, dp_max = 0;
+  int dp_active = 0;
+  uint64_t dp_batches = 0, dp_frames = 0, dp_wait_us = 0, dp_batch_us = 0;
+  int n_host_workers = 0;
+  uint32_t n_extra_workers = 0;  // workers added for device-parse batches
 
   double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 
@@ -325,13 +358,17 @@ struct rv9_engine {
     Stream& s = *sp;
     std::string err;
     std::unique_ptr<rv9g::Engine> engine(new rv9g::Engine);
-    bool ok = engine->init(device, &err);
+    // A stream that parses on the device keeps all its work on one CUDA
+    // stream (see Stream::dp).
+    bool ok = engine->init(device, &err, s.dp_window == 0);
     if (ok)
       ok = engine->reserve(s.spec.max_width, s.spec.max_height, s.spec.ss_x, s.spec.ss_y, s.spec.bit_depth,
                            kReservedFrames, stage_bytes_of(s.spec), &err) == rv9::ST_OK;
     std::vector<OutBuf> outs;
     size_t cap = packed_cap(s.spec) * kMaxShown;
-    for (int i = 0; ok && i < kOutBuffers; ++i) {
+    // A device-parse batch takes a free output buffer per request.
+    const int n_outs = std::max(kOutBuffers, (int)s.dp_window);
+    for (int i = 0; ok && i < n_outs; ++i) {
       OutBuf b;
       if (cudaMallocHost(&b.data, cap) != cudaSuccess) {
         ok = false;
@@ -341,10 +378,18 @@ struct rv9_engine {
       b.cap = cap;
       outs.push_back(b);
     }
+    std::unique_ptr<rv9g::DeviceParser> dp;
+    if (ok && s.dp_window) {
+      dp.reset(new rv9g::DeviceParser);
+      ok = dp->init(device, &err) == rv9::ST_OK &&
+           dp->reserve(s.spec.max_width, s.spec.max_height, s.spec.ss_x, s.spec.ss_y, s.dp_window, &err) ==
+               rv9::ST_OK;
+    }
     std::lock_guard<std::mutex> lock(mu);
     s.outs = std::move(outs);
     if (ok) {
       s.engine = std::move(engine);
+      s.dp = std::move(dp);
       for (int i = 0; i < (int)s.outs.size(); ++i) s.free_outs.push_back(i);
       if (!groups.empty()) s.group = next_group++ % (int)groups.size();
       s.state = ACTIVE;
@@ -376,6 +421,7 @@ struct rv9_engine {
       work_cv.notify_all();
     }
     engine.reset();  // outside the lock: frees device memory
+    s.dp.reset();
     std::lock_guard<std::mutex> lock(mu);
     idle_cv.notify_all();
   }
@@ -396,7 +442,16 @@ struct rv9_engine {
     Request req;
     int out;
     {
-      std::lock_guard<std::mutex> lock(mu);
+      std::unique_lock<std::mutex> lock(mu);
+      // Several requests queued: a device-parse batch of them, while fewer
+      // than dp_max batches are on the device.
+      if (s.dp_window && dp_active < (int)dp_max && s.queue.size() >= 2 && s.free_outs.size() >= 2) {
+        const size_t k = std::min<size_t>({s.queue.size(), s.free_outs.size(), s.dp_window});
+        ++dp_active;
+        lock.unlock();
+        decode_batch_device(sp, k);
+        return;
+      }
       req = std::move(s.queue.front());
       s.queue.pop_front();
       out = s.free_outs.back();
@@ -419,7 +474,7 @@ struct rv9_engine {
     rv9::ParsedFrame pf;
     size_t off = 0;
     for (auto& fr : frames) {
-      rv9::Status st = s.parser.parse_frame(req.packet.data() + fr.first, fr.second, &pf, &err);
+      rv9::Status st = host_parse(s, s.parser.begin(req.packet.data() + fr.first, fr.second, nullptr), &pf, &err);
       rv9g::DevFrame* shown = nullptr;
       if (st == rv9::ST_OK) st = s.engine->recon(pf, &shown, &err);
       if (st != rv9::ST_OK) {
@@ -446,6 +501,189 @@ struct rv9_engine {
     }
     complete_after_device(s, d);
     std::lock_guard<std::mutex> lock(mu);
+    s.busy = false;
+    work_cv.notify_all();
+  }
+
+  // One frame parsed on the host (a job from s.parser.begin; released here).
+  // When the frame before it was parsed on the device, the motion vectors
+  // the frame may read are on the device too: they are read back first.
+  rv9::Status host_parse(Stream& s, rv9::Parser::Job* job, rv9::ParsedFrame* pf, std::string* err) {
+    if (s.dp) {
+      s.parser.bind_prev(job);
+      if (s.parser.wants_external_prev(job) && s.dp->have_last()) {
+        std::vector<rv9g::tp::PrevMv> prev;
+        rv9::Status st = s.dp->last_prev(&prev, s.engine->stream(), err);
+        if (st != rv9::ST_OK) {
+          s.parser.release(job);
+          return st;
+        }
+        s.parser.provide_prev_mvs(job, prev.data(), prev.size());
+      }
+    }
+    s.parser.attach_work(job);
+    s.parser.run(job);
+    rv9::Status st = s.parser.finish(job, pf, err);
+    s.parser.release(job);
+    return st;
+  }
+
+  // Plain form with device parsing: the stream's next k requests. Their
+  // frames go, in decode order, to one device batch where the device parser
+  // takes them (rv9::Parser::external_tiles); a frame it does not take is
+  // parsed on the host once the batch before it is reconstructed. Each
+  // request completes behind the copies of its shown frames. A frame that
+  // fails fails its request and drops the batch's later frames, whose
+  // requests fail with it; the requests after the batch decode as usual.
+  void decode_batch_device(const std::shared_ptr<Stream>& sp, size_t k) {
+    Stream& s = *sp;
+    std::vector<Request> reqs(k);
+    std::vector<Done*> dones(k);
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      for (size_t r = 0; r < k; ++r) {
+        reqs[r] = std::move(s.queue.front());
+        s.queue.pop_front();
+        Done* d = new Done;
+        d->stream = sp;
+        d->stream_id = s.id;
+        d->tag = reqs[r].tag;
+        d->submit_ms = reqs[r].submit_ms;
+        d->out = s.free_outs.back();
+        s.free_outs.pop_back();
+        dones[r] = d;
+      }
+      s.inflight += (int)k;
+    }
+    const cudaStream_t es = s.engine->stream();
+    const auto t_batch = Clock::now();
+    uint64_t wait_us = 0;
+    std::string err;
+    std::vector<int> open(k, 0);         // the request's frames waiting in the batch
+    std::vector<char> begun(k, 0);       // every frame of the request begun
+    size_t next_done = 0;
+    uint64_t n_dev = 0;
+    auto fail = [&](size_t r, rv9::Status st, const std::string& msg) {
+      if (dones[r]->status != RV9_OK) return;
+      dones[r]->status = (rv9_status)st;
+      dones[r]->err = msg;
+    };
+    // Completions in request order, each once its frames are all queued.
+    auto complete_ready = [&]() {
+      while (next_done < k && begun[next_done] && open[next_done] == 0) complete_after_device(s, dones[next_done++]);
+    };
+    struct Pend {
+      rv9::Parser::Job* job;
+      size_t owner;
+    };
+    std::vector<Pend> pending;
+    // Drops the batch's frames from i on (their requests fail) and hands the
+    // stage buffer back behind the reconstructions already queued from it.
+    auto drop_from = [&](size_t i, rv9::Status st, const std::string& msg) {
+      for (size_t j = i; j < pending.size(); ++j) {
+        s.parser.release(pending[j].job);
+        fail(pending[j].owner, st, msg);
+        open[pending[j].owner] -= 1;
+      }
+      pending.clear();
+      std::string ignored;
+      s.dp->recon_queued(es, &ignored);
+      s.dp->clear();
+    };
+    auto flush = [&]() {
+      if (pending.empty()) return;
+      rv9g::DeviceParser& P = *s.dp;
+      std::string e2;
+      const auto tw = Clock::now();
+      rv9::Status st = P.launch(es, &e2);
+      if (st == rv9::ST_OK) st = P.collect(es, &e2);
+      wait_us += (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(Clock::now() - tw).count();
+      if (st != rv9::ST_OK) {
+        drop_from(0, st, e2);
+        complete_ready();
+        return;
+      }
+      for (size_t i = 0; i < pending.size(); ++i) {
+        const size_t r = pending[i].owner;
+        std::string msg;
+        const rv9::Status ts = P.frame_status(i, &msg);
+        rv9::ParsedFrame meta;
+        st = s.parser.finish_external(pending[i].job, ts, msg, &meta, &e2);
+        s.parser.release(pending[i].job);
+        pending[i].job = nullptr;
+        open[r] -= 1;
+        if (st == rv9::ST_OK) {
+          rv9g::FrameWork fw;
+          fw.desc = meta.desc;
+          fw.show_existing = false;
+          fw.show_frame = meta.show_frame;
+          fw.refresh_mask = meta.refresh_mask;
+          for (int q = 0; q < 3; ++q) fw.ref_slot[q] = meta.ref_slot[q];
+          P.frame_work(i, &fw);
+          rv9g::DevFrame* shown = nullptr;
+          st = s.engine->recon_resident(fw, P.frame_base(i), &shown, &e2);
+          if (st == rv9::ST_OK) {
+            ++n_dev;
+            if (shown && dones[r]->status == RV9_OK) place_frame(s, dones[r], shown, es);
+          }
+        }
+        if (st != rv9::ST_OK) {
+          fail(r, st, e2);
+          drop_from(i + 1, st, "an earlier frame of the stream failed: " + e2);
+          complete_ready();
+          return;
+        }
+        complete_ready();
+      }
+      pending.clear();
+      // Should the stage buffer's release fail to queue, the batch's
+      // reconstructions end before the buffer is written again.
+      if (P.recon_queued(es, &e2) != rv9::ST_OK) cudaStreamSynchronize(es);
+      P.clear();
+    };
+    std::vector<std::pair<size_t, size_t>> frames;
+    rv9::ParsedFrame pf;
+    for (size_t r = 0; r < k; ++r) {
+      const Request& q = reqs[r];
+      Done* d = dones[r];
+      if (q.packet.empty()) fail(r, rv9::ST_BITSTREAM, "empty packet");
+      rv9::superframe_split(q.packet.data(), q.packet.size(), &frames);
+      for (auto& fr : frames) {
+        if (d->status != RV9_OK) break;
+        rv9::Parser::Job* job = s.parser.begin(q.packet.data() + fr.first, fr.second, nullptr);
+        rv9::Parser::ExternalTiles x;
+        if (s.parser.external_tiles(job, &x) && s.dp->add(x, *x.desc)) {
+          pending.push_back({job, r});
+          open[r] += 1;
+          if (pending.size() >= s.dp_window || s.dp->stage_bytes() >= (4ull << 30)) flush();
+          continue;
+        }
+        // A frame for the host parser: the batch before it first.
+        flush();
+        if (d->status != RV9_OK) {
+          s.parser.release(job);
+          break;
+        }
+        rv9::Status st = host_parse(s, job, &pf, &err);
+        rv9g::DevFrame* shown = nullptr;
+        if (st == rv9::ST_OK) st = s.engine->recon(pf, &shown, &err);
+        if (st != rv9::ST_OK) {
+          fail(r, st, err);
+          break;
+        }
+        if (shown) place_frame(s, d, shown, es);
+      }
+      begun[r] = 1;
+      complete_ready();
+    }
+    flush();
+    complete_ready();
+    std::lock_guard<std::mutex> lock(mu);
+    --dp_active;
+    dp_batches += 1;
+    dp_frames += n_dev;
+    dp_wait_us += wait_us;
+    dp_batch_us += (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(Clock::now() - t_batch).count();
     s.busy = false;
     work_cv.notify_all();
   }
@@ -698,6 +936,12 @@ extern "C" {
 
 uint64_t rv9_stream_reservation(const rv9_stream_spec* spec) { return spec ? reservation_of(*spec) : 0; }
 
+uint64_t rv9_engine_stream_reservation(rv9_engine* e, const rv9_stream_spec* spec) {
+  if (!e || !spec) return 0;
+  std::lock_guard<std::mutex> lock(e->mu);
+  return reservation_of(*spec, e->dp_window);
+}
+
 static rv9_engine* engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers, uint32_t n_groups);
 
 rv9_engine* rv9_engine_create(int device, uint64_t hbm_budget_bytes, uint32_t workers) {
@@ -744,6 +988,7 @@ static rv9_engine* engine_create(int device, uint64_t hbm_budget_bytes, uint32_t
       e->groups[g]->launcher = std::thread([e, g] { e->launcher_loop((int)g); });
   }
   int n = workers ? (int)workers : (int)std::max(1u, std::thread::hardware_concurrency());
+  e->n_host_workers = n;
   for (int i = 0; i < n; ++i) e->workers.emplace_back([e] { e->worker_loop(); });
   return e;
 }
@@ -798,13 +1043,14 @@ rv9_status rv9_stream_open(rv9_engine* e, const rv9_stream_spec* spec, int64_t* 
   if (spec->max_width == 0 || spec->max_height == 0 || spec->max_width > 16384 || spec->max_height > 16384 ||
       (spec->bit_depth != 8 && spec->bit_depth != 10 && spec->bit_depth != 12) || spec->ss_x > 1 || spec->ss_y > 1)
     return RV9_INVALID_INPUT;
-  uint64_t r = reservation_of(*spec);
   std::lock_guard<std::mutex> lock(e->mu);
+  const uint64_t r = reservation_of(*spec, e->dp_window);
   if (r > e->budget) return RV9_UNSUPPORTED;
   auto s = std::make_shared<Stream>();
   s->id = e->next_id++;
   s->spec = *spec;
   s->reservation = r;
+  s->dp_window = e->dp_window;
   // Tile columns on threads: one request's latency shrinks when cores are
   // free; under load the workers keep every core busy anyway.
   s->parser.set_threads(0);
@@ -905,6 +1151,31 @@ void rv9_engine_get_stats(rv9_engine* e, rv9_engine_stats* out) {
     out->batched_steps += G->steps;
     out->batched_frames += G->frames;
   }
+  out->device_parse_batches = e->dp_batches;
+  out->device_parsed_frames = e->dp_frames;
+  out->device_parse_wait_us = e->dp_wait_us;
+  out->device_parse_batch_us = e->dp_batch_us;
+}
+
+rv9_status rv9_engine_set_device_parse(rv9_engine* e, int on, uint32_t window, uint32_t max_batches) {
+  if (!e) return RV9_INVALID_INPUT;
+  if (!e->groups.empty()) return RV9_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (!on) {
+    e->dp_window = 0;
+    e->dp_max = 0;
+    return RV9_OK;
+  }
+  e->dp_window = window ? std::min<uint32_t>(window, 64) : 8;
+  e->dp_max = max_batches ? max_batches : (uint32_t)e->n_host_workers;
+  // A worker waiting for its batch sleeps: one more worker per batch keeps
+  // the host's parsing rate while batches are on the device.
+  while (e->n_extra_workers < e->dp_max) {
+    e->workers.emplace_back([e] { e->worker_loop(); });
+    ++e->n_extra_workers;
+  }
+  e->work_cv.notify_all();
+  return RV9_OK;
 }
 
 }  // extern "C"

@@ -27,11 +27,14 @@ class CCompletion(ctypes.Structure):
 class CEngineStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("streams_open", "streams_pending", "requests_submitted",
                                               "requests_completed", "frames_decoded", "reserved_bytes",
-                                              "budget_bytes", "batched_steps", "batched_frames")]
+                                              "budget_bytes", "batched_steps", "batched_frames",
+                                              "device_parse_batches", "device_parsed_frames",
+                                              "device_parse_wait_us", "device_parse_batch_us")]
 
 
 EXPORTS = ("rv9_engine_create", "rv9_engine_create_batched", "rv9_engine_free", "rv9_stream_reservation", "rv9_stream_open", "rv9_stream_close",
-           "rv9_submit", "rv9_poll", "rv9_completion_release", "rv9_engine_get_stats", "rv9_cluster_create",
+           "rv9_submit", "rv9_poll", "rv9_completion_release", "rv9_engine_get_stats", "rv9_engine_set_device_parse", "rv9_engine_stream_reservation",
+           "rv9_cluster_create", "rv9_cluster_set_device_parse",
            "rv9_cluster_free", "rv9_cluster_stream_open", "rv9_cluster_stream_close", "rv9_cluster_submit",
            "rv9_cluster_poll", "rv9_cluster_completion_release", "rv9_cluster_get_stats", "rv9_place_least_loaded")
 
@@ -54,6 +57,10 @@ def _bind(lib):
     lib.rv9_poll.argtypes = [vp, ctypes.POINTER(CCompletion), ctypes.c_size_t, ctypes.c_int]
     lib.rv9_completion_release.argtypes = [vp, ctypes.POINTER(CCompletion)]
     lib.rv9_engine_get_stats.argtypes = [vp, ctypes.POINTER(CEngineStats)]
+    lib.rv9_engine_set_device_parse.argtypes = [vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
+    lib.rv9_engine_stream_reservation.restype = ctypes.c_uint64
+    lib.rv9_engine_stream_reservation.argtypes = [vp, ctypes.POINTER(CStreamSpec)]
+    lib.rv9_cluster_set_device_parse.argtypes = [vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
     lib.rv9_cluster_create.restype = vp
     lib.rv9_cluster_create.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint32]
     lib.rv9_cluster_free.argtypes = [vp]
@@ -104,7 +111,8 @@ class Engine:
     (rv9_engine_create_batched): the streams' frames reconstructed together,
     one launch per stage per step, in that many launch groups."""
 
-    def __init__(self, device=-1, hbm_budget=120 << 30, workers=0, lib_path=None, groups=0):
+    def __init__(self, device=-1, hbm_budget=120 << 30, workers=0, lib_path=None, groups=0, device_parse=False,
+                 window=0, max_batches=0):
         self._lib = _bind(load_library(lib_path))
         if groups:
             self._e = self._lib.rv9_engine_create_batched(device, hbm_budget, workers, groups)
@@ -112,6 +120,22 @@ class Engine:
             self._e = self._lib.rv9_engine_create(device, hbm_budget, workers)
         if not self._e:
             raise DeviceError(self._lib.rv9_last_global_error().decode(errors="replace"))
+        if device_parse:
+            self.set_device_parse(True, window, max_batches)
+
+    def set_device_parse(self, on=True, window=0, max_batches=0):
+        """rv9_engine_set_device_parse: queued requests of a stream parsed on
+        the GPU in batches of up to `window`, for the streams opened after
+        the call."""
+        st = self._lib.rv9_engine_set_device_parse(self._e, 1 if on else 0, window, max_batches)
+        if st != RV9_OK:
+            raise _ERRORS.get(st, Rv9Error)(f"rv9_engine_set_device_parse: status {st}")
+
+    def reservation(self, width, height, bit_depth=8, chroma=(1, 1)):
+        """Device bytes a stream of this size reserves in this engine
+        (rv9_engine_stream_reservation)."""
+        s = spec(width, height, bit_depth, chroma)
+        return self._lib.rv9_engine_stream_reservation(self._e, ctypes.byref(s))
 
     def open_stream(self, width, height, bit_depth=8, chroma=(1, 1)):
         s = spec(width, height, bit_depth, chroma)
@@ -185,6 +209,13 @@ class Cluster:
         if not self._c:
             raise DeviceError(self._lib.rv9_last_global_error().decode(errors="replace"))
         self.n_devices = len(devices)
+
+    def set_device_parse(self, on=True, window=0, max_batches=0):
+        """rv9_cluster_set_device_parse: every device's engine parses queued
+        requests on its GPU in batches (streams opened after the call)."""
+        st = self._lib.rv9_cluster_set_device_parse(self._c, 1 if on else 0, window, max_batches)
+        if st != RV9_OK:
+            raise _ERRORS.get(st, Rv9Error)(f"rv9_cluster_set_device_parse: status {st}")
 
     def open_stream(self, width, height, bit_depth=8, chroma=(1, 1)):
         """Returns (stream id, device ordinal it was placed on)."""

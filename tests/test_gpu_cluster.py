@@ -1,7 +1,8 @@
 """The multi-device front end (rv9_cluster) on the GPU: with one GPU here,
 two engines on device 0 stand in for two devices, so that placement spreads
 the streams over both by reserved bytes; every stream's frames must be its
-published MD5s whichever engine decoded it."""
+published MD5s whichever engine decoded it, with host parsing and with
+device parsing (rv9_cluster_set_device_parse)."""
 import hashlib
 import os
 
@@ -15,10 +16,15 @@ NAMES = ["vp90-2-02-size-130x132.webm", "vp90-2-05-resize.ivf", "vp91-2-04-yuv44
          "vp92-2-20-10bit-yuv420.webm", "vp90-2-10-show-existing-frame2.webm", "vp90-2-03-size-226x226.webm"]
 
 
-def test_cluster_places_and_decodes_exactly():
+@pytest.mark.parametrize("device_parse", [False, True], ids=["host_parse", "device_parse"])
+def test_cluster_places_and_decodes_exactly(device_parse):
     from rv9 import server
-    cl = server.Cluster([0, 0], hbm_budget=8 << 30, workers=4)
+    # Room for three streams per engine (with device parsing a stream also
+    # reserves its batch's device records).
+    cl = server.Cluster([0, 0], hbm_budget=(24 if device_parse else 8) << 30, workers=4)
     try:
+        if device_parse:
+            cl.set_device_parse(True, window=4)
         sids, placed, want = [], [], {}
         for n in NAMES:
             path = os.path.join(VECTORS_DIR, n)

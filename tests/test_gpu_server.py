@@ -2,8 +2,13 @@
 same in the mix as alone (the published MD5s), requests complete in order
 per stream, admission waits for the HBM budget, and a bad packet fails only
 its own request. Every test runs on the plain engine (each stream on its own
-CUDA stream) and on the batched one (rv9_engine_create_batched: the streams'
-frames reconstructed together, one launch per stage per step)."""
+CUDA stream), on the plain engine with device parsing
+(rv9_engine_set_device_parse: a stream's queued requests parsed on the GPU as
+one batch) and on the batched one (rv9_engine_create_batched: the streams'
+frames reconstructed together, one launch per stage per step). The
+device-parse tests at the end decode generated streams whose frames the
+device parser takes, mixed with frames it leaves to the host, against the
+oracle."""
 import hashlib
 import os
 import time
@@ -26,9 +31,18 @@ MIX = [
 ]
 
 
-@pytest.fixture(params=[0, 1, 3], ids=["plain", "batched_1group", "batched_3groups"])
+@pytest.fixture(params=[0, "dp", 1, 3], ids=["plain", "plain_device_parse", "batched_1group", "batched_3groups"])
 def groups(request):
     return request.param
+
+
+def _engine(groups, **kw):
+    """An engine of the form `groups` names: 0 plain, "dp" plain with device
+    parsing (batches of up to 4 requests), n > 0 batched in n groups."""
+    from rv9 import server
+    if groups == "dp":
+        return server.Engine(0, device_parse=True, window=4, **kw)
+    return server.Engine(0, groups=groups, **kw)
 
 
 def _drain(eng, expect, timeout_s=120):
@@ -44,8 +58,7 @@ def _md5s(done, sid):
 
 
 def test_mix_equals_alone(groups):
-    from rv9 import server
-    eng = server.Engine(0, workers=8, groups=groups)
+    eng = _engine(groups, workers=8)
     try:
         sids, packets = {}, {}
         for name, bd in MIX:
@@ -71,7 +84,11 @@ def test_mix_equals_alone(groups):
         st = eng.stats()
         assert st["streams_open"] == 0 and st["reserved_bytes"] == 0
         assert st["requests_completed"] == st["requests_submitted"] == total
-        if groups:
+        if groups == "dp":
+            # The requests queued together went as batches (the vectors'
+            # frames all adapt probabilities, so the host parsed them).
+            assert st["device_parse_batches"] > 0
+        elif groups:
             # Every reconstructed frame went through a step (steps of one
             # frame or more, as the frames arrived).
             assert 0 < st["batched_steps"] <= st["batched_frames"]
@@ -82,7 +99,16 @@ def test_mix_equals_alone(groups):
 def test_admission_waits_for_the_budget(groups):
     from rv9 import server
     one = server.reservation(1920, 1080, 12, (0, 0))
-    eng = server.Engine(0, hbm_budget=int(one * 1.5), workers=4, groups=groups)
+    if groups == "dp":
+        # The reservation with the device parser's buffers.
+        probe = _engine(groups, workers=1)
+        try:
+            probe.open_stream(1920, 1080, bit_depth=12, chroma=(0, 0))
+            one = probe.stats()["reserved_bytes"]
+            assert one > server.reservation(1920, 1080, 12, (0, 0))
+        finally:
+            probe.close()
+    eng = _engine(groups, hbm_budget=int(one * 1.5), workers=4)
     try:
         names = MIX[:3]
         sids = [eng.open_stream(1920, 1080, bit_depth=12, chroma=(0, 0)) for _ in names]
@@ -106,8 +132,7 @@ def test_admission_waits_for_the_budget(groups):
 
 def test_spec_over_budget_is_refused(groups):
     import rv9
-    from rv9 import server
-    eng = server.Engine(0, hbm_budget=1 << 20, workers=1, groups=groups)
+    eng = _engine(groups, hbm_budget=1 << 20, workers=1)
     try:
         with pytest.raises(rv9.UnsupportedError):
             eng.open_stream(1920, 1080)
@@ -116,9 +141,8 @@ def test_spec_over_budget_is_refused(groups):
 
 
 def test_a_bad_packet_fails_only_its_request(groups):
-    from rv9 import server
     name = "vp90-2-02-size-130x132.webm"
-    eng = server.Engine(0, workers=4, groups=groups)
+    eng = _engine(groups, workers=4)
     try:
         good = eng.open_stream(352, 288)
         bad = eng.open_stream(352, 288)
@@ -139,9 +163,87 @@ def test_a_bad_packet_fails_only_its_request(groups):
 
 def test_free_with_requests_in_flight(groups):
     # Freeing the engine drains every stream, with completions never polled.
-    from rv9 import server
-    eng = server.Engine(0, workers=2, groups=groups)
+    eng = _engine(groups, workers=2)
     sid = eng.open_stream(352, 288)
     for i, p in enumerate(read_packets(os.path.join(VECTORS_DIR, "vp90-2-02-size-130x132.webm"))):
         eng.submit(sid, p, tag=i)
     eng.close()
+
+
+def _submit_all(eng, sid, packets, first_tag=0):
+    for i, p in enumerate(packets):
+        eng.submit(sid, p, tag=first_tag + i)
+
+
+@pytest.mark.parametrize("window", [2, 8])
+def test_device_parse_streams_match_the_oracle(window, oracle_lib):
+    """Generated streams, their requests queued deep: error-resilient ones
+    (every frame parsed on the device) and linked ones (frames that read the
+    previous frame's motion vectors, every few a probability-adapting frame
+    the host parses between device batches). Every request's frames against
+    the oracle's, in order."""
+    from rv9 import server
+    from conftest import oracle_frames
+    from streams_cases import CASES, LINKED, generate, generate_linked
+    cases = [("cif_8bit_q60", generate("cif_8bit_q60")[0], CASES["cif_8bit_q60"]),
+             ("720p_10bit_422_q50", generate("720p_10bit_422_q50")[0], CASES["720p_10bit_422_q50"]),
+             ("cif_8bit_linked", generate_linked("cif_8bit_linked"), LINKED["cif_8bit_linked"]),
+             ("720p_8bit_linked", generate_linked("720p_8bit_linked"), LINKED["720p_8bit_linked"])]
+    eng = server.Engine(0, workers=4, device_parse=True, window=window)
+    try:
+        sids = {}
+        for name, packets, shape in cases:
+            sids[name] = eng.open_stream(shape[0], shape[1], bit_depth=shape[2], chroma=shape[3])
+        total = 0
+        for name, packets, _ in cases:
+            _submit_all(eng, sids[name], packets)
+            total += len(packets)
+            eng.close_stream(sids[name])
+        done = _drain(eng, total)
+        assert len(done) == total
+        for name, packets, _ in cases:
+            cs = [c for c in done if c.stream == sids[name]]
+            assert [c.tag for c in cs] == list(range(len(packets))), name
+            assert all(c.ok for c in cs), name
+            want = [m for m, _ in oracle_frames(oracle_lib, packets)]
+            assert _md5s(done, sids[name]) == want, name
+        st = eng.stats()
+        assert st["device_parse_batches"] > 0
+        assert 0 < st["device_parsed_frames"] <= total
+    finally:
+        eng.close()
+
+
+def test_device_parse_corrupted_request(oracle_lib):
+    """A request whose tile data is corrupted fails as it does with host
+    parsing, the requests before it decode exactly, and the stream decodes
+    exactly again from its next key frame."""
+    from rv9 import server
+    from conftest import oracle_frames
+    from streams_cases import generate
+    packets, _ = generate("cif_8bit_q60")
+    bad = list(packets)
+    flipped = bytearray(bad[3])
+    for i in range(len(flipped) // 2, len(flipped)):
+        flipped[i] ^= 0xA5
+    bad[3] = bytes(flipped)
+    want = [m for m, _ in oracle_frames(oracle_lib, packets)]
+    status = {}
+    for form in ("host", "device"):
+        eng = server.Engine(0, workers=2, device_parse=form == "device", window=8)
+        try:
+            sid = eng.open_stream(352, 288)
+            _submit_all(eng, sid, bad)
+            done = _drain(eng, len(bad))
+            assert [c.tag for c in done] == list(range(len(bad))), form
+            assert all(c.ok for c in done[:3]), form
+            assert _md5s(done[:3], sid) == want[:3], form
+            status[form] = done[3].status
+            # Then the stream from its key frame again.
+            _submit_all(eng, sid, packets[:3], first_tag=100)
+            again = _drain(eng, 3)
+            assert all(c.ok for c in again) and _md5s(again, sid) == want[:3], form
+            eng.close_stream(sid)
+        finally:
+            eng.close()
+    assert status["host"] == status["device"]
