@@ -50,16 +50,16 @@ void rv9_engine_free(rv9_engine* eng);
  * RV9_UNSUPPORTED for a batched engine). A worker that takes a stream with
  * two or more queued requests takes up to `window` of them (0: 8, at most
  * 64) and parses their frames on the GPU as one batch, as
- * rv9_decoder_set_device_parse does; a lone request is parsed on the host as
- * before, and so is any frame the device parser does not take. At most
- * `max_batches` batches are on the device at once (0: one per host worker);
- * the engine adds that many workers, which sleep while their batch parses,
- * so the host keeps parsing other streams meanwhile. Each such stream keeps
- * `window` output buffers and reserves room for a batch's device records
- * (rv9_stream_reservation plus the device parser's buffers). A frame that
+ * rv9_decoder_set_device_parse does; a lone request is parsed on the host
+ * as before (a batch takes as long as its longest tile column, hundreds of
+ * milliseconds at 2160p), and so is any frame the device parser does not
+ * take. At most `max_batches` batches are on the device at once (0: 32);
+ * the engine adds that many workers, which sleep while their batch parses.
+ * Each such stream keeps 2 x `window` output buffers and reserves room for
+ * a batch's device records (rv9_engine_stream_reservation). A frame that
  * fails fails its request and the requests of the same batch after it.
- * `on` = 0 turns it off for streams opened later. Results are bit-identical
- * to host parsing. */
+ * `on` = 0 turns it off for streams opened later. Results are
+ * bit-identical to host parsing. */
 rv9_status rv9_engine_set_device_parse(rv9_engine* eng, int on, uint32_t window, uint32_t max_batches);
 
 /* The largest frame a stream will carry, which sizes its reservation. */

@@ -200,10 +200,11 @@ FrameCaps frame_caps(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss
 
 }  // namespace
 
-uint64_t DeviceParser::footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames) {
+uint64_t DeviceParser::footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames,
+                                 int stage_buffers) {
   const FrameCaps c = frame_caps(width, height, ss_x, ss_y);
   const uint64_t records = c.blocks * sizeof(rv9_block) + c.toks * sizeof(rv9_tok) + c.coefs * 4;
-  const uint64_t per_frame = 2 * c.stage + records + c.mi * (sizeof(tp::Mi) + sizeof(tp::PrevMv)) + c.above +
+  const uint64_t per_frame = (uint64_t)stage_buffers * c.stage + records + c.mi * (sizeof(tp::Mi) + sizeof(tp::PrevMv)) + c.above +
                              c.blocks * 32 + c.data;
   return per_frame * frames + c.mi * sizeof(tp::PrevMv);
 }
@@ -226,7 +227,7 @@ rv9::Status DeviceParser::reserve(uint32_t width, uint32_t height, uint32_t ss_x
   DP_RESERVE(d_blocks_, blocks_cap_, n * c.blocks);
   DP_RESERVE(d_toks_, toks_cap_, n * c.toks);
   DP_RESERVE(d_coefs_, coefs_cap_, n * c.coefs);
-  for (int b = 0; b < 2; ++b) {
+  for (int b = 0; b < (single_stage_ ? 1 : 2); ++b) {
     if (stage_pending_[b] && n * c.stage > stage_cap_[b]) {
       DP_CK(cudaEventSynchronize(stage_free_[b]));
       stage_pending_[b] = false;
@@ -335,7 +336,11 @@ rv9::Status DeviceParser::launch(cudaStream_t s, std::string* err) {
     DP_CK(launch_parse_chains(T_, d_fin_, d_chains_, 0, (uint32_t)nc, d_spans_, d_data_, d_mi_, d_above_, d_prev_,
                               d_blocks_, d_toks_, d_coefs_, d_outs_, s));
   } else {
-    for (int w = 0; w <= max_wave; ++w)
+    for (int w = 0; w <= max_wave; ++w) {
+      if (w > 0) {  // the wave before, waited for on the host (see below)
+        DP_CK(cudaEventRecord(collected_, s));
+        DP_CK(cudaEventSynchronize(collected_));
+      }
       for (size_t i = 0; i < nf; ++i) {
         const FrameInfo& fi = fi_[i];
         if (fi.wave != w) continue;
@@ -345,7 +350,15 @@ rv9::Status DeviceParser::launch(cudaStream_t s, std::string* err) {
         DP_CK(launch_parse_chains(T_, d_fin_, d_chains_, fi.first_chain, fi.n_chains, d_spans_, d_data_, d_mi_,
                                   d_above_, d_prev_, d_blocks_, d_toks_, d_coefs_, d_outs_, s));
       }
+    }
   }
+  // The parse runs for up to hundreds of milliseconds. Nothing queued on
+  // `s` waits for it inside the device's queue: the host waits (asleep) for
+  // it before queuing the build. A CUDA stream whose work sits behind a
+  // long kernel's dependant in a hardware queue that another stream shares
+  // (the device has a fixed number of them) holds that stream up too.
+  DP_CK(cudaEventRecord(collected_, s));
+  DP_CK(cudaEventSynchronize(collected_));
   if (stage_pending_[cur_]) {
     DP_CK(cudaStreamWaitEvent(s, stage_free_[cur_], 0));
     stage_pending_[cur_] = false;
@@ -378,6 +391,12 @@ rv9::Status DeviceParser::collect(cudaStream_t s, std::string* err) {
     have_last_ = true;
     last_mi_len_ = mi_len;
   }
+  return rv9::ST_OK;
+}
+
+rv9::Status DeviceParser::wait_on(cudaStream_t s, std::string* err) {
+  DP_CK(cudaEventRecord(collected_, s));
+  DP_CK(cudaEventSynchronize(collected_));
   return rv9::ST_OK;
 }
 
@@ -427,7 +446,7 @@ rv9::Status DeviceParser::last_prev(std::vector<tp::PrevMv>* out, cudaStream_t s
 rv9::Status DeviceParser::recon_queued(cudaStream_t s, std::string* err) {
   DP_CK(cudaEventRecord(stage_free_[cur_], s));
   stage_pending_[cur_] = true;
-  cur_ ^= 1;
+  if (!single_stage_) cur_ ^= 1;
   return rv9::ST_OK;
 }
 

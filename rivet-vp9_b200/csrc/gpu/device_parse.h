@@ -75,9 +75,13 @@ class DeviceParser {
   // does not split into tiles (the caller leaves it to the host parser,
   // which reports the error).
   bool add(const rv9::Parser::ExternalTiles& x, const rv9_frame_desc& desc);
+  // Queues the batch on `s` and returns once its tile columns are parsed
+  // (its work lists are then being built on `s`).
   rv9::Status launch(cudaStream_t s, std::string* err);
   // Waits for the batch and reads back every frame's outcome.
   rv9::Status collect(cudaStream_t s, std::string* err);
+  // Waits (asleep) for the work queued on `s` so far.
+  rv9::Status wait_on(cudaStream_t s, std::string* err);
   // Frame i after collect: its tiles' status (and message), and its work.
   rv9::Status frame_status(size_t i, std::string* msg) const;
   void frame_work(size_t i, FrameWork* fw) const;  // counts, offsets and bytes (not the header fields)
@@ -97,12 +101,18 @@ class DeviceParser {
   // and motion vectors, and the build scratch, at the worst-case capacities
   // add() reserves (the compressed data and per-frame tables, which are
   // small beside them, excluded).
-  static uint64_t footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames);
+  static uint64_t footprint(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames,
+                            int stage_buffers = 2);
   // Allocates every buffer for batches of `frames` frames of this size at
   // the capacities footprint counts, so that such batches allocate nothing
   // (a device allocation or free waits for the whole device).
   rv9::Status reserve(uint32_t width, uint32_t height, uint32_t ss_x, uint32_t ss_y, uint32_t frames,
                       std::string* err);
+  // One stage buffer instead of two, for a caller whose batch's
+  // reconstruction has ended before it launches the next batch (a batch
+  // reuses the buffer after waiting for the last one's reconstruction on
+  // the device, as it would for the other buffer). Before reserve().
+  void set_single_stage() { single_stage_ = true; }
   // Lets go of the current stage buffer: the caller owns it (cudaFree) and
   // a new one is allocated for the next batch that uses this slot.
   uint8_t* release_stage();
@@ -162,9 +172,10 @@ class DeviceParser {
   uint8_t* d_stage_[2] = {nullptr, nullptr};
   size_t stage_cap_[2] = {0, 0};
   cudaEvent_t stage_free_[2] = {nullptr, nullptr};
-  cudaEvent_t collected_ = nullptr;  // collect's wait (blocking: the waiting thread sleeps)
+  cudaEvent_t collected_ = nullptr;  // the host's waits on the stream (blocking: the waiting thread sleeps)
   bool stage_pending_[2] = {false, false};  // stage_free_ recorded, not yet waited for
   int cur_ = 0;
+  bool single_stage_ = false;
   uint32_t* d_scratch_ = nullptr;
   size_t scratch_cap_ = 0;
   BuildFrame* d_build_ = nullptr;

@@ -59,6 +59,7 @@ constexpr int kOutBuffers = 4;       // pinned output buffers per stream
 constexpr int kMaxShown = 2;         // shown frames one request may carry
 constexpr int kStepsAhead = 2;       // batched form: steps queued on the device per group
 constexpr int kTableRing = kStepsAhead + 2;  // batch-table buffers per group
+constexpr uint32_t kDefaultBatches = 32;     // device-parse batches in flight (the device's hardware queues)
 
 struct OutBuf {
   uint8_t* data = nullptr;
@@ -143,7 +144,7 @@ uint64_t reservation_of(const rv9_stream_spec& s) {
 // batches of `window` frames: the device parser's buffers are added.
 uint64_t reservation_of(const rv9_stream_spec& s, uint32_t window) {
   uint64_t r = reservation_of(s);
-  if (window) r += rv9g::DeviceParser::footprint(s.max_width, s.max_height, s.ss_x, s.ss_y, window);
+  if (window) r += rv9g::DeviceParser::footprint(s.max_width, s.max_height, s.ss_x, s.ss_y, window, 1);
   return r;
 }
 
@@ -342,6 +343,26 @@ struct rv9_engine {
     delete c;
   }
 
+  // Device-parse batches: the worker waits (asleep) for the batch's copies,
+  // then completes its requests in order. A host function per request (as
+  // the plain form queues) was measured to block its own queuing call for
+  // seconds once 32 streams' batches were in flight, each request behind a
+  // parse hundreds of milliseconds long; one per batch still blocked for
+  // about a second.
+  void complete_when_done(Stream& s, std::vector<Done*>* ds) {
+    if (ds->empty()) return;
+    std::string e;
+    const rv9::Status st = s.dp->wait_on(s.engine->stream(), &e);
+    for (Done* d : *ds) {
+      if (st != rv9::ST_OK && d->status == RV9_OK) {
+        d->status = (rv9_status)st;
+        d->err = e;
+      }
+      finish(d);
+    }
+    ds->clear();
+  }
+
   // Queues the completion behind the stream's device work.
   void complete_after_device(Stream& s, Done* d) {
     Callback* cb = new Callback{this, d};
@@ -366,8 +387,10 @@ struct rv9_engine {
                            kReservedFrames, stage_bytes_of(s.spec), &err) == rv9::ST_OK;
     std::vector<OutBuf> outs;
     size_t cap = packed_cap(s.spec) * kMaxShown;
-    // A device-parse batch takes a free output buffer per request.
-    const int n_outs = std::max(kOutBuffers, (int)s.dp_window);
+    // A device-parse batch takes a free output buffer per request; twice
+    // the window lets the next batch fill while the last one's buffers are
+    // still with the caller.
+    const int n_outs = std::max(kOutBuffers, 2 * (int)s.dp_window);
     for (int i = 0; ok && i < n_outs; ++i) {
       OutBuf b;
       if (cudaMallocHost(&b.data, cap) != cudaSuccess) {
@@ -381,6 +404,9 @@ struct rv9_engine {
     std::unique_ptr<rv9g::DeviceParser> dp;
     if (ok && s.dp_window) {
       dp.reset(new rv9g::DeviceParser);
+      // A batch's reconstruction ends before the stream's next batch is
+      // launched (complete_when_done): one stage buffer is enough.
+      dp->set_single_stage();
       ok = dp->init(device, &err) == rv9::ST_OK &&
            dp->reserve(s.spec.max_width, s.spec.max_height, s.spec.ss_x, s.spec.ss_y, s.dp_window, &err) ==
                rv9::ST_OK;
@@ -444,7 +470,9 @@ struct rv9_engine {
     {
       std::unique_lock<std::mutex> lock(mu);
       // Several requests queued: a device-parse batch of them, while fewer
-      // than dp_max batches are on the device.
+      // than dp_max batches are on the device. A lone request (low load) is
+      // parsed on the host: a batch takes as long as its longest tile
+      // column, hundreds of milliseconds at 2160p.
       if (s.dp_window && dp_active < (int)dp_max && s.queue.size() >= 2 && s.free_outs.size() >= 2) {
         const size_t k = std::min<size_t>({s.queue.size(), s.free_outs.size(), s.dp_window});
         ++dp_active;
@@ -568,9 +596,11 @@ struct rv9_engine {
       dones[r]->status = (rv9_status)st;
       dones[r]->err = msg;
     };
-    // Completions in request order, each once its frames are all queued.
+    // Requests in order, each once its frames are all queued; they complete
+    // together when the batch's copies are done.
+    std::vector<Done*> ready;
     auto complete_ready = [&]() {
-      while (next_done < k && begun[next_done] && open[next_done] == 0) complete_after_device(s, dones[next_done++]);
+      while (next_done < k && begun[next_done] && open[next_done] == 0) ready.push_back(dones[next_done++]);
     };
     struct Pend {
       rv9::Parser::Job* job;
@@ -678,6 +708,7 @@ struct rv9_engine {
     }
     flush();
     complete_ready();
+    complete_when_done(s, &ready);
     std::lock_guard<std::mutex> lock(mu);
     --dp_active;
     dp_batches += 1;
@@ -1167,7 +1198,7 @@ rv9_status rv9_engine_set_device_parse(rv9_engine* e, int on, uint32_t window, u
     return RV9_OK;
   }
   e->dp_window = window ? std::min<uint32_t>(window, 64) : 8;
-  e->dp_max = max_batches ? max_batches : (uint32_t)e->n_host_workers;
+  e->dp_max = max_batches ? max_batches : kDefaultBatches;
   // A worker waiting for its batch sleeps: one more worker per batch keeps
   // the host's parsing rate while batches are on the device.
   while (e->n_extra_workers < e->dp_max) {

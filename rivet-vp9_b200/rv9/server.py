@@ -121,12 +121,12 @@ class Engine:
         if not self._e:
             raise DeviceError(self._lib.rv9_last_global_error().decode(errors="replace"))
         if device_parse:
-            self.set_device_parse(True, window, max_batches)
+            self.set_device_parse(device_parse, window, max_batches)
 
     def set_device_parse(self, on=True, window=0, max_batches=0):
-        """rv9_engine_set_device_parse: queued requests of a stream parsed on
-        the GPU in batches of up to `window`, for the streams opened after
-        the call."""
+        """rv9_engine_set_device_parse: a stream's queued requests (two or
+        more) parsed on the GPU in batches of up to `window`, for the streams
+        opened after the call."""
         st = self._lib.rv9_engine_set_device_parse(self._e, 1 if on else 0, window, max_batches)
         if st != RV9_OK:
             raise _ERRORS.get(st, Rv9Error)(f"rv9_engine_set_device_parse: status {st}")

@@ -38,7 +38,8 @@ def groups(request):
 
 def _engine(groups, **kw):
     """An engine of the form `groups` names: 0 plain, "dp" plain with device
-    parsing (batches of up to 4 requests), n > 0 batched in n groups."""
+    parsing (batches of up to 4 requests), n > 0
+    batched in n groups."""
     from rv9 import server
     if groups == "dp":
         return server.Engine(0, device_parse=True, window=4, **kw)
@@ -230,7 +231,7 @@ def test_device_parse_corrupted_request(oracle_lib):
     want = [m for m, _ in oracle_frames(oracle_lib, packets)]
     status = {}
     for form in ("host", "device"):
-        eng = server.Engine(0, workers=2, device_parse=form == "device", window=8)
+        eng = server.Engine(0, workers=2, window=8, device_parse=form == "device")
         try:
             sid = eng.open_stream(352, 288)
             _submit_all(eng, sid, bad)
@@ -247,3 +248,4 @@ def test_device_parse_corrupted_request(oracle_lib):
         finally:
             eng.close()
     assert status["host"] == status["device"]
+
