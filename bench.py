@@ -496,7 +496,7 @@ def run_batched(local, dev):
 
 
 SERVED_FORMS = (("per_stream", {}), ("batched", {"groups": 2}),
-                ("per_stream_device_parse", {"device_parse": True, "window": 24}))
+                ("per_stream_device_parse", {"device_parse": True, "window": 32}))
 
 
 def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4000, 120)), n_streams=32, frames=120,
@@ -643,7 +643,7 @@ def run_served(local, rates=((100, 30), (500, 120), (1000, 120), (2000, 120), (4
             "forms": {"batched": "rv9_engine_create_batched, 2 launch groups: the next parsed frame of every stream "
                                  "of a group reconstructed together, one launch per stage per step",
                       "per_stream": "rv9_engine_create: each stream's frames on its own CUDA stream",
-                      "per_stream_device_parse": "rv9_engine_create + rv9_engine_set_device_parse (window 24): "
+                      "per_stream_device_parse": "rv9_engine_create + rv9_engine_set_device_parse (window 32): "
                                                  "a stream's queued requests (two or more) parsed on the GPU as "
                                                  "one batch, lone requests on the host"},
             "plain_single_stream_e2e_mpixels_s": round(plain, 1),

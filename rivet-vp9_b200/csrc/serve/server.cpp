@@ -86,6 +86,9 @@ struct Done {
   uint32_t n_frames = 0;
   size_t out_used = 0;  // bytes of the output buffer its frames fill
   rv9_frame frames[kMaxShown];
+  // A second shown frame that the output buffer (one frame of the stream's
+  // largest size) cannot hold: a packet normally shows one frame.
+  std::vector<uint8_t> extra;
 };
 
 enum StreamState { PENDING, ADMITTING, ACTIVE, CLOSED };
@@ -386,7 +389,7 @@ struct rv9_engine {
       ok = engine->reserve(s.spec.max_width, s.spec.max_height, s.spec.ss_x, s.spec.ss_y, s.spec.bit_depth,
                            kReservedFrames, stage_bytes_of(s.spec), &err) == rv9::ST_OK;
     std::vector<OutBuf> outs;
-    size_t cap = packed_cap(s.spec) * kMaxShown;
+    size_t cap = packed_cap(s.spec);
     // A device-parse batch takes a free output buffer per request; twice
     // the window lets the next batch fill while the last one's buffers are
     // still with the caller.
@@ -500,7 +503,6 @@ struct rv9_engine {
       d->err = "empty packet";
     }
     rv9::ParsedFrame pf;
-    size_t off = 0;
     for (auto& fr : frames) {
       rv9::Status st = host_parse(s, s.parser.begin(req.packet.data() + fr.first, fr.second, nullptr), &pf, &err);
       rv9g::DevFrame* shown = nullptr;
@@ -511,21 +513,8 @@ struct rv9_engine {
         break;
       }
       if (!shown) continue;
-      size_t nb = rv9g::Engine::packed_bytes(shown);
-      if (d->n_frames >= (uint32_t)kMaxShown || off + nb > s.outs[out].cap) {
-        d->status = RV9_UNSUPPORTED;
-        d->err = "a request showed more frames, or larger ones, than its stream spec allows";
-        break;
-      }
-      rv9_frame& f = d->frames[d->n_frames++];
-      fill_frame(shown, s.outs[out].data + off, nb, &f);
-      rv9::Status s2 = s.engine->download_async(shown, f.data, &err);
-      if (s2 != rv9::ST_OK) {
-        d->status = (rv9_status)s2;
-        d->err = err;
-        break;
-      }
-      off += nb;
+      place_frame(s, d, shown, s.engine->stream());
+      if (d->status != RV9_OK) break;
     }
     complete_after_device(s, d);
     std::lock_guard<std::mutex> lock(mu);
@@ -894,23 +883,34 @@ struct rv9_engine {
     return s.open_done;
   }
 
-  // A shown frame's copy into its request's output buffer (queued on `gs`).
+  // A shown frame's copy into its request's output buffer (queued on `gs`),
+  // or, for a second frame the buffer cannot hold, into the request's heap
+  // buffer (a copy into pageable memory, which returns once done).
   void place_frame(Stream& s, Done* d, rv9g::DevFrame* shown, cudaStream_t gs) {
     const size_t nb = rv9g::Engine::packed_bytes(shown);
-    if (d->n_frames >= (uint32_t)kMaxShown || d->out_used + nb > s.outs[(size_t)d->out].cap) {
+    if (d->n_frames >= (uint32_t)kMaxShown || nb > packed_cap(s.spec)) {
       d->status = RV9_UNSUPPORTED;
       d->err = "a request showed more frames, or larger ones, than its stream spec allows";
       return;
     }
+    const OutBuf& b = s.outs[(size_t)d->out];
+    const bool fits = d->out_used + nb <= b.cap;
+    uint8_t* dst;
+    if (fits) {
+      dst = b.data + d->out_used;
+    } else {
+      d->extra.resize(nb);  // once: the first frame is in the output buffer
+      dst = d->extra.data();
+    }
     rv9_frame& f = d->frames[d->n_frames++];
-    fill_frame(shown, s.outs[(size_t)d->out].data + d->out_used, nb, &f);
+    fill_frame(shown, dst, nb, &f);
     std::string err;
     if (s.engine->download_on(shown, f.data, gs, &err) != rv9::ST_OK) {
       d->status = RV9_DEVICE;
       d->err = err;
       return;
     }
-    d->out_used += nb;
+    if (fits) d->out_used += nb;
   }
 
   // Queues the completion behind the work on `gs`.

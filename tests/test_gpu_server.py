@@ -249,3 +249,34 @@ def test_device_parse_corrupted_request(oracle_lib):
             eng.close()
     assert status["host"] == status["device"]
 
+
+
+def _superframe(frames):
+    """The frames as one VP9 superframe (the index of Annex B: a marker byte,
+    4-byte little-endian sizes, the marker again)."""
+    marker = 0xC0 | (3 << 3) | (len(frames) - 1)
+    index = bytes([marker]) + b"".join(len(f).to_bytes(4, "little") for f in frames) + bytes([marker])
+    return b"".join(frames) + index
+
+
+def test_a_request_showing_two_frames(groups, oracle_lib):
+    """A request whose packet shows two frames (two shown frames joined in a
+    superframe): the first goes to the request's output buffer, the second
+    to its own heap buffer; both exact, in order."""
+    from conftest import oracle_frames
+    from streams_cases import generate
+    packets, _ = generate("cif_8bit_q60")
+    want = [m for m, _ in oracle_frames(oracle_lib, packets)]
+    joined = [packets[0], _superframe([packets[1], packets[2]])] + packets[3:]
+    eng = _engine(groups, workers=2)
+    try:
+        sid = eng.open_stream(352, 288)
+        _submit_all(eng, sid, joined)
+        done = _drain(eng, len(joined))
+        assert [c.tag for c in done] == list(range(len(joined)))
+        assert all(c.ok for c in done)
+        assert [c.n_frames for c in done][:3] == [1, 2, 1]
+        assert _md5s(done, sid) == want
+        eng.close_stream(sid)
+    finally:
+        eng.close()
