@@ -58,8 +58,8 @@ void rv9_engine_free(rv9_engine* eng);
  * Each such stream keeps 2 x `window` output buffers and reserves room for
  * a batch's device records (rv9_engine_stream_reservation). A frame that
  * fails fails its request and the requests of the same batch after it.
- * `on` = 0 turns it off for streams opened later. Results are
- * bit-identical to host parsing. */
+ * `on` = 0 stops further batches; streams opened later reserve nothing
+ * for them. Results are bit-identical to host parsing. */
 rv9_status rv9_engine_set_device_parse(rv9_engine* eng, int on, uint32_t window, uint32_t max_batches);
 
 /* The largest frame a stream will carry, which sizes its reservation. */
