@@ -781,50 +781,64 @@ def run_gpu(args, world, rank, local):
     e2e_md5s = [frame_md5s(o[:nb].numpy(), sz) for o, (_, nb), sz in zip(host_outs, results, sizes)]
     # The same end-to-end passes with device parsing (rv9_decoder_set_device_parse):
     # every frame's tile columns parsed on the GPU and its work lists built
-    # there; the host keeps the frame headers.
-    for d in decs:
-        d.set_device_parse(True, 64)
-    dp_secs, dp_each, dp_results = 0.0, [], None
-    dp0 = [d.device_parse_stats() for d in decs]
+    # there; the host keeps the frame headers. Then shared: each stream's
+    # batch split between the host's threads and the device, the split
+    # balanced from the measured times of the passes before.
+    def device_parse_passes(mode, warm):
+        for d in decs:
+            d.set_device_parse(mode, 64)
+        secs, each, res = 0.0, [], None
+        s0 = [d.device_parse_stats() for d in decs]
+        for i in range(e2e_steps + warm):
+            dist_barrier(world)
+            dt, res = e2e_pass(decs, packets, host_outs)
+            if i < warm:
+                s0 = [d.device_parse_stats() for d in decs]
+            else:
+                secs += dt
+                each.append(round(dt * 1e3, 1))
+        s1 = [d.device_parse_stats() for d in decs]
+        for d in decs:
+            d.set_device_parse(False)
+        secs = dist_max(secs, world, dev)
+        md5s = [frame_md5s(o[:nb].numpy(), sz) for o, (_, nb), sz in zip(host_outs, res, sizes)]
+        line = {
+            "value": round(luma_per_step * e2e_steps * world / secs / 1e6, 2), "unit": "Mpixels/s",
+            "steps": e2e_steps, "ms_each_step": each,
+            "frames_device_parsed_per_step": int(sum(b[0] - a[0] for a, b in zip(s0, s1)) / e2e_steps),
+            "bools_per_step": int(sum(b[1] - a[1] for a, b in zip(s0, s1)) / e2e_steps),
+            "parse_device_ms_per_stream": [round((b[2] - a[2]) / e2e_steps, 1) for a, b in zip(s0, s1)],
+        }
+        return line, md5s
+
     # Two untimed passes: a call is one batch per stream, and batches
     # alternate between two stage buffers, each allocated on first use.
-    for i in range(e2e_steps + 2):
-        dist_barrier(world)
-        dt, dp_results = e2e_pass(decs, packets, host_outs)
-        if i <= 1:
-            dp0 = [d.device_parse_stats() for d in decs]
-        else:
-            dp_secs += dt
-            dp_each.append(round(dt * 1e3, 1))
-    dp1 = [d.device_parse_stats() for d in decs]
-    for d in decs:
-        d.set_device_parse(False)
-    dp_secs = dist_max(dp_secs, world, dev)
-    dp_md5s = [frame_md5s(o[:nb].numpy(), sz) for o, (_, nb), sz in zip(host_outs, dp_results, sizes)]
-    dp_bools = sum(b[1] - a[1] for a, b in zip(dp0, dp1)) / e2e_steps
-    dp_ms = [(b[2] - a[2]) / e2e_steps for a, b in zip(dp0, dp1)]
-    e2e_device_parse = {
-        "value": round(luma_per_step * e2e_steps * world / dp_secs / 1e6, 2), "unit": "Mpixels/s",
-        "steps": e2e_steps, "ms_each_step": dp_each,
-        "frames_device_parsed_per_step": int(sum(b[0] - a[0] for a, b in zip(dp0, dp1)) / e2e_steps),
-        "bools_per_step": int(dp_bools),
-        "parse_device_ms_per_stream": [round(m, 1) for m in dp_ms],
-        "how": "rv9_decode_packets with rv9_decoder_set_device_parse(1, 64): each stream's 60 frames go to the "
-               "GPU as one batch (one thread per tile column, 240 columns per stream; then one CTA per frame "
-               "builds its work lists), reconstructed in order as usual; parse_device_ms is the batch's CUDA-event "
-               "time on its stream (the two streams' batches overlap)",
-    }
+    e2e_device_parse, dp_md5s = device_parse_passes(1, 2)
+    e2e_device_parse["how"] = (
+        "rv9_decode_packets with rv9_decoder_set_device_parse(1, 64): each stream's 60 frames go to the GPU as one "
+        "batch (one thread per tile column, 240 columns per stream; then one CTA per frame builds its work lists), "
+        "reconstructed in order as usual; parse_device_ms is the batch's CUDA-event time on its stream (the two "
+        "streams' batches overlap)")
+    # Four untimed passes: the split settles.
+    e2e_shared, sh_md5s = device_parse_passes(rv9.DEVICE_PARSE_SHARED, 4)
+    e2e_shared["how"] = (
+        "rv9_decode_packets with rv9_decoder_set_device_parse(RV9_DEVICE_PARSE_SHARED, 64): each stream's batch "
+        "(its frames are all error-resilient) split so that the host parses its first part on its threads while "
+        "the device parses the rest, the split balanced from the passes before; frames_device_parsed_per_step "
+        "is the device's part")
     del host_outs
     check = {"how": "per-frame MD5 of every shown frame of both streams, from an untimed replay (frame sinks) "
                     "and from the last end-to-end pass, against the oracle's decode of the same packets"}
     if want:
-        for s, w, r, e, dp in zip(W.CONFIG2, want, replay_md5s, e2e_md5s, dp_md5s):
+        for s, w, r, e, dp, sh in zip(W.CONFIG2, want, replay_md5s, e2e_md5s, dp_md5s, sh_md5s):
             check[f"replay_{s['name']}"] = compare(r, [m for m, _ in w])
             check[f"e2e_{s['name']}"] = compare(e, [m for m, _ in w])
             check[f"e2e_device_parse_{s['name']}"] = compare(dp, [m for m, _ in w])
+            check[f"e2e_shared_{s['name']}"] = compare(sh, [m for m, _ in w])
     else:
         check["e2e_equals_replay"] = e2e_md5s == replay_md5s
         check["e2e_device_parse_equals_replay"] = dp_md5s == replay_md5s
+        check["e2e_shared_equals_replay"] = sh_md5s == replay_md5s
     extra = {}
     sections = args.sections.split(",") if world == 1 else []
     if "config3" in sections:
@@ -849,6 +863,7 @@ def run_gpu(args, world, rank, local):
                             "prediction, no backward adaptation), as the reference's own encoder does; the 15 "
                             "conformance vectors cover the rest for parity"},
             "e2e_device_parse": e2e_device_parse,
+            "e2e_shared": e2e_shared,
             "roofline": roofline,
             "autotune": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in tuned.items()},
             "graph_replay": {"value": round(whole_job_value(luma_per_step, world, ms_graph), 2),

@@ -102,7 +102,13 @@ void rv9_decoder_set_max_pixels(rv9_decoder* dec, uint64_t pixels);
  * (every frame of the generated streams but 4:2:2 / 4:4:4 key frames). The
  * other frames parse on the host, in order. Results are identical to host
  * parsing. rv9_sequence_load takes the device path only when every frame
- * allows it. */
+ * allows it. With `on` = RV9_DEVICE_PARSE_SHARED, rv9_decode_packets splits
+ * each batch whose frames are all independent of one another (key frames
+ * and error-resilient frames) between the host, which parses its first part
+ * frame-parallel on its threads, and the device, which parses the rest
+ * meanwhile; the split follows the two sides' measured times, so that both
+ * end together. */
+#define RV9_DEVICE_PARSE_SHARED 2
 rv9_status rv9_decoder_set_device_parse(rv9_decoder* dec, int on, uint32_t window_frames);
 /* Frames the device parser took, its boolean decodes, and the device time
  * of its batches (tile parse and work lists, CUDA events on its stream). */

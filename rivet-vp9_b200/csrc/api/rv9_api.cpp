@@ -27,6 +27,8 @@ struct rv9_decoder {
   uint32_t threads = 0;      // set_threads value; 0: one per core
   // Device parsing (rv9_decoder_set_device_parse).
   bool device_parse = false;
+  bool dp_shared = false;  // RV9_DEVICE_PARSE_SHARED
+  double dp_share = 0.25;  // the device's part of a shared batch, as last balanced
   uint32_t dp_window = 64;
   std::unique_ptr<rv9g::DeviceParser> dp;
   cudaStream_t dp_stream = nullptr;
@@ -101,6 +103,7 @@ rv9_status rv9_decoder_set_device_parse(rv9_decoder* d, int on, uint32_t window_
   if (!d) return RV9_INVALID_INPUT;
   d->dp_window = window_frames ? window_frames : 64;
   d->device_parse = on != 0;
+  d->dp_shared = on == RV9_DEVICE_PARSE_SHARED;
   if (!on || d->dp) return RV9_OK;
   cudaError_t e = cudaSetDevice(d->engine.device());
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d->dp_stream, cudaStreamNonBlocking);
@@ -236,8 +239,117 @@ static rv9_status decode_packets_device(rv9_decoder* d, const uint8_t* const* pk
     ++*n_frames;
     return RV9_OK;
   };
+  // A shared batch: pending[0, h) parse on the host, frame-parallel on its
+  // threads, while pending[h, n) parse on the device (a thread of its own
+  // waits for them); then both parts reconstruct in order. Only for frames
+  // that depend on nothing earlier frames decide at finish, so that every
+  // one may parse before those before it finish.
+  auto flush_shared = [&]() -> rv9_status {
+    const size_t n = pending.size();
+    size_t n_dev = (size_t)(d->dp_share * (double)n + 0.5);
+    n_dev = std::max<size_t>(1, std::min(n - 1, n_dev));
+    const size_t h = n - n_dev;
+    P.clear();
+    for (size_t i = h; i < n; ++i) {
+      rv9::Parser::ExternalTiles x;
+      if (!d->parser.external_tiles(pending[i], &x) || !P.add(x, *x.desc)) {
+        // Cannot happen for a frame the batch took; kept whole on the host.
+        P.clear();
+        return RV9_DEVICE;
+      }
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    rv9::Status dst = rv9::ST_OK;
+    std::string derr;
+    double dev_s = 0;
+    const int device = d->engine.device();
+    std::thread dev([&]() {
+      cudaSetDevice(device);
+      cudaEventRecord(d->dp_ev[0], d->dp_stream);
+      dst = P.launch(d->dp_stream, &derr);
+      if (dst == rv9::ST_OK) dst = P.collect(d->dp_stream, &derr);
+      cudaEventRecord(d->dp_ev[1], d->dp_stream);
+      dev_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+    const size_t depth = (size_t)parse_depth(d);
+    size_t started = 0;
+    while (started < std::min(depth, h)) d->parser.run_async(pending[started++]);
+    rv9_status st = RV9_OK;
+    size_t i = 0;
+    for (; i < h && st == RV9_OK; ++i) {
+      d->parser.wait(pending[i]);
+      rv9::Status s2 = d->parser.finish(pending[i], &d->pf, &d->err);
+      d->parser.release(pending[i]);
+      pending[i] = nullptr;
+      rv9g::DevFrame* shown = nullptr;
+      if (s2 == rv9::ST_OK) s2 = d->engine.recon(d->pf, &shown, &d->err);
+      st = s2 == rv9::ST_OK ? show(shown) : (rv9_status)s2;
+      if (started < h) d->parser.run_async(pending[started++]);
+    }
+    const double host_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    dev.join();
+    if (st == RV9_OK && dst != rv9::ST_OK) {
+      d->err = derr;
+      st = (rv9_status)dst;
+    }
+    if (st != RV9_OK) {
+      release_pending(i);  // the jobs not finished (release joins any still parsing)
+      return st;
+    }
+    float ms = 0;
+    if (cudaEventSynchronize(d->dp_ev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, d->dp_ev[0], d->dp_ev[1]) == cudaSuccess)
+      d->dp_ms += ms;
+    // The next split: the device's part takes about as long whatever its
+    // size (its tile columns run side by side), the host's grows with its
+    // frames, so the host takes as many as it parses in the device's time.
+    if (host_s > 0 && dev_s > 0) {
+      const double per_frame = host_s / (double)h;
+      const double want = 1.0 - std::min(1.0, dev_s / (per_frame * (double)n));
+      d->dp_share = std::max(0.05, std::min(0.95, 0.5 * (d->dp_share + want)));
+    }
+    for (size_t j = h; j < n; ++j) {
+      std::string msg;
+      const rv9::Status ts = P.frame_status(j - h, &msg);
+      rv9::ParsedFrame meta;
+      rv9::Status s2 = d->parser.finish_external(pending[j], ts, msg, &meta, &d->err);
+      d->parser.release(pending[j]);
+      pending[j] = nullptr;
+      if (s2 != rv9::ST_OK) {
+        release_pending(j + 1);
+        return (rv9_status)s2;
+      }
+      rv9g::FrameWork fw;
+      fw.desc = meta.desc;
+      fw.show_existing = false;
+      fw.show_frame = meta.show_frame;
+      fw.refresh_mask = meta.refresh_mask;
+      for (int k = 0; k < 3; ++k) fw.ref_slot[k] = meta.ref_slot[k];
+      P.frame_work(j - h, &fw);
+      rv9g::DevFrame* shown = nullptr;
+      s2 = d->engine.recon_resident(fw, P.frame_base(j - h), &shown, &d->err);
+      if (s2 != rv9::ST_OK) {
+        release_pending(j + 1);
+        return (rv9_status)s2;
+      }
+      ++d->dp_frames;
+      rv9_status s3 = show(shown);
+      if (s3 != RV9_OK) {
+        release_pending(j + 1);
+        return s3;
+      }
+    }
+    pending.clear();
+    rv9::Status s4 = P.recon_queued(d->engine.stream(), &d->err);
+    P.clear();
+    return (rv9_status)s4;
+  };
   auto flush = [&]() -> rv9_status {
     if (pending.empty()) return RV9_OK;
+    if (d->dp_shared && pending.size() >= 2) {
+      bool all = true;
+      for (rv9::Parser::Job* j : pending) all = all && d->parser.independent(j);
+      if (all) return flush_shared();
+    }
     rv9::Status st;
     cudaEventRecord(d->dp_ev[0], d->dp_stream);
     if ((st = P.launch(d->dp_stream, &d->err)) != rv9::ST_OK || (st = P.collect(d->dp_stream, &d->err)) != rv9::ST_OK) {

@@ -940,6 +940,23 @@ Status Parser::finish_external(Job* job, Status tiles_st, const std::string& til
   return finish(job, out, err);
 }
 
+bool Parser::independent(const Job* job) const {
+  return job->st == ST_OK && !job->show_existing && !job->use_prev &&
+         (job->h.error_resilient_mode || job->h.frame_type == KEY_FRAME);
+}
+
+void Parser::run_async(Job* job) {
+  attach_work(job);
+  if (job->st != ST_OK || job->show_existing) return;
+  job->running = true;
+  job->th = std::thread([this, job]() { run(job); });
+}
+
+void Parser::wait(Job* job) {
+  if (job->th.joinable()) job->th.join();
+  job->running = false;
+}
+
 void Parser::bind_prev(Job* job) {
   if (job->st != ST_OK || job->show_existing || !job->use_prev_hdr) return;
   const FrameState& S = impl_->s;

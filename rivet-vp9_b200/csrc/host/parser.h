@@ -129,6 +129,14 @@ class Parser {
     const rv9_frame_desc* desc = nullptr;    // the records' frame description
   };
   bool external_tiles(const Job* job, ExternalTiles* out) const;
+  // Whether the frame depends on nothing that frames before it decide at
+  // finish (a key frame or an error-resilient one: contexts reset, no
+  // previous motion vectors), so that it may parse while they do.
+  bool independent(const Job* job) const;
+  // attach_work, then run on a thread of the job's own; wait joins it
+  // (finish and release need it joined; release joins it too).
+  void run_async(Job* job);
+  void wait(Job* job);
   Status finish_external(Job* job, Status tiles_st, const std::string& tiles_err, ParsedFrame* out,
                          std::string* err);
   void bind_prev(Job* job);

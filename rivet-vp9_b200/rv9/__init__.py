@@ -204,6 +204,7 @@ class Sequence:
             self._h = None
 
 
+DEVICE_PARSE_SHARED = 2  # rv9_decoder_set_device_parse: host and device share a batch
 RV9_RUN_PER_KERNEL = 1
 RV9_RUN_GRAPH = 2
 
@@ -351,8 +352,11 @@ class Decoder:
 
     def set_device_parse(self, on=True, window_frames=0):
         """Parse tiles on the GPU where the frames allow it (rv9_decoder_set_device_parse):
-        decode_packets and load_sequence then take that path; results are identical."""
-        st = self._lib.rv9_decoder_set_device_parse(self._dec, 1 if on else 0, window_frames)
+        decode_packets and load_sequence then take that path; results are identical.
+        on=DEVICE_PARSE_SHARED splits batches of independent frames between the host's
+        threads and the device."""
+        mode = on if (isinstance(on, int) and not isinstance(on, bool)) else (1 if on else 0)
+        st = self._lib.rv9_decoder_set_device_parse(self._dec, mode, window_frames)
         if st != 0:
             _raise(self._lib, self._dec, st)
 

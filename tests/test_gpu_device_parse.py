@@ -158,3 +158,29 @@ def test_corrupted_frame_reports_like_host_parsing(oracle_lib):
         finally:
             dec.close()
     assert results[0] == results[1]
+
+
+@pytest.mark.parametrize("window", [4, 64])
+@pytest.mark.parametrize("name", ["cif_8bit_q60", "1080p_8bit_q40", "720p_10bit_422_q50", "cif_8bit_linked",
+                                  "720p_8bit_linked"])
+def test_shared_batches(name, window, oracle_lib):
+    """RV9_DEVICE_PARSE_SHARED: a batch of independent frames split between
+    the host's threads and the device (the split moving between calls), the
+    linked streams' batches left whole on the device; every frame exact."""
+    import rv9
+    packets = generate(name)[0] if name in CASES else generate_linked(name)
+    want = oracle_frames(oracle_lib, packets)
+    sizes = [s for _, s in want]
+    dec = rv9.Decoder(0)
+    try:
+        dec.set_device_parse(rv9.DEVICE_PARSE_SHARED, window)
+        for _ in range(3):
+            nf, nb, buf = _decode(dec, packets, sum(sizes))
+            assert (nf, nb) == (len(sizes), sum(sizes))
+            assert split_md5s(buf, sizes) == [m for m, _ in want]
+        frames, bools, ms = dec.device_parse_stats()
+        assert 0 < frames <= 3 * len(packets)
+        if name in CASES:
+            assert frames < 3 * len(packets)  # the host took its part
+    finally:
+        dec.close()
