@@ -2,7 +2,10 @@
 and decoder state of frame-by-frame parsing: on every conformance vector
 (whose frames mostly depend on each other, so the pipeline settles them in
 turn), on generated error-resilient streams (which parse several frames at
-once), and across corrupted packets."""
+once), and across corrupted packets. So does the host side of a shared
+device-parse batch (RV9_DEVICE_PARSE_SHARED): frames begun in batches before
+any finishes, an all-independent batch run on threads (Parser::run_async)
+and finished in order."""
 import ctypes
 import os
 import subprocess
@@ -28,6 +31,9 @@ def shim():
     lib.pipeline_check.restype = ctypes.c_int
     lib.pipeline_check.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    lib.shared_batch_check.restype = ctypes.c_int
+    lib.shared_batch_check.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     return lib
 
 
@@ -71,3 +77,40 @@ def test_corrupted_packets(shim):
     vec = read_packets(os.path.join(REPO, "tests", "golden", "vectors", "vp90-2-05-resize.ivf"))
     vec[5] = bytes(b ^ 0x5A for b in vec[5])
     assert check(shim, vec, depth=3) == len(vec)
+
+
+def shared_check(lib, packets, window, depth):
+    n = len(packets)
+    arr = (ctypes.c_char_p * n)(*packets)
+    lens = (ctypes.c_size_t * n)(*[len(p) for p in packets])
+    msg = ctypes.create_string_buffer(256)
+    r = lib.shared_batch_check(arr, lens, n, window, depth, msg, 256)
+    assert r >= 0, msg.value.decode()
+    return r
+
+
+@pytest.mark.parametrize("name", ["cif_8bit_q60", "720p_10bit_422_q50"])
+def test_shared_batches_error_resilient(shim, name):
+    # Every inter frame is independent: batches of two or more run on threads.
+    packets, _ = generate(name)
+    for window, depth in ((2, 1), (3, 2), (64, 8)):
+        assert shared_check(shim, packets, window, depth) > 0
+
+
+@pytest.mark.parametrize("name", sorted(LINKED))
+def test_shared_batches_linked(shim, name):
+    # Frames that read the previous frame's motion vectors are not independent:
+    # their batches finish one by one.
+    packets = generate_linked(name)
+    for window in (2, 8):
+        shared_check(shim, packets, window, 4)
+
+
+def test_shared_batches_vectors_and_corruption(shim):
+    for path in vector_paths()[:6]:
+        shared_check(shim, read_packets(path), 8, 4)
+    packets, _ = generate("cif_8bit_q60")
+    bad = list(packets)
+    bad[2] = bad[2][: len(bad[2]) // 3]
+    bad.insert(4, b"\x82\x49\x83\x42\x00garbage")
+    shared_check(shim, bad, 8, 4)
