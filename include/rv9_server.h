@@ -107,7 +107,8 @@ typedef struct rv9_completion {
  * `timeout_ms` for the first (0: no wait). Returns how many were written. */
 size_t rv9_poll(rv9_engine* eng, rv9_completion* out, size_t cap, int timeout_ms);
 /* Returns a completion's frame buffers to its stream. A stream holds four
- * output buffers: requests wait while all four are out. */
+ * output buffers (twice the window with device parsing), each one frame of
+ * its largest size: requests wait while all are out. */
 void rv9_completion_release(rv9_engine* eng, rv9_completion* c);
 
 typedef struct rv9_engine_stats {
